@@ -1,0 +1,118 @@
+/*
+ * psdns_gpu.h -- C-ABI of libpsdns_gpu, the B200 (sm_100a) implementation of
+ * the PSDNS RK2 time-step hot path.
+ *
+ * The reference exposes no plugin API: one RK stage is the sequence of
+ * Fortran calls in rksubstep (PSDNS/timestep_module.f:152-318) operating on
+ * module globals (PSDNS/module.f:324-385), and one time step is the call
+ * `call timestep()` at PSDNS/main.f:463 preceded by `call shifts` at
+ * PSDNS/main.f:409.  Each entry point below names the reference routine(s)
+ * it replaces.
+ *
+ * Conventions (Fortran iso_c_binding friendly):
+ *  - every function returns int status: 0 = ok, nonzero = error; the
+ *    message is available from psdns_gpu_last_error();
+ *  - nothing aborts or traps; device-side failures set a status word;
+ *  - scalars that the driver may want to pass by reference are pointers;
+ *  - arrays are plain pointers with explicit sizes; complex data is
+ *    interleaved (re, im) doubles, i.e. Fortran complex(8);
+ *  - host buffers are borrowed for the duration of the call only; the
+ *    library owns all device memory.
+ *  - one host thread per context; one CUDA stream per context.
+ */
+#ifndef PSDNS_GPU_H
+#define PSDNS_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Precision of the device state and of the bulk FFT arithmetic. */
+#define PSDNS_PREC_FP32 0
+#define PSDNS_PREC_FP64 1
+
+/* State layouts for set/get.
+ * PSDNS_LAYOUT_YCYL: the reference's y-cylinder array uy(ny,num_al,nv) of a
+ *   single rank (jproc = 1), column-major: element (y, a, v) at
+ *   ((v*xz_tot + a)*ny + y); a enumerates the (kx,kz) columns inside the
+ *   truncation cylinder in the order of next_xz (PSDNS/mpisetup.f:710-732). */
+#define PSDNS_LAYOUT_YCYL 0
+
+/* Which field get_state returns. */
+#define PSDNS_FIELD_U  0   /* u  (module comp, PSDNS/module.f:324-385) */
+#define PSDNS_FIELD_UN 1   /* un */
+
+typedef struct psdns_params {
+    int32_t nx, ny, nz;      /* grid; cubic boxes (nx = ny = nz), nx even */
+    int32_t nc;              /* passive scalars (0 or 1)                     */
+    int32_t precision;       /* PSDNS_PREC_FP32 or PSDNS_PREC_FP64           */
+    int32_t kshift;          /* 1..4, PSDNS/shifts.f:7-26                    */
+    int32_t ksran;           /* RNG sequence for shifts (PSDNS/input.f:269)  */
+    int32_t seed_input;      /* iseed record of the input file               */
+    int32_t kranf1, kranf2;  /* RNG sequences for forcing (PSDNS/input.f:268)*/
+    int32_t reserved_i[6];
+    double viscos;           /* kinematic viscosity                          */
+    double beta1, beta2, beta3; /* box scaling; 1 for a 2*pi box             */
+    double cfl;              /* > 0: dt = cfl/velmax (PSDNS/step.f:77-78)    */
+    double dt;               /* fixed time step when cfl <= 0                */
+    double kforce;           /* Eswaran-Pope forcing radius; 0 = unforced    */
+    double tforce, epsfor, tfiuo; /* forcing parameters (PSDNS/force.f:20-27) */
+    double pr;               /* Schmidt number of the scalar                 */
+    double grad[3];          /* mean scalar gradient                         */
+    double reserved_d[8];
+} psdns_params;
+
+/* Fill *p with the reference's defaults (PSDNS/input and PSDNS/input.f). */
+int psdns_gpu_default_params(psdns_params *p);
+
+/* Truncation-cylinder geometry for an n^3 box (PSDNS/mpisetup.f:307-357):
+ * number of kx columns kept (max_al_x), xz_tot, and optionally cut_z(x)
+ * (array of *kxn ints) and the column start offsets (array of *kxn+1). */
+int psdns_gpu_geometry(int32_t n, int32_t *kxn, int32_t *xz_tot,
+                       int32_t *cut_z, int32_t *colstart);
+
+/* Create a context: validate parameters, build the cylinder map and the
+ * spherical mask (PSDNS/masks.f), allocate the device state and work
+ * arrays, and build twiddle tables.  Replaces the set-up calls of
+ * PSDNS/main.f:160-286 (param_set, mpisetup, mpisetup2, epfftw, masks). */
+int psdns_gpu_init(const psdns_params *p, void **ctx);
+
+/* Release the context (and its device memory).  Replaces the end of main. */
+int psdns_gpu_finalize(void *ctx);
+
+/* Load the velocity state un (and u = un, PSDNS/incond.f:146) from a host
+ * array in the given layout (complex(8), 3+nc variables). */
+int psdns_gpu_set_state(void *ctx, const double *un, int32_t layout);
+
+/* Copy u or un back to a host array (complex(8), 3+nc variables). */
+int psdns_gpu_get_state(void *ctx, double *out, int32_t which, int32_t layout);
+
+/* One full RK2 time step: shifts (PSDNS/shifts.f), then rksubstep(1) and
+ * rksubstep(2) (PSDNS/timestep_module.f:25-55) with step/force at stage 1.
+ * On return info[0..7] = dt, time, velmax, courant number, gsh(1..3,1)
+ * (predictor shifts; info may be NULL). */
+int psdns_gpu_step(void *ctx, double *info);
+
+/* One RK stage with caller-supplied shifts and time step (the Fortran
+ * driver keeps control of dt, PSDNS/timestep_module.f:70-481):
+ * kstep = 1 or 2; gsh = gsh(3,2) column-major (PSDNS/shifts.f);
+ * dt = time step (stage 1; ignored at stage 2, which reuses stage 1's);
+ * velmax_out (stage 1) receives max N(|u|+|v|+|w|) (PSDNS/realspace_vel.f:108-110).
+ * forcing may be NULL (unforced); otherwise for(kfor,k2fo,k2fo,3) complex(8)
+ * (PSDNS/force.f:115-161). */
+int psdns_gpu_rk_stage(void *ctx, int32_t kstep, const double *gsh, const double *dt,
+                       const double *forcing, double *velmax_out);
+
+/* Run statistics: time, dt, velmax, jstep. */
+int psdns_gpu_get_time(void *ctx, double *out4);
+
+/* Message of the last error on this thread ("" if none). */
+int psdns_gpu_last_error(char *buf, int32_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSDNS_GPU_H */

@@ -1,0 +1,678 @@
+// psdns_api.cu -- host side of libpsdns_gpu: the C-ABI of include/psdns_gpu.h.
+//
+// Host responsibilities mirror the parts of the reference driver that stay on
+// the CPU: the cylinder geometry and mask (PSDNS/mpisetup.f:307-357,
+// PSDNS/masks.f), the grid-shift random numbers (PSDNS/shifts.f with
+// PSDNS/ranu.f, PSDNS/ranseq.f), the time-step control and integrating
+// factors (PSDNS/step.f) and the forcing table (PSDNS/force.f).  Everything
+// proportional to the grid runs in the kernels of stage_kernels.cuh.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "psdns_gpu.h"
+#include "psdns_host.h"
+#include "stage_kernels.cuh"
+
+namespace psdns {
+
+static thread_local std::string g_last_error;
+
+int set_error(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return 1;
+}
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) return set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// geometry (PSDNS/mpisetup.f:307-357, next_xz :710-732, masks.f:46-83)
+// ---------------------------------------------------------------------------
+void build_geometry(int n, Geometry& g) {
+  g.n = n;
+  g.kx.resize(n / 2 + 1);
+  g.ky.resize(n);
+  g.kz.resize(n);
+  for (int x = 0; x <= n / 2; x++) g.kx[x] = x;
+  for (int y = 0; y < n; y++) g.ky[y] = (y > n / 2) ? y - n : y;
+  for (int z = 0; z < n; z++) g.kz[z] = (z > n / 2) ? z - n : z;
+  const int ikmax = (int)((double)n * std::sqrt(2.0) / 3.0);
+  int kxn = ikmax + 1;
+  if (kxn > n / 2) kxn = n / 2;
+  g.kxn = kxn;
+  g.cut.assign(kxn, 0);
+  g.colstart.assign(kxn + 1, 0);
+  const double rnxi = 1.0 / n;
+  int tot = 0;
+  for (int x = 0; x < kxn; x++) {
+    const double t = g.kx[x] * rnxi;
+    const double rc = n * (1.0 - 2.0 * std::sqrt(2.0 / 9.0 - t * t));
+    const int c = (int)(rc / 2);
+    g.cut[x] = c;
+    g.colstart[x] = tot;
+    tot += n - 1 - c * 2;
+  }
+  g.colstart[kxn] = tot;
+  g.xz_tot = tot;
+  g.ax.resize(tot);
+  g.az.resize(tot);
+  g.kymax.resize(tot);
+  const double two9 = 2. / 9., rnyi = 1. / n, rnzi = 1. / n;
+  for (int x = 0; x < kxn; x++) {
+    const int kcx = n / 2 - 1 - g.cut[x];
+    for (int i = 0; i < 2 * kcx + 1; i++) {
+      const int a = g.colstart[x] + i;
+      const int kz = (i <= kcx) ? i : i - (2 * kcx + 1);
+      const int z = kz < 0 ? kz + n : kz;
+      g.ax[a] = x;
+      g.az[a] = z;
+      // volatile keeps each product rounded on its own (no contraction)
+      volatile double tx = g.kx[x] * rnxi;
+      volatile double sqkx = tx * tx;
+      volatile double tz = g.kz[z] * rnzi;
+      volatile double tz2 = tz * tz;
+      volatile double sqkz = tz2 + sqkx;
+      int km = -1;
+      for (int m = 0; m <= n / 2; m++) {
+        volatile double ty = m * rnyi;
+        volatile double ty2 = ty * ty;
+        volatile double sqk = ty2 + sqkz;
+        if (sqk > two9) break;
+        km = m;
+      }
+      g.kymax[a] = km;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// random numbers (PSDNS/ranu.f:27-29, PSDNS/ranseq.f:62-141)
+// ---------------------------------------------------------------------------
+void Rng::init(int32_t seed) {
+  for (int i = 0; i < 20; i++) iseq[i] = 0;
+  klast = 1;
+  iseed = 0;
+  ifst = 0;
+  seed_input = seed;
+}
+void Rng::ranseq(int k) {
+  if (ifst == 0) {
+    ifst = 1;
+    for (int i = 0; i < 20; i++) iseq[i] = seed_input;
+    klast = 1;
+    iseed = iseq[0];
+  }
+  iseq[klast - 1] = iseed;
+  klast = k;
+  iseed = iseq[k - 1];
+}
+double Rng::ranu() {
+  uint32_t s = (uint32_t)iseed * 65539u;
+  int32_t is = (int32_t)s;
+  if (is < 0) is = (int32_t)((uint32_t)is + 2147483647u + 1u);
+  iseed = is;
+  return (double)is * 0.46566127e-9;
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct Ctx {
+  psdns_params p;
+  Geometry g;
+  int n, prec, nzt, nab_i, nab_f;
+  size_t csz;  // sizeof complex element on device
+  int *d_colstart = nullptr, *d_ax = nullptr, *d_az = nullptr, *d_kymax = nullptr;
+  void *d_tw = nullptr, *d_tabs = nullptr, *d_u = nullptr, *d_un = nullptr, *d_ub = nullptr, *d_uz = nullptr;
+  void *d_forc = nullptr;
+  double* d_efkz = nullptr;
+  unsigned long long* d_velmax = nullptr;
+  void* h_tabs = nullptr;          // pinned staging of the stage tables
+  unsigned long long* h_velmax = nullptr;
+  cudaStream_t stream = nullptr;
+  size_t ub_elems = 0, uz_elems = 0, st_elems = 0;
+  // stepping state
+  Rng rng;
+  double gsh[3][2] = {{0, 0}, {0, 0}, {0, 0}}, gsh4[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  int jstep = 0;
+  double time = 0, dt = 0, dt0 = 0, dt2 = 0, velmax = 0;
+  int kfor = 0, k2fo = 0;
+};
+
+template <typename T> struct TabLayout {
+  // offsets in bytes inside the stage-table block
+  size_t sx[2], sy[2], sz[2], xf, yf, zf, total;
+  explicit TabLayout(int n) {
+    const size_t c = sizeof(C2<T>), r = sizeof(T);
+    size_t o = 0;
+    for (int k = 0; k < 2; k++) { sx[k] = o; o += c * (n / 2 + 1); }
+    for (int k = 0; k < 2; k++) { sy[k] = o; o += c * n; }
+    for (int k = 0; k < 2; k++) { sz[k] = o; o += c * n; }
+    xf = o; o += r * (n / 2 + 1);
+    yf = o; o += r * n;
+    zf = o; o += r * n;
+    total = (o + 255) & ~size_t(255);
+  }
+};
+
+static Geo make_geo(const Ctx& c) {
+  Geo g;
+  g.n = c.n; g.kxn = c.g.kxn; g.xz_tot = c.g.xz_tot; g.nzt = c.nzt;
+  g.nab_i = c.nab_i; g.nab_f = c.nab_f;
+  g.colstart = c.d_colstart; g.ax = c.d_ax; g.az = c.d_az; g.kymax = c.d_kymax;
+  return g;
+}
+
+template <typename T>
+static StageTables<T> make_tables(const Ctx& c, int ks) {
+  TabLayout<T> L(c.n);
+  const char* b = (const char*)c.d_tabs;
+  StageTables<T> st;
+  st.sx = (const C2<T>*)(b + L.sx[ks]);
+  st.sy = (const C2<T>*)(b + L.sy[ks]);
+  st.sz = (const C2<T>*)(b + L.sz[ks]);
+  st.xfac = (const T*)(b + L.xf);
+  st.yfac = (const T*)(b + L.yf);
+  st.zfac = (const T*)(b + L.zf);
+  st.forc = (c.p.kforce > 0) ? (const C2<T>*)c.d_forc : nullptr;
+  st.kfor = c.kfor; st.k2fo = c.k2fo;
+  st.kforce2 = c.p.kforce * c.p.kforce;
+  st.b11 = (T)(c.p.beta1 * c.p.beta1);
+  st.b22 = (T)(c.p.beta2 * c.p.beta2);
+  st.b33 = (T)(c.p.beta3 * c.p.beta3);
+  st.norm = (T)(c.dt2 / c.n / c.n);
+  return st;
+}
+
+// ---------------------------------------------------------------------------
+// per-(precision, n) kernel launch sequence
+// ---------------------------------------------------------------------------
+template <typename T, int N> struct Impl {
+  using C = C2<T>;
+  using TL = Tiles<T>;
+  static constexpr int L = LS<N>::value;
+  static constexpr size_t TWB = sizeof(C) * FFTPlan<T, N>::TWSIZE;
+  static size_t sm1() { return TWB + sizeof(C) * TL::TB_I * L; }
+  static size_t sm2() { return TWB + sizeof(C) * TL::XT2 * L; }
+  static size_t sm3() { return TWB + sizeof(C) * 4 * (TL::TZ / 2) * L; }
+  static size_t sm4() { return TWB + sizeof(C) * 2 * TL::XT4 * L; }
+  static size_t sm5() { return TWB + sizeof(C) * 4 * TL::TB_F * L; }
+
+  static int setup() {
+    CK(cudaFuncSetAttribute(k_yinv<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1()));
+    CK(cudaFuncSetAttribute(k_zinv<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2()));
+    CK(cudaFuncSetAttribute(k_xchain<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3()));
+    CK(cudaFuncSetAttribute(k_zfwd<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm4()));
+    CK(cudaFuncSetAttribute(k_yfwd<T, N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
+    CK(cudaFuncSetAttribute(k_yfwd<T, N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
+    return 0;
+  }
+
+  static int twiddles(Ctx& c) {
+    std::vector<C> tw(FFTPlan<T, N>::TWSIZE);
+    build_twiddles<T, N>(tw.data());
+    CK(cudaMalloc(&c.d_tw, sizeof(C) * tw.size()));
+    CK(cudaMemcpy(c.d_tw, tw.data(), sizeof(C) * tw.size(), cudaMemcpyHostToDevice));
+    return 0;
+  }
+
+  // stage part A: K1..K4 (through the forward z transform)
+  static int stage_a(Ctx& c, int kstep) {
+    Geo g = make_geo(c);
+    StageTables<T> st = make_tables<T>(c, kstep - 1);
+    const C* tw = (const C*)c.d_tw;
+    C* u = (C*)c.d_u;
+    C* ub = (C*)c.d_ub;
+    C* uz = (C*)c.d_uz;
+    const int kxn = c.g.kxn;
+    {
+      constexpr int TH = Launch<T, N, TL::TB_I>::THREADS;
+      k_yinv<T, N><<<dim3(c.nab_i, 3), TH, sm1(), c.stream>>>(g, st, u, ub, tw);
+    }
+    {
+      constexpr int TH = Launch<T, N, TL::XT2>::THREADS;
+      k_zinv<T, N><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3), TH, sm2(), c.stream>>>(g, ub, uz, tw);
+    }
+    {
+      constexpr int TH = Launch<T, N, 2 * TL::TZ>::THREADS;
+      k_xchain<T, N><<<dim3(c.nzt, N), TH, sm3(), c.stream>>>(g, uz, tw, st.b11, st.b22, st.b33, c.d_velmax,
+                                                                kstep == 1 ? 1 : 0);
+    }
+    {
+      constexpr int TH = Launch<T, N, 2 * TL::XT4>::THREADS;
+      k_zfwd<T, N><<<dim3(N, (kxn + TL::XT4 - 1) / TL::XT4), TH, sm4(), c.stream>>>(g, uz, ub, tw, st.b11, st.b33);
+    }
+    CK(cudaGetLastError());
+    return 0;
+  }
+
+  // stage part B: K5
+  static int stage_b(Ctx& c, int kstep) {
+    Geo g = make_geo(c);
+    StageTables<T> st = make_tables<T>(c, kstep - 1);
+    constexpr int TH = Launch<T, N, 4 * TL::TB_F>::THREADS;
+    if (kstep == 1)
+      k_yfwd<T, N, 1><<<c.nab_f, TH, sm5(), c.stream>>>(g, st, (const C*)c.d_ub, (C*)c.d_u, (C*)c.d_un,
+                                                        (const C*)c.d_tw, c.d_efkz);
+    else
+      k_yfwd<T, N, 2><<<c.nab_f, TH, sm5(), c.stream>>>(g, st, (const C*)c.d_ub, (C*)c.d_u, (C*)c.d_un,
+                                                        (const C*)c.d_tw, c.d_efkz);
+    CK(cudaGetLastError());
+    return 0;
+  }
+};
+
+struct Ops {
+  int (*setup)();
+  int (*twiddles)(Ctx&);
+  int (*stage_a)(Ctx&, int);
+  int (*stage_b)(Ctx&, int);
+};
+
+template <typename T, int N> static Ops ops_for() {
+  return Ops{&Impl<T, N>::setup, &Impl<T, N>::twiddles, &Impl<T, N>::stage_a, &Impl<T, N>::stage_b};
+}
+
+static bool get_ops(int prec, int n, Ops& o) {
+#define PSDNS_CASE(NN)                                                    \
+  case NN:                                                                \
+    o = (prec == PSDNS_PREC_FP64) ? ops_for<double, NN>() : ops_for<float, NN>(); \
+    return true;
+  switch (n) {
+    PSDNS_CASE(16)
+    PSDNS_CASE(32)
+    PSDNS_CASE(64)
+    PSDNS_CASE(128)
+    PSDNS_CASE(256)
+    PSDNS_CASE(512)
+    PSDNS_CASE(1024)
+    default:
+      return false;
+  }
+#undef PSDNS_CASE
+}
+
+// ---------------------------------------------------------------------------
+// shifts (PSDNS/shifts.f:40-178, compiled with -DRKFOUR as in the makefile,
+// which draws gsh(:,3:4) as well) and stage tables
+// ---------------------------------------------------------------------------
+static double cancel(double d) { return std::fmod(d + 0.5, 1.); }
+
+static void draw_shifts(Ctx& c) {
+  const int ks = c.p.kshift;
+  if (c.jstep == 1 && (ks == 1 || ks == 3)) {
+    c.rng.ranseq(c.p.ksran);
+    for (int i = 0; i < 3; i++) c.gsh[i][1] = c.rng.ranu();
+    for (int i = 0; i < 3; i++) c.gsh4[i][1] = c.rng.ranu();
+  }
+  if (ks == 1 || ks == 2) c.rng.ranseq(c.p.ksran);
+  for (int pass = 0; pass < 2; pass++) {
+    double(*g)[2] = pass == 0 ? c.gsh : c.gsh4;
+    for (int i = 0; i < 3; i++) {
+      if (ks == 1) { g[i][0] = cancel(g[i][1]); g[i][1] = c.rng.ranu(); }
+      else if (ks == 2) { g[i][0] = c.rng.ranu(); g[i][1] = cancel(g[i][0]); }
+      else if (ks == 3) { g[i][0] = cancel(g[i][1]); g[i][1] = cancel(g[i][0]); }
+      else { g[i][0] = 0.; g[i][1] = 0.; }
+    }
+  }
+}
+
+template <typename T>
+static void fill_shift_tables(Ctx& c) {
+  TabLayout<T> L(c.n);
+  char* b = (char*)c.h_tabs;
+  const int n = c.n;
+  const double pi = 4. * std::atan(1.);
+  const double ph = 2. * pi / n;
+  for (int k = 0; k < 2; k++) {
+    C2<T>* sx = (C2<T>*)(b + L.sx[k]);
+    C2<T>* sy = (C2<T>*)(b + L.sy[k]);
+    C2<T>* sz = (C2<T>*)(b + L.sz[k]);
+    for (int x = 0; x <= n / 2; x++) {
+      const double th = (ph * c.g.kx[x]) * c.gsh[0][k];
+      sx[x] = cmk<C2<T>>((T)std::cos(th), (T)std::sin(th));
+    }
+    for (int y = 0; y < n; y++) {
+      const double th = (ph * c.g.ky[y]) * c.gsh[1][k];
+      sy[y] = cmk<C2<T>>((T)std::cos(th), (T)std::sin(th));
+    }
+    for (int z = 0; z < n; z++) {
+      const double th = (ph * c.g.kz[z]) * c.gsh[2][k];
+      sz[z] = cmk<C2<T>>((T)std::cos(th), (T)std::sin(th));
+    }
+  }
+}
+
+template <typename T>
+static void fill_factor_tables(Ctx& c) {
+  TabLayout<T> L(c.n);
+  char* b = (char*)c.h_tabs;
+  const int n = c.n;
+  T* xf = (T*)(b + L.xf);
+  T* yf = (T*)(b + L.yf);
+  T* zf = (T*)(b + L.zf);
+  const double b11 = c.p.beta1 * c.p.beta1, b22 = c.p.beta2 * c.p.beta2, b33 = c.p.beta3 * c.p.beta3;
+  const double nu = c.p.viscos;
+  double term = b11 * c.dt;
+  for (int x = 0; x <= n / 2; x++) xf[x] = (T)std::exp(-(nu * (c.g.kx[x] * c.g.kx[x]) * term));
+  term = b22 * c.dt;
+  for (int y = 0; y < n; y++) yf[y] = (T)std::exp(-(nu * (c.g.ky[y] * c.g.ky[y]) * term));
+  term = b33 * c.dt;
+  for (int z = 0; z < n; z++) zf[z] = (T)std::exp(-(nu * (c.g.kz[z] * c.g.kz[z]) * term));
+}
+
+static int upload_tables(Ctx& c) {
+  const size_t tot = c.prec == PSDNS_PREC_FP64 ? TabLayout<double>(c.n).total : TabLayout<float>(c.n).total;
+  CK(cudaMemcpyAsync(c.d_tabs, c.h_tabs, tot, cudaMemcpyHostToDevice, c.stream));
+  // the staging buffer is reused by the next fill: wait for the copy
+  CK(cudaStreamSynchronize(c.stream));
+  return 0;
+}
+
+// step.f:49-99, :247-262, :280-295.  Returns nonzero on the reference's abort
+// conditions (the step is still completed; the caller decides).
+static int step_control(Ctx& c) {
+  c.dt = c.dt0;
+  int err = 0;
+  if (c.p.cfl > 0.) {
+    c.dt = c.p.cfl / c.velmax;
+    if (c.velmax < .001) err = set_error("velmax %.6e below 0.001 (step.f:79)", c.velmax);
+  }
+  c.time = c.time + c.dt;
+  if (c.dt == 0.) err = set_error("dt unexpectedly zero (step.f:256)");
+  c.dt2 = c.dt / 2.;
+  if (c.p.cfl > 0.) {
+    if (c.dt > 10. || c.dt < 1.e-7) err = set_error("dt out of control: %.6e (step.f:280)", c.dt);
+  } else if (c.p.cfl < 0.) {
+    const double cn = c.velmax * c.dt / 2. / (4. * std::atan(1.));
+    if (cn > 1) err = set_error("courant number %.4f exceeds 1 (step.f:292)", cn);
+  }
+  return err;
+}
+
+static int run_stage(Ctx& c, const Ops& o, int kstep, int* ctl_err) {
+  if (kstep == 1) CK(cudaMemsetAsync(c.d_velmax, 0, sizeof(unsigned long long), c.stream));
+  if (o.stage_a(c, kstep)) return 1;
+  if (kstep == 1) {
+    CK(cudaMemcpyAsync(c.h_velmax, c.d_velmax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    double vm;
+    std::memcpy(&vm, c.h_velmax, sizeof vm);
+    c.velmax = vm;
+    *ctl_err = step_control(c);
+    if (c.prec == PSDNS_PREC_FP64) fill_factor_tables<double>(c); else fill_factor_tables<float>(c);
+    if (upload_tables(c)) return 1;
+  }
+  if (o.stage_b(c, kstep)) return 1;
+  return 0;
+}
+
+}  // namespace psdns
+
+using namespace psdns;
+
+extern "C" {
+
+int psdns_gpu_last_error(char* buf, int32_t len) {
+  if (!buf || len <= 0) return 1;
+  std::snprintf(buf, (size_t)len, "%s", g_last_error.c_str());
+  return 0;
+}
+
+int psdns_gpu_default_params(psdns_params* p) {
+  if (!p) return set_error("null params");
+  std::memset(p, 0, sizeof *p);
+  p->nx = p->ny = p->nz = 64;
+  p->nc = 0;
+  p->precision = PSDNS_PREC_FP32;
+  p->kshift = 1;
+  p->ksran = 1;
+  p->seed_input = 122929298;   // PSDNS/input, iseed record
+  p->kranf1 = 5;
+  p->kranf2 = 5;
+  p->viscos = 0.0028;
+  p->beta1 = p->beta2 = p->beta3 = 1.0;
+  p->cfl = 3.77;
+  p->dt = 0.0;
+  p->kforce = 0.0;
+  p->tforce = 6.199433e-01;
+  p->epsfor = 1.77063e-03;
+  p->tfiuo = 0.4;
+  p->pr = 1.0;
+  return 0;
+}
+
+int psdns_gpu_geometry(int32_t n, int32_t* kxn, int32_t* xz_tot, int32_t* cut_z, int32_t* colstart) {
+  if (n < 8 || (n & 1)) return set_error("grid size %d not supported", n);
+  Geometry g;
+  build_geometry(n, g);
+  if (kxn) *kxn = g.kxn;
+  if (xz_tot) *xz_tot = g.xz_tot;
+  if (cut_z) for (int i = 0; i < g.kxn; i++) cut_z[i] = g.cut[i];
+  if (colstart) for (int i = 0; i <= g.kxn; i++) colstart[i] = g.colstart[i];
+  return 0;
+}
+
+int psdns_gpu_init(const psdns_params* p, void** out) {
+  if (!p || !out) return set_error("null argument");
+  *out = nullptr;
+  if (p->nx != p->ny || p->nx != p->nz) return set_error("only cubic boxes are supported (nx=ny=nz)");
+  if (p->nc != 0) return set_error("nc=%d: passive scalars are not supported by this build", p->nc);
+  if (p->precision != PSDNS_PREC_FP32 && p->precision != PSDNS_PREC_FP64)
+    return set_error("precision must be PSDNS_PREC_FP32 or PSDNS_PREC_FP64");
+  if (p->kshift < 1 || p->kshift > 4) return set_error("kshift must be 1..4");
+  if (p->ksran < 1 || p->ksran > 20 || p->kranf1 < 1 || p->kranf1 > 20 || p->kranf2 < 1 || p->kranf2 > 20)
+    return set_error("RNG sequence numbers must be 1..20 (ranseq.f:131)");
+  if (p->seed_input <= 0) return set_error("seed iseed=%d must be positive (ranu.f:33)", p->seed_input);
+  if (p->cfl <= 0. && !(p->dt > 0.)) return set_error("fixed dt must be positive when cfl <= 0");
+  Ops o;
+  if (!get_ops(p->precision, p->nx, o)) return set_error("grid size %d not supported (16..1024, powers of 2)", p->nx);
+  Ctx* c = new Ctx();
+  c->p = *p;
+  c->n = p->nx;
+  c->prec = p->precision;
+  build_geometry(c->n, c->g);
+  const int n = c->n;
+  const bool dbl = c->prec == PSDNS_PREC_FP64;
+  c->csz = dbl ? sizeof(double2) : sizeof(float2);
+  const int tbi = dbl ? Tiles<double>::TB_I : Tiles<float>::TB_I;
+  const int tbf = dbl ? Tiles<double>::TB_F : Tiles<float>::TB_F;
+  const int tz = dbl ? Tiles<double>::TZ : Tiles<float>::TZ;
+  c->nzt = n / tz;
+  c->nab_i = (c->g.xz_tot + tbi - 1) / tbi;
+  c->nab_f = (c->g.xz_tot + tbf - 1) / tbf;
+  c->ub_elems = std::max((size_t)3 * c->nab_i * tbi, (size_t)4 * c->nab_f * tbf) * n;
+  c->uz_elems = (size_t)5 * n * n * c->g.kxn;
+  c->st_elems = (size_t)3 * c->g.xz_tot * n;
+  c->rng.init(p->seed_input);
+  c->dt0 = p->dt;
+  c->dt = p->dt;
+  // forcing dimensions (param_set.f:33,37)
+  c->kfor = (int)(p->kforce / std::min(p->beta1, p->beta2 + p->beta3) + 1.5);
+  c->k2fo = 2 * c->kfor - 1;
+  auto fail = [&](int rc) { psdns_gpu_finalize(c); return rc; };
+  size_t need = c->csz * (2 * c->st_elems + c->ub_elems + c->uz_elems);
+  size_t freeb = 0, totb = 0;
+  if (cudaMemGetInfo(&freeb, &totb) != cudaSuccess) { delete c; return set_error("no CUDA device available"); }
+  if (need + (size_t)256 * 1024 * 1024 > freeb) {
+    delete c;
+    return set_error("need %.2f GB of device memory, %.2f GB free", need / 1e9, freeb / 1e9);
+  }
+  if (o.setup()) return fail(1);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(set_error("stream"));
+  const Geometry& g = c->g;
+#define ALLOC(ptr, bytes) if (cudaMalloc((void**)&(ptr), (bytes)) != cudaSuccess) return fail(set_error("cudaMalloc of %zu bytes failed", (size_t)(bytes)))
+  ALLOC(c->d_colstart, sizeof(int) * (g.kxn + 1));
+  ALLOC(c->d_ax, sizeof(int) * g.xz_tot);
+  ALLOC(c->d_az, sizeof(int) * g.xz_tot);
+  ALLOC(c->d_kymax, sizeof(int) * g.xz_tot);
+  ALLOC(c->d_u, c->csz * c->st_elems);
+  ALLOC(c->d_un, c->csz * c->st_elems);
+  ALLOC(c->d_ub, c->csz * c->ub_elems);
+  ALLOC(c->d_uz, c->csz * c->uz_elems);
+  const size_t tabb = dbl ? TabLayout<double>(n).total : TabLayout<float>(n).total;
+  ALLOC(c->d_tabs, tabb);
+  ALLOC(c->d_velmax, sizeof(unsigned long long));
+  const size_t nfor = (size_t)c->kfor * c->k2fo * c->k2fo * 3;
+  ALLOC(c->d_forc, c->csz * std::max<size_t>(nfor, 1));
+  ALLOC(c->d_efkz, sizeof(double) * 3 * (n / 2 + 2));
+#undef ALLOC
+  if (cudaMallocHost(&c->h_tabs, tabb) != cudaSuccess) return fail(set_error("cudaMallocHost"));
+  if (cudaMallocHost((void**)&c->h_velmax, sizeof(unsigned long long)) != cudaSuccess) return fail(set_error("cudaMallocHost"));
+  std::memset(c->h_tabs, 0, tabb);
+  if (cudaMemcpy(c->d_colstart, g.colstart.data(), sizeof(int) * (g.kxn + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_ax, g.ax.data(), sizeof(int) * g.xz_tot, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_az, g.az.data(), sizeof(int) * g.xz_tot, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_kymax, g.kymax.data(), sizeof(int) * g.xz_tot, cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(set_error("geometry upload failed"));
+  if (o.twiddles(*c)) return fail(1);
+  if (cudaMemset(c->d_u, 0, c->csz * c->st_elems) != cudaSuccess ||
+      cudaMemset(c->d_un, 0, c->csz * c->st_elems) != cudaSuccess ||
+      cudaMemset(c->d_forc, 0, c->csz * std::max<size_t>(nfor, 1)) != cudaSuccess ||
+      cudaMemset(c->d_efkz, 0, sizeof(double) * 3 * (n / 2 + 2)) != cudaSuccess)
+    return fail(set_error("memset failed"));
+  *out = c;
+  return 0;
+}
+
+int psdns_gpu_finalize(void* ctx) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return 0;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  void* ptrs[] = {c->d_colstart, c->d_ax, c->d_az, c->d_kymax, c->d_tw, c->d_tabs, c->d_u, c->d_un,
+                  c->d_ub, c->d_uz, c->d_forc, c->d_efkz, c->d_velmax};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  if (c->h_tabs) cudaFreeHost(c->h_tabs);
+  if (c->h_velmax) cudaFreeHost(c->h_velmax);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return 0;
+}
+
+// host (complex double, YCYL) -> device state, through ub as staging
+int psdns_gpu_set_state(void* ctx, const double* un, int32_t layout) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !un) return set_error("null argument");
+  if (layout != PSDNS_LAYOUT_YCYL) return set_error("unsupported layout %d", layout);
+  const size_t vs = (size_t)c->g.xz_tot * c->n;
+  // stage one variable at a time: ub holds >= 2 variables of complex double
+  for (int v = 0; v < 3; v++) {
+    CK(cudaMemcpyAsync(c->d_ub, un + 2 * v * vs, sizeof(double2) * vs, cudaMemcpyHostToDevice, c->stream));
+    const int blocks = 148 * 8;
+    if (c->prec == PSDNS_PREC_FP64)
+      k_from_f64<double><<<blocks, 256, 0, c->stream>>>((const double2*)c->d_ub, (double2*)c->d_un + v * vs,
+                                                         (double2*)c->d_u + v * vs, vs);
+    else
+      k_from_f64<float><<<blocks, 256, 0, c->stream>>>((const double2*)c->d_ub, (float2*)c->d_un + v * vs,
+                                                        (float2*)c->d_u + v * vs, vs);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int psdns_gpu_get_state(void* ctx, double* out, int32_t which, int32_t layout) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !out) return set_error("null argument");
+  if (layout != PSDNS_LAYOUT_YCYL) return set_error("unsupported layout %d", layout);
+  if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
+  const size_t vs = (size_t)c->g.xz_tot * c->n;
+  void* src = which == PSDNS_FIELD_U ? c->d_u : c->d_un;
+  for (int v = 0; v < 3; v++) {
+    const int blocks = 148 * 8;
+    if (c->prec == PSDNS_PREC_FP64)
+      k_to_f64<double><<<blocks, 256, 0, c->stream>>>((const double2*)src + v * vs, (double2*)c->d_ub, vs);
+    else
+      k_to_f64<float><<<blocks, 256, 0, c->stream>>>((const float2*)src + v * vs, (double2*)c->d_ub, vs);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out + 2 * v * vs, c->d_ub, sizeof(double2) * vs, cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int psdns_gpu_step(void* ctx, double* info) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return set_error("null context");
+  Ops o;
+  if (!get_ops(c->prec, c->n, o)) return set_error("bad context");
+  c->jstep += 1;
+  draw_shifts(*c);
+  if (c->prec == PSDNS_PREC_FP64) fill_shift_tables<double>(*c); else fill_shift_tables<float>(*c);
+  if (c->jstep == 1) {
+    // factor tables are filled at stage 1; zero them before the first use
+  }
+  if (upload_tables(*c)) return 1;
+  int ctl = 0;
+  if (run_stage(*c, o, 1, &ctl)) return 1;
+  if (run_stage(*c, o, 2, &ctl)) return 1;
+  CK(cudaStreamSynchronize(c->stream));
+  if (info) {
+    info[0] = c->dt;
+    info[1] = c->time;
+    info[2] = c->velmax;
+    info[3] = c->velmax * c->dt / 2. / (4. * std::atan(1.));
+    info[4] = c->gsh[0][0];
+    info[5] = c->gsh[1][0];
+    info[6] = c->gsh[2][0];
+    info[7] = (double)c->jstep;
+  }
+  return ctl ? 2 : 0;
+}
+
+int psdns_gpu_rk_stage(void* ctx, int32_t kstep, const double* gsh, const double* dt, const double* forcing,
+                       double* velmax_out) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !gsh) return set_error("null argument");
+  if (kstep != 1 && kstep != 2) return set_error("kstep must be 1 or 2");
+  if (forcing != nullptr) return set_error("forcing tables are not supported by this entry point yet");
+  Ops o;
+  if (!get_ops(c->prec, c->n, o)) return set_error("bad context");
+  for (int i = 0; i < 3; i++) { c->gsh[i][0] = gsh[i]; c->gsh[i][1] = gsh[3 + i]; }
+  if (c->prec == PSDNS_PREC_FP64) fill_shift_tables<double>(*c); else fill_shift_tables<float>(*c);
+  if (kstep == 1) {
+    if (!dt || !(*dt > 0)) return set_error("stage 1 needs a positive dt");
+    c->dt = *dt;
+    c->dt2 = c->dt / 2.;
+    if (c->prec == PSDNS_PREC_FP64) fill_factor_tables<double>(*c); else fill_factor_tables<float>(*c);
+    CK(cudaMemsetAsync(c->d_velmax, 0, sizeof(unsigned long long), c->stream));
+  }
+  if (upload_tables(*c)) return 1;
+  if (o.stage_a(*c, kstep)) return 1;
+  if (kstep == 1) {
+    CK(cudaMemcpyAsync(c->h_velmax, c->d_velmax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::memcpy(&c->velmax, c->h_velmax, sizeof(double));
+    if (velmax_out) *velmax_out = c->velmax;
+  }
+  if (o.stage_b(*c, kstep)) return 1;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int psdns_gpu_get_time(void* ctx, double* out4) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !out4) return set_error("null argument");
+  out4[0] = c->time;
+  out4[1] = c->dt;
+  out4[2] = c->velmax;
+  out4[3] = (double)c->jstep;
+  return 0;
+}
+
+}  // extern "C"

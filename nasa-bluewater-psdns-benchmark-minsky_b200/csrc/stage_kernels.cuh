@@ -1,0 +1,515 @@
+// stage_kernels.cuh -- the five fused kernels of one RK stage.
+//
+// Device data layout (one box, n^3, kxn kx columns, xz_tot cylinder columns):
+//   u, un  [v][a][y]                 y-cylinders, the reference's uy(ny,num_al,v)
+//   ub     [v][a/TB][y][a%TB]         cylinder data with y and a swapped in
+//                                    blocks of TB columns (TB_I inverse, TB_F forward)
+//   uz     [v][y][z/TZ][x][z%TZ]      z-pencils for x < kxn, blocked in z so that an
+//                                    x-line tile of TZ lines is one contiguous block
+// Per stage:
+//   K1 k_yinv   : phase shift + mask (phshift.f:71-135), y backward FFT
+//                 (kxcomm1_clean.f:118), transposed store into ub
+//   K2 k_zinv   : cylinder unpack with zero fill (kxcomm1_clean.f:205-255),
+//                 z backward FFT (itransform_vel.f:80-94), store into uz
+//   K3 k_xchain : x complex-to-real (kxcomm2.f:308-321), the five products and
+//                 velmax (realspace_vel.f:105-114), x real-to-complex times 1/n
+//                 (xkcomm1.f:97,135); the physical field never leaves the chip
+//   K4 k_zfwd   : z forward FFT (transform.f:129-138), derivative combination
+//                 (transform.f:230-234), cylinder pack (xkcomm2.f:96-125) into ub
+//   K5 k_yfwd   : y forward FFT (xkcomm2.f:229), wavespace closure
+//                 (wavespace_vel.f:163-174), proc4a/proc4b update, projection and
+//                 Eswaran-Pope forcing (proc4a.f:418-651, proc4b.f:38-205)
+#pragma once
+#include "fft_core.cuh"
+
+namespace psdns {
+
+struct Geo {
+  int n, kxn, xz_tot, nzt, nab_i, nab_f;
+  const int* colstart;   // [kxn+1]
+  const int* ax;         // [xz_tot] x index of column a
+  const int* az;         // [xz_tot] z index (0..n-1) of column a
+  const int* kymax;      // [xz_tot] largest |ky| inside the sphere
+};
+
+template <typename T> struct StageTables {
+  const C2<T>* sx;   // [n/2+1] shift factors of this stage
+  const C2<T>* sy;   // [n]
+  const C2<T>* sz;   // [n]
+  const T* xfac;     // [n/2+1] integrating factors
+  const T* yfac;     // [n]
+  const T* zfac;     // [n]
+  const C2<T>* forc; // for(kfor,k2fo,k2fo,3) or null
+  int kfor, k2fo;
+  double kforce2;    // kforce^2
+  T b11, b22, b33;
+  T norm;            // dt2/ny/nz
+};
+
+// per-precision tile sizes: TB_I = columns per K1 block (64 B segments),
+// TB_F = columns per K5 block, TZ = z lines per K3 tile (32 B runs),
+// XT2/XT4 = x lines per K2/K4 block.
+template <typename T> struct Tiles;
+template <> struct Tiles<float> { static constexpr int TB_I = 8, TB_F = 4, TZ = 4, XT2 = 8, XT4 = 4; };
+template <> struct Tiles<double> { static constexpr int TB_I = 4, TB_F = 2, TZ = 2, XT2 = 4, XT4 = 2; };
+
+template <int N> __device__ __forceinline__ int kwave(int i) { return i > N / 2 ? i - N : i; }
+
+__device__ __forceinline__ bool mask_ok(const Geo& g, int a, int y, int n) {
+  if (y == n / 2) return false;
+  int ky = y > n / 2 ? n - y : y;
+  return ky <= __ldg(g.kymax + a);
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void load_twiddles(C2<T>* tw_s, const C2<T>* __restrict__ tw_g) {
+  constexpr int TS = FFTPlan<T, N>::TWSIZE;
+  for (int i = threadIdx.x; i < TS; i += blockDim.x) tw_s[i] = tw_g[i];
+}
+
+template <typename T, int N, int LINES>
+struct Launch {
+  static constexpr int P = FFTPlan<T, N>::P;
+  static constexpr int want = LINES * P;
+  static constexpr int THREADS = want >= 256 ? 256 : (want < 32 ? 32 : want);
+  static_assert(THREADS % P == 0, "threads per line must divide the block");
+};
+
+template <int N> struct LS { static constexpr int value = N + N / 32 + 4; };
+
+// ---------------------------------------------------------------------------
+// K1: phase shift + mask + y backward FFT, transposed store to ub (TB_I block)
+// grid (ceil(xz_tot/TB_I), 3); one block = one ub block of TB_I columns
+// ---------------------------------------------------------------------------
+template <typename T, int N>
+__global__ void __launch_bounds__(Launch<T, N, Tiles<T>::TB_I>::THREADS)
+k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict__ ub,
+       const C2<T>* __restrict__ tw_g) {
+  using C = C2<T>;
+  constexpr int TB = Tiles<T>::TB_I;
+  constexpr int THREADS = Launch<T, N, TB>::THREADS;
+  constexpr int L = LS<N>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* buf = tw + FFTPlan<T, N>::TWSIZE;
+  load_twiddles<T, N>(tw, tw_g);
+  const int at = blockIdx.x, v = blockIdx.y;
+  const int a0 = at * TB;
+  const size_t vs = (size_t)g.xz_tot * N;
+  for (int e = threadIdx.x; e < TB * N; e += THREADS) {
+    const int l = e / N, y = e % N, a = a0 + l;
+    C val = cmk<C>(0, 0);
+    if (a < g.xz_tot && mask_ok(g, a, y, N)) {
+      C sxz = cmul(__ldg(st.sx + __ldg(g.ax + a)), __ldg(st.sz + __ldg(g.az + a)));
+      C sh = cmul(__ldg(st.sy + y), sxz);
+      val = cmul(u[v * vs + (size_t)a * N + y], sh);
+    }
+    buf[l * L + pad32(y)] = cconj(val);
+  }
+  __syncthreads();
+  fft_lines<T, N, THREADS>(buf, TB, L, tw);
+  C* out = ub + ((size_t)v * g.nab_i + at) * N * TB;
+  for (int e = threadIdx.x; e < TB * N; e += THREADS) {
+    const int y = e / TB, l = e % TB;
+    out[e] = cconj(buf[l * L + pad32(y)]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K2: cylinder unpack (zero fill) + z backward FFT, store to uz
+// grid (n, ceil(kxn/XT2), 3)
+// ---------------------------------------------------------------------------
+template <typename T, int N>
+__global__ void __launch_bounds__(Launch<T, N, Tiles<T>::XT2>::THREADS)
+k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g) {
+  using C = C2<T>;
+  constexpr int XT = Tiles<T>::XT2, TB = Tiles<T>::TB_I, TZ = Tiles<T>::TZ;
+  constexpr int THREADS = Launch<T, N, XT>::THREADS;
+  constexpr int L = LS<N>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* buf = tw + FFTPlan<T, N>::TWSIZE;
+  load_twiddles<T, N>(tw, tw_g);
+  const int y = blockIdx.x, x0 = blockIdx.y * XT, v = blockIdx.z;
+  const int x1 = min(x0 + XT, g.kxn);
+  const int nl = x1 - x0;
+  for (int e = threadIdx.x; e < XT * N; e += THREADS) buf[(e / N) * L + pad32(e % N)] = cmk<C>(0, 0);
+  __syncthreads();
+  const int abeg = __ldg(g.colstart + x0), aend = __ldg(g.colstart + x1);
+  const C* src = ub + (size_t)v * g.nab_i * N * TB;
+  for (int a = abeg + threadIdx.x; a < aend; a += THREADS) {
+    const int l = __ldg(g.ax + a) - x0, z = __ldg(g.az + a);
+    C val = src[((size_t)(a / TB) * N + y) * TB + (a % TB)];
+    buf[l * L + pad32(z)] = cconj(val);
+  }
+  __syncthreads();
+  fft_lines<T, N, THREADS>(buf, nl, L, tw);
+  const size_t vbase = ((size_t)v * N + y) * g.nzt;
+  for (int e = threadIdx.x; e < nl * N; e += THREADS) {
+    const int zt = e / (nl * TZ), rem = e % (nl * TZ), l = rem / TZ, zz = rem % TZ;
+    uz[((vbase + zt) * g.kxn + x0 + l) * TZ + zz] = cconj(buf[l * L + pad32(zt * TZ + zz)]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K3: x-line chain.  grid (nzt, n): one block = TZ x-lines (z = zt*TZ + zz)
+// at one y.  Two real lines are carried in one complex FFT (pairs zz=2p,2p+1).
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void atomic_max_pos(unsigned long long* addr, double v) {
+  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void xchain_store(const Geo& g, const C2<T>* buf, int nbuf, int L,
+                                             C2<T>* __restrict__ uz, int slot0, int y, int zt,
+                                             T half_factor) {
+  using C = C2<T>;
+  constexpr int TZ = Tiles<T>::TZ, NPAIR = TZ / 2;
+  const int kxn = g.kxn;
+  for (int e = threadIdx.x; e < nbuf * kxn * NPAIR; e += blockDim.x) {
+    const int b = e / (kxn * NPAIR), rem = e % (kxn * NPAIR), x = rem / NPAIR, p = rem % NPAIR;
+    const C* line = buf + (b * NPAIR + p) * L;
+    const C Y = line[pad32(x)];
+    const C Yn = line[pad32(x == 0 ? 0 : N - x)];
+    const C A = cmk<C>((Y.x + Yn.x) * half_factor, (Y.y - Yn.y) * half_factor);
+    const C B = cmk<C>((Y.y + Yn.y) * half_factor, (Yn.x - Y.x) * half_factor);
+    C* dst = uz + ((((size_t)(slot0 + b) * N + y) * g.nzt + zt) * kxn + x) * TZ + 2 * p;
+    dst[0] = A;
+    dst[1] = B;
+  }
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(Launch<T, N, 2 * Tiles<T>::TZ>::THREADS)
+k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T b22, T b33,
+         unsigned long long* velmax_bits, int want_velmax) {
+  using C = C2<T>;
+  constexpr int TZ = Tiles<T>::TZ, NPAIR = TZ / 2;
+  constexpr int THREADS = Launch<T, N, 2 * TZ>::THREADS;
+  constexpr int L = LS<N>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* bufU = tw + FFTPlan<T, N>::TWSIZE;
+  C* bufV = bufU + NPAIR * L;
+  C* bufW = bufV + NPAIR * L;
+  C* bufE = bufW + NPAIR * L;
+  load_twiddles<T, N>(tw, tw_g);
+  const int zt = blockIdx.x, y = blockIdx.y;
+  const int kxn = g.kxn;
+  // zero the band kx in [kxn, n-kxn] (includes the Nyquist column)
+  const int nz0 = N - 2 * kxn + 1;
+  for (int e = threadIdx.x; e < 3 * NPAIR * nz0; e += THREADS)
+    bufU[(e / nz0) * L + pad32(kxn + e % nz0)] = cmk<C>(0, 0);
+  // pack two real lines per complex line: Z(k) = A(k) + i B(k), with the
+  // Hermitian extension and the imaginary part of the kx=0 term dropped;
+  // stored conjugated (backward transform by conjugation)
+  for (int e = threadIdx.x; e < 3 * kxn * NPAIR; e += THREADS) {
+    const int v = e / (kxn * NPAIR), rem = e % (kxn * NPAIR), x = rem / NPAIR, p = rem % NPAIR;
+    const C* src = uz + ((((size_t)v * N + y) * g.nzt + zt) * kxn + x) * TZ + 2 * p;
+    const C A = src[0], B = src[1];
+    C* line = bufU + (v * NPAIR + p) * L;
+    if (x == 0) {
+      line[pad32(0)] = cmk<C>(A.x, -B.x);
+    } else {
+      line[pad32(x)] = cmk<C>(A.x - B.y, -(A.y + B.x));
+      line[pad32(N - x)] = cmk<C>(A.x + B.y, -(B.x - A.y));
+    }
+  }
+  __syncthreads();
+  fft_lines<T, N, THREADS>(bufU, 3 * NPAIR, L, tw);
+  // buffers now hold conj(a + i b): a = re, b = -im
+  double vm = 0.0;
+  const double xn = (double)b11 * N, yn = (double)b22 * N, zn = (double)b33 * N;
+  for (int e = threadIdx.x; e < NPAIR * N; e += THREADS) {
+    const int i = (e / N) * L + pad32(e % N);
+    const C U = bufU[i], V = bufV[i], W = bufW[i];
+    if (want_velmax) {
+      double va = xn * fabs((double)U.x) + yn * fabs((double)V.x) + zn * fabs((double)W.x);
+      double vb = xn * fabs((double)U.y) + yn * fabs((double)V.y) + zn * fabs((double)W.y);
+      vm = fmax(vm, fmax(va, vb));
+    }
+    bufE[i] = cmk<C>(U.x * W.x, U.y * W.y);   // uw (sign of b cancels in the product)
+  }
+  if (want_velmax) {
+    // block max through warp shuffles then one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) vm = fmax(vm, __shfl_xor_sync(0xffffffffu, vm, o));
+    if ((threadIdx.x & 31) == 0) atomic_max_pos<T>(velmax_bits, vm);
+  }
+  __syncthreads();
+  const T hf = T(0.5) / T(N);
+  fft_lines<T, N, THREADS>(bufE, NPAIR, L, tw);
+  xchain_store<T, N>(g, bufE, 1, L, uz, 4, y, zt, hf);   // slot is2 = 5: u*w
+  __syncthreads();
+  for (int e = threadIdx.x; e < NPAIR * N; e += THREADS) {
+    const int i = (e / N) * L + pad32(e % N);
+    const C V = bufV[i], W = bufW[i];
+    bufE[i] = cmk<C>(V.x * W.x, V.y * W.y);   // vw
+  }
+  __syncthreads();
+  fft_lines<T, N, THREADS>(bufE, NPAIR, L, tw);
+  xchain_store<T, N>(g, bufE, 1, L, uz, 3, y, zt, hf);   // slot is1 = 4: v*w
+  for (int e = threadIdx.x; e < NPAIR * N; e += THREADS) {
+    const int i = (e / N) * L + pad32(e % N);
+    const C U = bufU[i], V = bufV[i], W = bufW[i];
+    const T ua = U.x, ub = -U.y, va = V.x, vb = -V.y, wa = W.x, wb = -W.y;
+    const T bva = b22 * va * va, bvb = b22 * vb * vb;
+    bufW[i] = cmk<C>(b33 * wa * wa - bva, b33 * wb * wb - bvb);
+    bufV[i] = cmk<C>(ua * va, ub * vb);
+    bufU[i] = cmk<C>(b11 * ua * ua - bva, b11 * ub * ub - bvb);
+  }
+  __syncthreads();
+  fft_lines<T, N, THREADS>(bufU, 3 * NPAIR, L, tw);
+  xchain_store<T, N>(g, bufU, 3, L, uz, 0, y, zt, hf);
+}
+
+// ---------------------------------------------------------------------------
+// K4: z forward FFT + derivative combination + cylinder pack into ub (TB_F)
+// grid (n, ceil(kxn/XT4)).  Output slots: 0 = d/dx(u^2-v^2)+d/dz(uw) partial,
+// 1 = uv, 2 = d/dx(uw)+d/dz(w^2-v^2), 3 = vw (y derivatives added in K5).
+// ---------------------------------------------------------------------------
+template <typename T, int N>
+__device__ __forceinline__ void zfwd_load(const Geo& g, const C2<T>* __restrict__ uz, int slot, int y,
+                                          int x0, int nl, C2<T>* buf, int L) {
+  constexpr int TZ = Tiles<T>::TZ;
+  const size_t vbase = ((size_t)slot * N + y) * g.nzt;
+  for (int e = threadIdx.x; e < nl * N; e += blockDim.x) {
+    const int zt = e / (nl * TZ), rem = e % (nl * TZ), l = rem / TZ, zz = rem % TZ;
+    buf[l * L + pad32(zt * TZ + zz)] = uz[((vbase + zt) * g.kxn + x0 + l) * TZ + zz];
+  }
+}
+
+template <typename T, int N, int MODE>
+__device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const C2<T>* s1, int L,
+                                           C2<T>* __restrict__ ub, int slot, int y, int x0, int x1,
+                                           T b11, T b33) {
+  using C = C2<T>;
+  constexpr int TB = Tiles<T>::TB_F;
+  const int abeg = __ldg(g.colstart + x0), aend = __ldg(g.colstart + x1);
+  C* dst = ub + (size_t)slot * g.nab_f * N * TB;
+  for (int a = abeg + threadIdx.x; a < aend; a += blockDim.x) {
+    const int x = __ldg(g.ax + a), z = __ldg(g.az + a), l = x - x0;
+    const int i = l * L + pad32(z);
+    C out;
+    if constexpr (MODE == 0) {          // i kx P1 + i b33 kz P5   (s1 = P1, s0 = P5)
+      const T kx = T(x), bk3 = b33 * T(kwave<N>(z));
+      const C p1 = s1[i], p5 = s0[i];
+      out = cmk<C>(-kx * p1.y - bk3 * p5.y, kx * p1.x + bk3 * p5.x);
+    } else if constexpr (MODE == 1) {   // i b11 kx P5 + i kz P3   (s1 = P3, s0 = P5)
+      const T bk1 = b11 * T(x), kz = T(kwave<N>(z));
+      const C p3 = s1[i], p5 = s0[i];
+      out = cmk<C>(-bk1 * p5.y - kz * p3.y, bk1 * p5.x + kz * p3.x);
+    } else if constexpr (MODE == 2) {
+      out = s0[i];
+    } else {
+      out = s1[i];
+    }
+    dst[((size_t)(a / TB) * N + y) * TB + (a % TB)] = out;
+  }
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(Launch<T, N, 2 * Tiles<T>::XT4>::THREADS)
+k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>* __restrict__ tw_g,
+       T b11, T b33) {
+  using C = C2<T>;
+  constexpr int XT = Tiles<T>::XT4;
+  constexpr int THREADS = Launch<T, N, 2 * XT>::THREADS;
+  constexpr int L = LS<N>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* s0 = tw + FFTPlan<T, N>::TWSIZE;
+  C* s1 = s0 + XT * L;
+  load_twiddles<T, N>(tw, tw_g);
+  const int y = blockIdx.x, x0 = blockIdx.y * XT;
+  const int x1 = min(x0 + XT, g.kxn);
+  const int nl = x1 - x0;
+  // round 1: P5 -> s0, P1 -> s1
+  zfwd_load<T, N>(g, uz, 4, y, x0, nl, s0, L);
+  zfwd_load<T, N>(g, uz, 0, y, x0, nl, s1, L);
+  __syncthreads();
+  if (nl == XT) {
+    fft_lines<T, N, THREADS>(s0, 2 * XT, L, tw);
+  } else {
+    fft_lines<T, N, THREADS>(s0, nl, L, tw);
+    fft_lines<T, N, THREADS>(s1, nl, L, tw);
+  }
+  zfwd_store<T, N, 0>(g, s0, s1, L, ub, 0, y, x0, x1, b11, b33);
+  __syncthreads();
+  // round 2: P3 -> s1
+  zfwd_load<T, N>(g, uz, 2, y, x0, nl, s1, L);
+  __syncthreads();
+  fft_lines<T, N, THREADS>(s1, nl, L, tw);
+  zfwd_store<T, N, 1>(g, s0, s1, L, ub, 2, y, x0, x1, b11, b33);
+  __syncthreads();
+  // round 3: P2 -> s0, P4 -> s1
+  zfwd_load<T, N>(g, uz, 1, y, x0, nl, s0, L);
+  zfwd_load<T, N>(g, uz, 3, y, x0, nl, s1, L);
+  __syncthreads();
+  if (nl == XT) {
+    fft_lines<T, N, THREADS>(s0, 2 * XT, L, tw);
+  } else {
+    fft_lines<T, N, THREADS>(s0, nl, L, tw);
+    fft_lines<T, N, THREADS>(s1, nl, L, tw);
+  }
+  zfwd_store<T, N, 2>(g, s0, s1, L, ub, 1, y, x0, x1, b11, b33);
+  zfwd_store<T, N, 3>(g, s0, s1, L, ub, 3, y, x0, x1, b11, b33);
+}
+
+// ---------------------------------------------------------------------------
+// K5: y forward FFT + wavespace closure + proc4a (kstep 1) / proc4b (kstep 2)
+// grid (nab_f): one block = one ub block of TB_F columns
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void project3(C2<T>& u1, C2<T>& u2, C2<T>& u3, T kx, T ky, T kz,
+                                         T b11, T b22, T b33) {
+  using C = C2<T>;
+  const T bk1 = b11 * kx, bk3 = b33 * kz, bkk3 = bk3 * kz;
+  const T bk12 = bk1 * kx + b22 * (ky * ky);
+  const T den = bk12 + bkk3;
+  const T c2 = b22 * ky;
+  const C s = cmk<C>(bk1 * u1.x + c2 * u2.x + bk3 * u3.x, bk1 * u1.y + c2 * u2.y + bk3 * u3.y);
+  const C psi = cmk<C>(-(s.x / den), -(s.y / den));
+  u1 = cmk<C>(u1.x + kx * psi.x, u1.y + kx * psi.y);
+  u2 = cmk<C>(u2.x + ky * psi.x, u2.y + ky * psi.y);
+  u3 = cmk<C>(u3.x + kz * psi.x, u3.y + kz * psi.y);
+}
+
+template <typename T, int N, int KSTEP>
+__global__ void __launch_bounds__(Launch<T, N, 4 * Tiles<T>::TB_F>::THREADS)
+k_yfwd(Geo g, StageTables<T> st, const C2<T>* __restrict__ ub, C2<T>* __restrict__ u,
+       C2<T>* __restrict__ un, const C2<T>* __restrict__ tw_g, double* __restrict__ efkz) {
+  using C = C2<T>;
+  constexpr int TB = Tiles<T>::TB_F;
+  constexpr int THREADS = Launch<T, N, 4 * TB>::THREADS;
+  constexpr int L = LS<N>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* buf = tw + FFTPlan<T, N>::TWSIZE;   // [4][TB] lines
+  load_twiddles<T, N>(tw, tw_g);
+  const int at = blockIdx.x, a0 = at * TB;
+  for (int v = 0; v < 4; v++) {
+    const C* src = ub + ((size_t)v * g.nab_f + at) * N * TB;
+    for (int e = threadIdx.x; e < TB * N; e += THREADS) {
+      const int y = e / TB, l = e % TB;
+      buf[(v * TB + l) * L + pad32(y)] = src[e];
+    }
+  }
+  __syncthreads();
+  fft_lines<T, N, THREADS>(buf, 4 * TB, L, tw);
+  const size_t vs = (size_t)g.xz_tot * N;
+  for (int e = threadIdx.x; e < TB * N; e += THREADS) {
+    const int l = e / N, y = e % N, a = a0 + l;
+    if (a >= g.xz_tot) continue;
+    const size_t o = (size_t)a * N + y;
+    if (!mask_ok(g, a, y, N)) {
+      u[o] = cmk<C>(0, 0);
+      u[vs + o] = cmk<C>(0, 0);
+      u[2 * vs + o] = cmk<C>(0, 0);
+      continue;
+    }
+    const int x = __ldg(g.ax + a), z = __ldg(g.az + a);
+    const int iky = kwave<N>(y), ikz = kwave<N>(z);
+    const T kx = T(x), ky = T(iky), kz = T(ikz);
+    const int i = pad32(y);
+    const C V1 = buf[(0 * TB + l) * L + i], V2 = buf[(1 * TB + l) * L + i];
+    const C V3 = buf[(2 * TB + l) * L + i], V4 = buf[(3 * TB + l) * L + i];
+    // wavespace_vel.f:165-169
+    const C sxz = cmul(__ldg(st.sz + z), __ldg(st.sx + x));
+    const C s = cconj(cmul(sxz, __ldg(st.sy + y)));
+    const C sxyz = cmk<C>(-st.norm * s.x, -st.norm * s.y);
+    const T tb = st.b22 * ky;
+    const C ut1 = cmk<C>(-tb * sxyz.y, tb * sxyz.x);
+    C w1 = cadd(cmul(sxyz, V1), cmul(ut1, V2));
+    const C si = cmk<C>(-sxyz.y, sxyz.x);
+    const T bk1 = st.b11 * kx, bk3 = st.b33 * kz;
+    C w2 = cmul(si, cmk<C>(bk1 * V2.x + bk3 * V4.x, bk1 * V2.y + bk3 * V4.y));
+    C w3 = cadd(cmul(sxyz, V3), cmul(ut1, V4));
+    const bool k0 = (a == 0 && y == 0);
+    C n1 = un[o], n2 = un[vs + o], n3 = un[2 * vs + o];
+    C u1, u2, u3;
+    if constexpr (KSTEP == 1) {
+      // proc4a.f:427, 479-486
+      const T f = k0 ? T(1) : __ldg(st.xfac + x) * __ldg(st.yfac + y) * __ldg(st.zfac + z);
+      u1 = cscale(f, cmk<C>(n1.x + T(2) * w1.x, n1.y + T(2) * w1.y));
+      u2 = cscale(f, cmk<C>(n2.x + T(2) * w2.x, n2.y + T(2) * w2.y));
+      u3 = cscale(f, cmk<C>(n3.x + T(2) * w3.x, n3.y + T(2) * w3.y));
+      n1 = cscale(f, cadd(n1, w1));
+      n2 = cscale(f, cadd(n2, w2));
+      n3 = cscale(f, cadd(n3, w3));
+    } else {
+      // proc4b.f:54-58
+      u1 = cadd(n1, w1);
+      u2 = cadd(n2, w2);
+      u3 = cadd(n3, w3);
+    }
+    if (!k0) project3<T>(u1, u2, u3, kx, ky, kz, st.b11, st.b22, st.b33);
+    // Eswaran-Pope forcing (proc4a.f:588-651, proc4b.f:118-163)
+    if (st.forc != nullptr && x < st.kfor) {
+      const int kf = st.kfor, k2 = st.k2fo;
+      int izi = (ikz >= 0 && ikz < kf) ? ikz : ((ikz < 0 && ikz > -kf) ? ikz + k2 : -1);
+      int iyi = (iky >= 0 && iky < kf) ? iky : ((iky < 0 && iky > -kf) ? iky + k2 : -1);
+      if (izi >= 0 && iyi >= 0) {
+        bool add = true;
+        double rks = 0.0;
+        if constexpr (KSTEP == 1) {
+          rks = (double)x * x * (double)st.b11 + (double)iky * iky * (double)st.b22 +
+                (double)ikz * ikz * (double)st.b33;
+          add = rks <= st.kforce2;
+        }
+        if (add) {
+          const size_t fo = ((size_t)izi * k2 + iyi) * kf + x;
+          const size_t fs = (size_t)kf * k2 * k2;
+          const C f1 = st.forc[fo], f2 = st.forc[fs + fo], f3 = st.forc[2 * fs + fo];
+          if constexpr (KSTEP == 1) {
+            if (efkz != nullptr) {
+              const int kk = (int)(sqrt(rks) + 1.5);
+              const double tf = (x == 0) ? 1.0 : 2.0;
+              const double e1 = (double)u1.x * f1.x + (double)u1.y * f1.y;
+              const double e2 = (double)u2.x * f2.x + (double)u2.y * f2.y;
+              const double e3 = (double)u3.x * f3.x + (double)u3.y * f3.y;
+              atomicAdd(efkz + (kk - 1) * 3 + 0, 2. * e1 * tf * (double)st.b11);
+              atomicAdd(efkz + (kk - 1) * 3 + 1, 2. * e2 * tf * (double)st.b22);
+              atomicAdd(efkz + (kk - 1) * 3 + 2, 2. * e3 * tf * (double)st.b33);
+            }
+          }
+          u1 = cadd(u1, f1);
+          u2 = cadd(u2, f2);
+          u3 = cadd(u3, f3);
+        }
+      }
+    }
+    if constexpr (KSTEP == 2) {
+      if (k0) {
+        u1 = u2 = u3 = cmk<C>(0, 0);
+      }
+      n1 = u1; n2 = u2; n3 = u3;
+    }
+    u[o] = u1; u[vs + o] = u2; u[2 * vs + o] = u3;
+    un[o] = n1; un[vs + o] = n2; un[2 * vs + o] = n3;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// State conversion (complex double host layout <-> device precision)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_from_f64(const double2* __restrict__ src, C2<T>* __restrict__ dst, C2<T>* __restrict__ dst2,
+                           size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 s = src[i];
+    const C2<T> d = cmk<C2<T>>((T)s.x, (T)s.y);
+    dst[i] = d;
+    if (dst2) dst2[i] = d;
+  }
+}
+
+template <typename T>
+__global__ void k_to_f64(const C2<T>* __restrict__ src, double2* __restrict__ dst, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const C2<T> s = src[i];
+    dst[i] = make_double2((double)s.x, (double)s.y);
+  }
+}
+
+}  // namespace psdns

@@ -1,0 +1,199 @@
+"""Python binding of libpsdns_gpu (the C-ABI declared in include/psdns_gpu.h).
+
+The binding mirrors how the reference's Fortran driver would use the library:
+`Solver(params)` replaces the set-up calls of PSDNS/main.f:160-286,
+`set_state` replaces incond (PSDNS/incond.f), `step` replaces one pass of the
+time loop (`call shifts` + `call timestep`, PSDNS/main.f:409-463) and
+`rk_stage` replaces one `rksubstep` (PSDNS/timestep_module.f:70-481).
+
+The library must be built (build.py) and a CUDA device present; there is no
+CPU fallback: every method raises if the library or the device is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBPATH = os.path.join(_HERE, "libpsdns_gpu.so")
+_LIB = None
+
+PREC_FP32 = 0
+PREC_FP64 = 1
+LAYOUT_YCYL = 0
+FIELD_U = 0
+FIELD_UN = 1
+
+# every entry point declared in include/psdns_gpu.h
+EXPORTS = (
+    "psdns_gpu_default_params",
+    "psdns_gpu_geometry",
+    "psdns_gpu_init",
+    "psdns_gpu_finalize",
+    "psdns_gpu_set_state",
+    "psdns_gpu_get_state",
+    "psdns_gpu_step",
+    "psdns_gpu_rk_stage",
+    "psdns_gpu_get_time",
+    "psdns_gpu_last_error",
+)
+
+
+class Params(ctypes.Structure):
+    """psdns_params of include/psdns_gpu.h."""
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+        ("nc", ctypes.c_int32), ("precision", ctypes.c_int32), ("kshift", ctypes.c_int32),
+        ("ksran", ctypes.c_int32), ("seed_input", ctypes.c_int32),
+        ("kranf1", ctypes.c_int32), ("kranf2", ctypes.c_int32),
+        ("reserved_i", ctypes.c_int32 * 6),
+        ("viscos", ctypes.c_double), ("beta1", ctypes.c_double), ("beta2", ctypes.c_double),
+        ("beta3", ctypes.c_double), ("cfl", ctypes.c_double), ("dt", ctypes.c_double),
+        ("kforce", ctypes.c_double), ("tforce", ctypes.c_double), ("epsfor", ctypes.c_double),
+        ("tfiuo", ctypes.c_double), ("pr", ctypes.c_double), ("grad", ctypes.c_double * 3),
+        ("reserved_d", ctypes.c_double * 8),
+    ]
+
+
+class PsdnsError(RuntimeError):
+    pass
+
+
+def lib_path():
+    return _LIBPATH
+
+
+def load():
+    """Load libpsdns_gpu.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(_LIBPATH):
+        raise PsdnsError(f"{_LIBPATH} is missing: run build.py (there is no CPU fallback)")
+    L = ctypes.CDLL(_LIBPATH)
+    vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)
+    L.psdns_gpu_default_params.argtypes = [ctypes.POINTER(Params)]
+    L.psdns_gpu_geometry.argtypes = [ctypes.c_int32, ip, ip, ip, ip]
+    L.psdns_gpu_init.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p)]
+    L.psdns_gpu_finalize.argtypes = [vp]
+    L.psdns_gpu_set_state.argtypes = [vp, dp, ctypes.c_int32]
+    L.psdns_gpu_get_state.argtypes = [vp, dp, ctypes.c_int32, ctypes.c_int32]
+    L.psdns_gpu_step.argtypes = [vp, dp]
+    L.psdns_gpu_rk_stage.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
+    L.psdns_gpu_get_time.argtypes = [vp, dp]
+    L.psdns_gpu_last_error.argtypes = [ctypes.c_char_p, ctypes.c_int32]
+    for name in EXPORTS:
+        getattr(L, name).restype = ctypes.c_int
+    _LIB = L
+    return L
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(512)
+    load().psdns_gpu_last_error(buf, 512)
+    return buf.value.decode()
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise PsdnsError(f"{what} failed (status {rc}): {last_error()}")
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def default_params(**kw):
+    p = Params()
+    _check(load().psdns_gpu_default_params(ctypes.byref(p)), "psdns_gpu_default_params")
+    for k, v in kw.items():
+        if k == "n":
+            p.nx = p.ny = p.nz = int(v)
+        elif k == "grad":
+            for i in range(3):
+                p.grad[i] = float(v[i])
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def geometry(n):
+    kxn = ctypes.c_int32()
+    tot = ctypes.c_int32()
+    _check(load().psdns_gpu_geometry(n, ctypes.byref(kxn), ctypes.byref(tot), None, None), "geometry")
+    cut = np.zeros(kxn.value, np.int32)
+    col = np.zeros(kxn.value + 1, np.int32)
+    ip = ctypes.POINTER(ctypes.c_int32)
+    _check(load().psdns_gpu_geometry(n, None, None, cut.ctypes.data_as(ip), col.ctypes.data_as(ip)), "geometry")
+    return {"kxn": kxn.value, "xz_tot": tot.value, "cut": cut, "colstart": col}
+
+
+class Solver:
+    """One periodic box advanced on the GPU by the RK2 step of PSDNS."""
+
+    def __init__(self, params=None, **kw):
+        L = load()
+        self.params = params if params is not None else default_params(**kw)
+        self._ctx = ctypes.c_void_p()
+        _check(L.psdns_gpu_init(ctypes.byref(self.params), ctypes.byref(self._ctx)), "psdns_gpu_init")
+        self.n = self.params.nx
+        g = geometry(self.n)
+        self.kxn = g["kxn"]
+        self.xz_tot = g["xz_tot"]
+
+    def close(self):
+        if self._ctx:
+            load().psdns_gpu_finalize(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def state_shape(self):
+        return (3, self.xz_tot, self.n)
+
+    def set_state(self, un):
+        a = np.ascontiguousarray(un, dtype=np.complex128)
+        if a.shape != self.state_shape():
+            raise ValueError(f"state shape {a.shape} != {self.state_shape()}")
+        _check(load().psdns_gpu_set_state(self._ctx, _dp(a.view(np.float64)), LAYOUT_YCYL), "set_state")
+
+    def set_state_ptr(self, ptr):
+        """set_state from a raw host pointer (complex(8) YCYL, e.g. pinned memory)."""
+        _check(load().psdns_gpu_set_state(self._ctx, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)),
+                                          LAYOUT_YCYL), "set_state")
+
+    def get_state(self, which=FIELD_UN, out=None):
+        if out is None:
+            out = np.zeros(self.state_shape(), np.complex128)
+        _check(load().psdns_gpu_get_state(self._ctx, _dp(out.view(np.float64)), which, LAYOUT_YCYL),
+               "get_state")
+        return out
+
+    def get_state_ptr(self, ptr, which=FIELD_UN):
+        _check(load().psdns_gpu_get_state(self._ctx, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)),
+                                          which, LAYOUT_YCYL), "get_state")
+
+    def step(self):
+        info = np.zeros(8, np.float64)
+        rc = load().psdns_gpu_step(self._ctx, _dp(info))
+        if rc not in (0, 2):
+            _check(rc, "psdns_gpu_step")
+        return {"dt": info[0], "time": info[1], "velmax": info[2], "courant": info[3],
+                "gsh1": info[4:7].copy(), "jstep": int(info[7]), "status": rc}
+
+    def rk_stage(self, kstep, gsh, dt=None):
+        g = np.ascontiguousarray(np.asarray(gsh, np.float64).reshape(3, 2).T.reshape(-1))
+        dtv = np.array([dt if dt is not None else 0.0], np.float64)
+        vm = np.zeros(1, np.float64)
+        _check(load().psdns_gpu_rk_stage(self._ctx, int(kstep), _dp(g), _dp(dtv), None, _dp(vm)),
+               "psdns_gpu_rk_stage")
+        return vm[0]
+
+    def time_info(self):
+        out = np.zeros(4, np.float64)
+        _check(load().psdns_gpu_get_time(self._ctx, _dp(out)), "get_time")
+        return {"time": out[0], "dt": out[1], "velmax": out[2], "jstep": int(out[3])}

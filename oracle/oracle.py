@@ -1,0 +1,149 @@
+"""ctypes binding of the CPU FP64 oracle (liboracle.so).
+
+Test infrastructure only: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, as the checker.  The product library never
+imports this module.
+
+The oracle restates the PSDNS RK2 time step (timestep_module.f:70-481 and the
+routines it calls) in FP64 C.  Parity status: unpinned at the FFT boundary
+(the reference's FFTW is not vendored, and the reference ships no golden
+vectors); the oracle FFT is cross-checked against numpy.fft by the tests.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def build():
+    """Compile liboracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+        L.orc_create.restype = vp
+        L.orc_create.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.orc_destroy.argtypes = [vp]
+        L.orc_kxn.argtypes = [vp]
+        L.orc_xz_tot.argtypes = [vp]
+        L.orc_geometry.argtypes = [vp, ip, ip, ip, ip]
+        L.orc_set_state.argtypes = [vp, dp]
+        L.orc_get_state.argtypes = [vp, dp, dp]
+        L.orc_get_scalars.argtypes = [vp, dp]
+        L.orc_step.argtypes = [vp]
+        L.orc_stage.argtypes = [vp, ctypes.c_int]
+        L.orc_set_shifts.argtypes = [vp, dp]
+        L.orc_itransform_only.argtypes = [vp, ctypes.c_int, dp, dp]
+        L.orc_fft.argtypes = [dp, ctypes.c_int, ctypes.c_int]
+        L.orc_field_init.argtypes = [vp, ctypes.c_int, dp]
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_get_threads.restype = ctypes.c_int
+        _LIB = L
+    return _LIB
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def fft(x, sign):
+    """Unnormalised complex FFT of a 1-D array (sign -1 forward, +1 backward)."""
+    a = np.ascontiguousarray(x, dtype=np.complex128).copy()
+    lib().orc_fft(_dp(a.view(np.float64)), a.size, int(sign))
+    return a
+
+
+def set_threads(n):
+    lib().orc_set_threads(int(n))
+
+
+def get_threads():
+    return lib().orc_get_threads()
+
+
+class Oracle:
+    """One periodic box advanced by the FP64 restatement of the RK2 step."""
+
+    def __init__(self, n, viscos, cfl=-1.0, dt=0.005, kshift=1, seed_input=122929298, ksran=1,
+                 beta=(1.0, 1.0, 1.0)):
+        self.n = n
+        self._c = lib().orc_create(n, viscos, cfl, dt, kshift, seed_input, ksran, *beta)
+        self.kxn = lib().orc_kxn(self._c)
+        self.xz_tot = lib().orc_xz_tot(self._c)
+
+    def close(self):
+        if self._c:
+            lib().orc_destroy(self._c)
+            self._c = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def geometry(self):
+        cut = np.zeros(self.kxn, np.int32)
+        col = np.zeros(self.kxn + 1, np.int32)
+        kym = np.zeros(self.xz_tot, np.int32)
+        az = np.zeros(self.xz_tot, np.int32)
+        lib().orc_geometry(self._c, _ip(cut), _ip(col), _ip(kym), _ip(az))
+        return {"cut": cut, "colstart": col, "kymax": kym, "az": az}
+
+    def state_shape(self):
+        return (3, self.xz_tot, self.n)
+
+    def field_init(self, seed):
+        out = np.zeros(self.state_shape(), np.complex128)
+        lib().orc_field_init(self._c, int(seed), _dp(out.view(np.float64)))
+        return out
+
+    def set_state(self, un):
+        a = np.ascontiguousarray(un, dtype=np.complex128)
+        assert a.shape == self.state_shape()
+        lib().orc_set_state(self._c, _dp(a.view(np.float64)))
+
+    def get_state(self):
+        u = np.zeros(self.state_shape(), np.complex128)
+        un = np.zeros(self.state_shape(), np.complex128)
+        lib().orc_get_state(self._c, _dp(u.view(np.float64)), _dp(un.view(np.float64)))
+        return u, un
+
+    def scalars(self):
+        out = np.zeros(11, np.float64)
+        lib().orc_get_scalars(self._c, _dp(out))
+        return {"dt": out[0], "time": out[1], "velmax": out[2], "dt2": out[3],
+                "gsh": out[4:10].reshape(2, 3).T.copy(), "status": int(out[10])}
+
+    def step(self):
+        return lib().orc_step(self._c)
+
+    def set_shifts(self, gsh):
+        g = np.ascontiguousarray(gsh, dtype=np.float64).reshape(3, 2)
+        lib().orc_set_shifts(self._c, _dp(g))
+
+    def stage(self, kstep):
+        return lib().orc_stage(self._c, int(kstep))
+
+    def itransform(self, ucyl, kstep=1):
+        a = np.ascontiguousarray(ucyl, dtype=np.complex128)
+        p = np.zeros((3, self.n, self.n, self.n), np.float64)
+        lib().orc_itransform_only(self._c, int(kstep), _dp(a.view(np.float64)), _dp(p))
+        return p

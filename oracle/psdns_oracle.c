@@ -1,0 +1,856 @@
+/*
+ * psdns_oracle.c -- CPU FP64 restatement of the PSDNS RK2 time step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product library links, loads or
+ * calls this file; only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg use it, as the checker.
+ *
+ * Parity status: UNPINNED at the FFT boundary.  The reference (a Fortran/MPI
+ * code, PSDNS) builds against FFTW 3, which is neither vendored nor pinned in
+ * the reference tree, and the reference ships no golden vectors or known-answer
+ * tests.  The reference cannot be compiled in this container (no Fortran
+ * compiler, MPI or FFTW).  This restatement therefore follows the reference's
+ * arithmetic statement by statement (citations below, paths relative to the
+ * PSDNS project) and uses its own FP64 FFT, which tests cross-check against
+ * numpy.fft.
+ *
+ * Storage follows the reference's own single-rank layout:
+ *   y-cylinders  uy(ny, num_al, nv)   -> here u[v][a][y]   (complex)
+ *   z-pencils    uz(nz, xisz, yjsz)   -> here z[v][y][x][z] (complex, x < kxn)
+ *   x-pencils    ux(nx, zisz, yjsz)   -> here p[v][y][z][x] (real)
+ * where a enumerates the (kx,kz) columns of the cylinder in the order of
+ * next_xz (mpisetup.f:710-732).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef struct { double re, im; } cx;
+
+static inline cx cmul(cx a, cx b) { cx r = {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; return r; }
+static inline cx cadd(cx a, cx b) { cx r = {a.re + b.re, a.im + b.im}; return r; }
+static inline cx csub(cx a, cx b) { cx r = {a.re - b.re, a.im - b.im}; return r; }
+static inline cx cscale(double s, cx a) { cx r = {s * a.re, s * a.im}; return r; }
+static inline cx cconj(cx a) { cx r = {a.re, -a.im}; return r; }
+static inline cx cmk(double re, double im) { cx r = {re, im}; return r; }
+static const cx CZERO = {0.0, 0.0};
+
+/* ------------------------------------------------------------------------ */
+/* Random numbers: ranu.f:22-30 (32-bit multiplicative LCG, multiplier      */
+/* 65539) with the sequence bookkeeping of ranseq.f:58-141 (20 sequences,  */
+/* all seeded with seed_input).                                             */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int32_t iseq[20];
+    int klast;      /* 1-based */
+    int32_t iseed;
+    int ifst;
+    int32_t seed_input;
+} orc_rng;
+
+static void rng_init(orc_rng *r, int32_t seed_input)
+{
+    memset(r, 0, sizeof(*r));
+    r->seed_input = seed_input;
+}
+
+/* ranseq(k,0), ranseq.f:62-141 (k > 0 only) */
+static void rng_ranseq(orc_rng *r, int k)
+{
+    if (r->ifst == 0) {
+        r->ifst = 1;
+        for (int i = 0; i < 20; i++) r->iseq[i] = r->seed_input;
+        r->klast = 1;
+        r->iseed = r->iseq[0];
+    }
+    r->iseq[r->klast - 1] = r->iseed;
+    r->klast = k;
+    r->iseed = r->iseq[k - 1];
+}
+
+/* ranu, ranu.f:27-29: iseed*65539 with 32-bit wrap, folded to >= 0 */
+static double rng_ranu(orc_rng *r)
+{
+    uint32_t s = (uint32_t)r->iseed * 65539u;
+    int32_t is = (int32_t)s;
+    if (is < 0) is = (int32_t)((uint32_t)is + 2147483647u + 1u);
+    r->iseed = is;
+    return (double)is * 0.46566127e-9;
+}
+
+/* ------------------------------------------------------------------------ */
+/* FP64 FFT (own implementation; mixed radix 2/3/5 with a direct-DFT        */
+/* fallback).  Unnormalised, X_k = sum_j x_j exp(sign*2*pi*i*j*k/n).        */
+/* ------------------------------------------------------------------------ */
+typedef struct { int n; cx *w; } fft_tw;   /* w[m] = exp(-2 pi i m / n) */
+
+static void tw_make(fft_tw *t, int n)
+{
+    t->n = n;
+    t->w = (cx *)malloc(sizeof(cx) * (size_t)n);
+    for (int m = 0; m < n; m++) {
+        /* reduce the angle to keep full FP64 accuracy */
+        double ang = -2.0 * M_PI * (double)m / (double)n;
+        t->w[m] = cmk(cos(ang), sin(ang));
+    }
+}
+
+static void fft_rec(cx *x, cx *tmp, int n, int stride_tw, const fft_tw *t)
+{
+    if (n == 1) return;
+    int p = 0;
+    if (n % 4 == 0) p = 4; else if (n % 2 == 0) p = 2; else if (n % 3 == 0) p = 3; else if (n % 5 == 0) p = 5;
+    if (p == 0) { /* direct DFT for other primes */
+        for (int k = 0; k < n; k++) {
+            cx s = CZERO;
+            for (int j = 0; j < n; j++) {
+                long idx = ((long)j * k) % n;
+                s = cadd(s, cmul(x[j], t->w[idx * stride_tw]));
+            }
+            tmp[k] = s;
+        }
+        memcpy(x, tmp, sizeof(cx) * (size_t)n);
+        return;
+    }
+    int m = n / p;
+    /* decimation in time: split into p interleaved subsequences */
+    for (int r = 0; r < p; r++)
+        for (int j = 0; j < m; j++) tmp[r * m + j] = x[j * p + r];
+    for (int r = 0; r < p; r++) fft_rec(tmp + r * m, x + r * m, m, stride_tw * p, t);
+    for (int k = 0; k < m; k++) {
+        cx v[5];
+        for (int r = 0; r < p; r++) {
+            v[r] = tmp[r * m + k];
+            if (r) v[r] = cmul(v[r], t->w[(long)r * k * stride_tw]);
+        }
+        for (int q = 0; q < p; q++) {
+            cx s = CZERO;
+            for (int r = 0; r < p; r++) {
+                long e = ((long)r * q * m) % n;   /* W_p^{rq} = W_n^{rqm} */
+                s = cadd(s, r == 0 ? v[0] : cmul(v[r], t->w[e * stride_tw]));
+            }
+            x[q * m + k] = s;
+        }
+    }
+}
+
+/* forward (sign=-1) or backward (sign=+1) unnormalised complex FFT */
+static void fft_line(cx *x, cx *tmp, int n, int sign, const fft_tw *t)
+{
+    if (sign > 0) for (int j = 0; j < n; j++) x[j].im = -x[j].im;
+    fft_rec(x, tmp, n, 1, t);
+    if (sign > 0) for (int j = 0; j < n; j++) x[j].im = -x[j].im;
+}
+
+void orc_fft(double *x, int n, int sign)
+{
+    fft_tw t; tw_make(&t, n);
+    cx *tmp = (cx *)malloc(sizeof(cx) * (size_t)n);
+    fft_line((cx *)x, tmp, n, sign, &t);
+    free(tmp); free(t.w);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Context                                                                  */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int n, kxn, xz_tot;
+    int *cut;       /* cut_z(x), mpisetup.f:322-332 */
+    int *kc;        /* largest |kz| kept in column x */
+    int *colstart;  /* first a of column x */
+    int *ax, *az;   /* per a: x index (0-based), z index (0-based, 0..n-1) */
+    int *kymax;     /* per a: largest |ky| inside the sphere, masks.f:67-77 */
+    double *kx, *ky, *kz;  /* init.f:15-27 */
+    double b11, b22, b33;  /* init.f:33-37 (beta^2) */
+    double viscos, cfl, dt0, dt, dt2, time, velmax;
+    int kshift, ksran;
+    int nc;
+    orc_rng rng;
+    double gsh[3][2];      /* shifts.f */
+    double gsh4[3][2];     /* gsh(:,3:4) drawn by the RKFOUR-compiled build */
+    int jstep;
+    cx *sx, *sy, *sz;      /* [2][n]: shifts.f:146-178 */
+    double *xfac, *yfac, *zfac;  /* step.f:366-385 */
+    cx *u, *un;            /* [3][xz_tot][n] */
+    fft_tw tw;
+    int status;
+} orc_ctx;
+
+static int mask_ok(const orc_ctx *c, int a, int y)
+{
+    int n = c->n;
+    if (y == n / 2) return 0;
+    double aky = fabs(c->ky[y]);
+    return aky <= (double)c->kymax[a];
+}
+
+/* geometry: init.f:15-29, mpisetup.f:307-357 (cut_z, xz_tot), next_xz
+ * (mpisetup.f:710-732), masks.f:46-83 */
+static void geom_build(orc_ctx *c)
+{
+    int n = c->n;
+    c->kx = (double *)malloc(sizeof(double) * (size_t)(n / 2 + 1));
+    c->ky = (double *)malloc(sizeof(double) * (size_t)n);
+    c->kz = (double *)malloc(sizeof(double) * (size_t)n);
+    for (int x = 0; x <= n / 2; x++) c->kx[x] = x;
+    for (int y = 0; y < n; y++) c->ky[y] = (y > n / 2) ? y - n : y;
+    for (int z = 0; z < n; z++) c->kz[z] = (z > n / 2) ? z - n : z;
+
+    int ikmax = (int)((double)n * sqrt(2.0) / 3.0);
+    int kxn = ikmax + 1;
+    if (kxn > n / 2) kxn = n / 2;
+    c->kxn = kxn;
+    c->cut = (int *)malloc(sizeof(int) * (size_t)kxn);
+    c->kc = (int *)malloc(sizeof(int) * (size_t)kxn);
+    c->colstart = (int *)malloc(sizeof(int) * (size_t)(kxn + 1));
+    double rnxi = 1.0 / n;
+    int tot = 0;
+    for (int x = 0; x < kxn; x++) {
+        double t = c->kx[x] * rnxi;
+        double rc = n * (1.0 - 2.0 * sqrt(2.0 / 9.0 - t * t));
+        int cc = (int)(rc / 2);
+        c->cut[x] = cc;
+        c->kc[x] = n / 2 - 1 - cc;
+        c->colstart[x] = tot;
+        tot += n - 1 - cc * 2;
+    }
+    c->colstart[kxn] = tot;
+    c->xz_tot = tot;
+    c->ax = (int *)malloc(sizeof(int) * (size_t)tot);
+    c->az = (int *)malloc(sizeof(int) * (size_t)tot);
+    c->kymax = (int *)malloc(sizeof(int) * (size_t)tot);
+    double two9 = 2. / 9.;
+    double rnyi = 1. / n, rnzi = 1. / n;
+    for (int x = 0; x < kxn; x++) {
+        int kcx = c->kc[x];
+        for (int i = 0; i < 2 * kcx + 1; i++) {
+            int a = c->colstart[x] + i;
+            int kz = (i <= kcx) ? i : i - (2 * kcx + 1);
+            int z = (kz < 0) ? kz + n : kz;
+            c->ax[a] = x;
+            c->az[a] = z;
+            double sqkx = (c->kx[x] * rnxi) * (c->kx[x] * rnxi);
+            double tz = c->kz[z] * rnzi;
+            double sqkz = tz * tz + sqkx;
+            int km = -1;
+            for (int m = 0; m <= n / 2; m++) {
+                double ty = m * rnyi;
+                double sqk = ty * ty + sqkz;
+                if (sqk > two9) break;
+                km = m;
+            }
+            c->kymax[a] = km;
+        }
+    }
+}
+
+orc_ctx *orc_create(int n, double viscos, double cfl, double dt, int kshift,
+                    int seed_input, int ksran, double beta1, double beta2, double beta3)
+{
+    orc_ctx *c = (orc_ctx *)calloc(1, sizeof(orc_ctx));
+    c->n = n;
+    c->viscos = viscos; c->cfl = cfl; c->dt0 = dt; c->dt = dt;
+    c->kshift = kshift; c->ksran = ksran;
+    c->b11 = beta1 * beta1; c->b22 = beta2 * beta2; c->b33 = beta3 * beta3;
+    rng_init(&c->rng, seed_input);
+    geom_build(c);
+    size_t nst = (size_t)3 * c->xz_tot * n;
+    c->u = (cx *)calloc(nst, sizeof(cx));
+    c->un = (cx *)calloc(nst, sizeof(cx));
+    c->sx = (cx *)calloc((size_t)2 * n, sizeof(cx));
+    c->sy = (cx *)calloc((size_t)2 * n, sizeof(cx));
+    c->sz = (cx *)calloc((size_t)2 * n, sizeof(cx));
+    c->xfac = (double *)calloc((size_t)n, sizeof(double));
+    c->yfac = (double *)calloc((size_t)n, sizeof(double));
+    c->zfac = (double *)calloc((size_t)n, sizeof(double));
+    tw_make(&c->tw, n);
+    return c;
+}
+
+void orc_destroy(orc_ctx *c)
+{
+    if (!c) return;
+    free(c->kx); free(c->ky); free(c->kz); free(c->cut); free(c->kc); free(c->colstart);
+    free(c->ax); free(c->az); free(c->kymax); free(c->u); free(c->un);
+    free(c->sx); free(c->sy); free(c->sz); free(c->xfac); free(c->yfac); free(c->zfac);
+    free(c->tw.w);
+    free(c);
+}
+
+int orc_kxn(orc_ctx *c) { return c->kxn; }
+int orc_xz_tot(orc_ctx *c) { return c->xz_tot; }
+void orc_geometry(orc_ctx *c, int *cut, int *colstart, int *kymax, int *az)
+{
+    memcpy(cut, c->cut, sizeof(int) * (size_t)c->kxn);
+    memcpy(colstart, c->colstart, sizeof(int) * (size_t)(c->kxn + 1));
+    memcpy(kymax, c->kymax, sizeof(int) * (size_t)c->xz_tot);
+    memcpy(az, c->az, sizeof(int) * (size_t)c->xz_tot);
+}
+
+/* state I/O: [3][xz_tot][n] complex (re,im interleaved), the reference's
+ * uy(ny,num_al,3) layout.  set_state copies un into both un and u
+ * (incond.f:146). */
+void orc_set_state(orc_ctx *c, const double *un)
+{
+    size_t nst = (size_t)3 * c->xz_tot * c->n;
+    memcpy(c->un, un, nst * sizeof(cx));
+    memcpy(c->u, un, nst * sizeof(cx));
+}
+
+void orc_get_state(orc_ctx *c, double *u, double *un)
+{
+    size_t nst = (size_t)3 * c->xz_tot * c->n;
+    if (u) memcpy(u, c->u, nst * sizeof(cx));
+    if (un) memcpy(un, c->un, nst * sizeof(cx));
+}
+
+void orc_get_scalars(orc_ctx *c, double *out)
+{
+    out[0] = c->dt; out[1] = c->time; out[2] = c->velmax; out[3] = c->dt2;
+    out[4] = c->gsh[0][0]; out[5] = c->gsh[1][0]; out[6] = c->gsh[2][0];
+    out[7] = c->gsh[0][1]; out[8] = c->gsh[1][1]; out[9] = c->gsh[2][1];
+    out[10] = (double)c->status;
+}
+
+/* ------------------------------------------------------------------------ */
+/* shifts.f:40-178 (kshift 1..4) as compiled with -DRKFOUR (the makefile's  */
+/* configuration), which also draws gsh(:,3:4) each step.                   */
+/* ------------------------------------------------------------------------ */
+static double cancel(double d) { return fmod(d + 0.5, 1.); }
+
+static void shifts(orc_ctx *c)
+{
+    int n = c->n;
+    int ks = c->kshift;
+    if (c->jstep == 1 && (ks == 1 || ks == 3)) {
+        rng_ranseq(&c->rng, c->ksran);
+        for (int i = 0; i < 3; i++) c->gsh[i][1] = rng_ranu(&c->rng);
+        for (int i = 0; i < 3; i++) c->gsh4[i][1] = rng_ranu(&c->rng);
+    }
+    if (ks == 1 || ks == 2) rng_ranseq(&c->rng, c->ksran);
+    for (int i = 0; i < 3; i++) {
+        if (ks == 1) { c->gsh[i][0] = cancel(c->gsh[i][1]); c->gsh[i][1] = rng_ranu(&c->rng); }
+        else if (ks == 2) { c->gsh[i][0] = rng_ranu(&c->rng); c->gsh[i][1] = cancel(c->gsh[i][0]); }
+        else if (ks == 3) { c->gsh[i][0] = cancel(c->gsh[i][1]); c->gsh[i][1] = cancel(c->gsh[i][0]); }
+        else { c->gsh[i][0] = 0.; c->gsh[i][1] = 0.; }
+    }
+    for (int i = 0; i < 3; i++) {
+        if (ks == 1) { c->gsh4[i][0] = cancel(c->gsh4[i][1]); c->gsh4[i][1] = rng_ranu(&c->rng); }
+        else if (ks == 2) { c->gsh4[i][0] = rng_ranu(&c->rng); c->gsh4[i][1] = cancel(c->gsh4[i][0]); }
+        else if (ks == 3) { c->gsh4[i][0] = cancel(c->gsh4[i][1]); c->gsh4[i][1] = cancel(c->gsh4[i][0]); }
+        else { c->gsh4[i][0] = 0.; c->gsh4[i][1] = 0.; }
+    }
+    double pi = 4. * atan(1.);
+    double ph = 2. * pi / n;
+    for (int k = 0; k < 2; k++) {
+        for (int x = 0; x <= n / 2 && x < n; x++) {
+            double th = (ph * c->kx[x]) * c->gsh[0][k];
+            c->sx[k * n + x] = cmk(cos(th), sin(th));
+        }
+        for (int y = 0; y < n; y++) {
+            double th = (ph * c->ky[y]) * c->gsh[1][k];
+            c->sy[k * n + y] = cmk(cos(th), sin(th));
+        }
+        for (int z = 0; z < n; z++) {
+            double th = (ph * c->kz[z]) * c->gsh[2][k];
+            c->sz[k * n + z] = cmk(cos(th), sin(th));
+        }
+    }
+}
+
+/* Externally supplied grid shifts (for tests that drive stages directly). */
+void orc_set_shifts(orc_ctx *c, const double *gsh /* [3][2] */)
+{
+    int n = c->n;
+    for (int i = 0; i < 3; i++) { c->gsh[i][0] = gsh[2 * i]; c->gsh[i][1] = gsh[2 * i + 1]; }
+    double pi = 4. * atan(1.);
+    double ph = 2. * pi / n;
+    for (int k = 0; k < 2; k++) {
+        for (int x = 0; x <= n / 2 && x < n; x++) {
+            double th = (ph * c->kx[x]) * c->gsh[0][k];
+            c->sx[k * n + x] = cmk(cos(th), sin(th));
+        }
+        for (int y = 0; y < n; y++) {
+            double th = (ph * c->ky[y]) * c->gsh[1][k];
+            c->sy[k * n + y] = cmk(cos(th), sin(th));
+        }
+        for (int z = 0; z < n; z++) {
+            double th = (ph * c->kz[z]) * c->gsh[2][k];
+            c->sz[k * n + z] = cmk(cos(th), sin(th));
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Stage pieces                                                             */
+/* ------------------------------------------------------------------------ */
+
+/* phshift_inplace (phshift.f:71-135): uy *= sy(y)*(sx(x)*sz(z)); masked -> 0 */
+static void phase_shift(orc_ctx *c, cx *u, int nv, int ks)
+{
+    int n = c->n;
+    #pragma omp parallel for schedule(static)
+    for (int a = 0; a < c->xz_tot; a++) {
+        cx sxz = cmul(c->sx[ks * n + c->ax[a]], c->sz[ks * n + c->az[a]]);
+        for (int y = 0; y < n; y++) {
+            if (mask_ok(c, a, y)) {
+                cx sh = cmul(c->sy[ks * n + y], sxz);
+                for (int v = 0; v < nv; v++) {
+                    cx *p = &u[((size_t)v * c->xz_tot + a) * n + y];
+                    *p = cmul(*p, sh);
+                }
+            } else {
+                for (int v = 0; v < nv; v++) u[((size_t)v * c->xz_tot + a) * n + y] = CZERO;
+            }
+        }
+    }
+}
+
+/* itransform_vel.f:11-129 with kxcomm1_clean.f (y backward FFT, scatter to z
+ * pencils with zero fill of the cut band, :205-255), the z backward FFT with
+ * the Nyquist row zeroed (itransform_vel.f:80-94) and kxcomm2.f (x backward
+ * complex-to-real, kx >= kxn zero padded, :308-321).
+ * in: u[v][a][y] (overwritten: y transformed), out: p[v][y][z][x] real. */
+static void itransform(orc_ctx *c, cx *u, int nv, double *p)
+{
+    int n = c->n, kxn = c->kxn, tot = c->xz_tot;
+    /* y backward */
+    #pragma omp parallel
+    {
+        cx *tmp = (cx *)malloc(sizeof(cx) * (size_t)n);
+        #pragma omp for schedule(static)
+        for (long l = 0; l < (long)nv * tot; l++) fft_line(u + l * n, tmp, n, +1, &c->tw);
+        free(tmp);
+    }
+    /* z pencils: zl[v][y][x][z] */
+    cx *zl = (cx *)calloc((size_t)nv * n * kxn * n, sizeof(cx));
+    #pragma omp parallel
+    {
+        cx *tmp = (cx *)malloc(sizeof(cx) * (size_t)n);
+        #pragma omp for schedule(static) collapse(2)
+        for (int v = 0; v < nv; v++)
+            for (int y = 0; y < n; y++)
+                for (int x = 0; x < kxn; x++) {
+                    cx *line = zl + (((size_t)v * n + y) * kxn + x) * n;
+                    for (int a = c->colstart[x]; a < c->colstart[x + 1]; a++)
+                        line[c->az[a]] = u[((size_t)v * tot + a) * n + y];
+                    line[n / 2] = CZERO;
+                    fft_line(line, tmp, n, +1, &c->tw);
+                }
+        free(tmp);
+    }
+    /* x complex-to-real: Hermitian extension; imaginary part of the kx=0
+     * term ignored, as a c2r transform does */
+    #pragma omp parallel
+    {
+        cx *line = (cx *)malloc(sizeof(cx) * (size_t)n);
+        cx *tmp = (cx *)malloc(sizeof(cx) * (size_t)n);
+        #pragma omp for schedule(static) collapse(2)
+        for (int v = 0; v < nv; v++)
+            for (int y = 0; y < n; y++)
+                for (int z = 0; z < n; z++) {
+                    for (int k = 0; k < n; k++) line[k] = CZERO;
+                    for (int x = 0; x < kxn; x++) {
+                        cx val = zl[(((size_t)v * n + y) * kxn + x) * n + z];
+                        if (x == 0) { line[0] = cmk(val.re, 0.0); }
+                        else { line[x] = val; line[n - x] = cconj(val); }
+                    }
+                    fft_line(line, tmp, n, +1, &c->tw);
+                    double *out = p + (((size_t)v * n + y) * n + z) * n;
+                    for (int x = 0; x < n; x++) out[x] = line[x].re;
+                }
+        free(line); free(tmp);
+    }
+    free(zl);
+}
+
+/* realspace_vel.f:61-118 (stage 1, with velmax) and :143-178 (stage 2).
+ * in: p[0..2] = u,v,w ; out: p[0..4] = b11 u^2 - bv2, uv, b33 w^2 - bv2, vw, uw */
+static double realspace(orc_ctx *c, double *p, int want_velmax)
+{
+    int n = c->n;
+    size_t np = (size_t)n * n * n;
+    double xnorm = c->b11 * n, ynorm = c->b22 * n, znorm = c->b33 * n;
+    double vm = 0.;
+    #pragma omp parallel for reduction(max:vm) schedule(static)
+    for (long i = 0; i < (long)np; i++) {
+        double u = p[i], v = p[np + i], w = p[2 * np + i];
+        double bv2 = c->b22 * v * v;
+        p[4 * np + i] = u * w;
+        p[3 * np + i] = v * w;
+        if (want_velmax) {
+            double vel = xnorm * fabs(u) + ynorm * fabs(v) + znorm * fabs(w);
+            if (vel > vm) vm = vel;
+        }
+        p[2 * np + i] = c->b33 * w * w - bv2;
+        p[np + i] = u * v;
+        p[i] = c->b11 * u * u - bv2;
+    }
+    return vm;
+}
+
+/* transform.f:10-301: x forward real-to-complex times 1/nx (xkcomm1.f:97,135),
+ * z forward FFT (transform.f:129-138), derivative combination
+ * (transform.f:230-234, Nyquist z row skipped), cylinder gather keeping
+ * |kz| <= kc(x) (xkcomm2.f:96-125) and y forward FFT (xkcomm2.f:229).
+ * in: p[5][y][z][x] ; out: u[4][a][y] */
+static void transform(orc_ctx *c, const double *p, cx *u)
+{
+    int n = c->n, kxn = c->kxn, tot = c->xz_tot;
+    double factor = 1. / (double)n;
+    cx *zl = (cx *)calloc((size_t)5 * n * kxn * n, sizeof(cx));
+    /* x r2c, scale, transpose to z pencils zl[v][y][x][z] */
+    #pragma omp parallel
+    {
+        cx *line = (cx *)malloc(sizeof(cx) * (size_t)n);
+        cx *tmp = (cx *)malloc(sizeof(cx) * (size_t)n);
+        #pragma omp for schedule(static) collapse(2)
+        for (int v = 0; v < 5; v++)
+            for (int y = 0; y < n; y++)
+                for (int z = 0; z < n; z++) {
+                    const double *in = p + (((size_t)v * n + y) * n + z) * n;
+                    for (int x = 0; x < n; x++) line[x] = cmk(in[x], 0.0);
+                    fft_line(line, tmp, n, -1, &c->tw);
+                    for (int x = 0; x < kxn; x++)
+                        zl[(((size_t)v * n + y) * kxn + x) * n + z] = cscale(factor, line[x]);
+                }
+        free(line); free(tmp);
+    }
+    /* z forward */
+    #pragma omp parallel
+    {
+        cx *tmp = (cx *)malloc(sizeof(cx) * (size_t)n);
+        #pragma omp for schedule(static)
+        for (long l = 0; l < (long)5 * n * kxn; l++) fft_line(zl + l * n, tmp, n, -1, &c->tw);
+        free(tmp);
+    }
+    /* derivative combination, m = 2 mesh (b11(2) = b11 etc.) */
+    size_t vs = (size_t)n * kxn * n;
+    #pragma omp parallel for schedule(static) collapse(2)
+    for (int y = 0; y < n; y++)
+        for (int x = 0; x < kxn; x++) {
+            cx bk1i1 = cmk(0.0, c->kx[x]);
+            cx bk1i2 = cmk(0.0, c->b11 * c->kx[x]);
+            for (int z = 0; z < n; z++) {
+                if (z == n / 2) continue;
+                cx bk3i1 = cmk(0.0, c->b33 * c->kz[z]);
+                cx bk3i2 = cmk(0.0, c->kz[z]);
+                size_t o = ((size_t)y * kxn + x) * n + z;
+                cx u1 = zl[o], u3 = zl[2 * vs + o], u5 = zl[4 * vs + o];
+                zl[o] = cadd(cmul(bk1i1, u1), cmul(bk3i1, u5));
+                zl[2 * vs + o] = cadd(cmul(bk1i2, u5), cmul(bk3i2, u3));
+            }
+        }
+    /* cylinder gather (4 variables: slots 1,2,3,4) and y forward */
+    #pragma omp parallel
+    {
+        cx *tmp = (cx *)malloc(sizeof(cx) * (size_t)n);
+        #pragma omp for schedule(static) collapse(2)
+        for (int v = 0; v < 4; v++)
+            for (int a = 0; a < tot; a++) {
+                cx *line = u + ((size_t)v * tot + a) * n;
+                int x = c->ax[a], z = c->az[a];
+                for (int y = 0; y < n; y++) line[y] = zl[(((size_t)v * n + y) * kxn + x) * n + z];
+                fft_line(line, tmp, n, -1, &c->tw);
+            }
+        free(tmp);
+    }
+    free(zl);
+}
+
+/* step.f:49-99 (dt from CFL), :247-262 (time, dt2), :366-385 (integrating
+ * factors; a11=a22=a33=0 so term = b(1)*dt).  Returns nonzero on the abort
+ * conditions of step.f:79-84, :280-283, :289-295. */
+static int step_control(orc_ctx *c)
+{
+    int n = c->n;
+    c->dt = c->dt0;
+    int err = 0;
+    if (c->cfl > 0.) {
+        c->dt = c->cfl / c->velmax;
+        if (c->velmax < .001) err = 1;
+    }
+    c->time = c->time + c->dt;
+    if (c->dt == 0.) err = 2;
+    c->dt2 = c->dt / 2.;
+    if (c->cfl > 0.) {
+        if (c->dt > 10. || c->dt < 1.e-7) err = 3;
+    } else if (c->cfl < 0.) {
+        double cn = c->velmax * c->dt / 2. / (4. * atan(1.));
+        if (cn > 1) err = 4;
+    }
+    double term = c->b11 * c->dt;
+    for (int x = 0; x <= n / 2 && x < n; x++) c->xfac[x] = exp(-(c->viscos * (c->kx[x] * c->kx[x]) * term));
+    term = c->b22 * c->dt;
+    for (int y = 0; y < n; y++) c->yfac[y] = exp(-(c->viscos * (c->ky[y] * c->ky[y]) * term));
+    term = c->b33 * c->dt;
+    for (int z = 0; z < n; z++) c->zfac[z] = exp(-(c->viscos * (c->kz[z] * c->kz[z]) * term));
+    return err;
+}
+
+/* wavespace_vel.f:80,163-174: un-shift and finish the y derivatives.
+ * in: w[4][a][y]; out: w[0..2] = (dt/2) N(u) */
+static void wavespace(orc_ctx *c, cx *w, int ks)
+{
+    int n = c->n, tot = c->xz_tot;
+    double norm = c->dt2 / n / n;
+    #pragma omp parallel for schedule(static)
+    for (int a = 0; a < tot; a++) {
+        int x = c->ax[a], z = c->az[a];
+        cx sxz = cmul(c->sz[ks * n + z], c->sx[ks * n + x]);
+        double bk1 = c->b11 * c->kx[x], bk3 = c->b33 * c->kz[z];
+        for (int y = 0; y < n; y++) {
+            size_t o = (size_t)a * n + y;
+            size_t vs = (size_t)tot * n;
+            if (mask_ok(c, a, y)) {
+                cx s = cconj(cmul(sxz, c->sy[ks * n + y]));
+                cx sxyz = cscale(-norm, s);
+                cx ib = cmk(0.0, c->b22);
+                ib = cscale(c->ky[y], ib);
+                cx utmp1 = cmul(ib, sxyz);
+                cx u1 = w[o], u2 = w[vs + o], u3 = w[2 * vs + o], u4 = w[3 * vs + o];
+                w[o] = cadd(cmul(sxyz, u1), cmul(utmp1, u2));
+                cx si = cmul(sxyz, cmk(0.0, 1.0));
+                w[vs + o] = cmul(si, cadd(cscale(bk1, u2), cscale(bk3, u4)));
+                w[2 * vs + o] = cadd(cmul(sxyz, u3), cmul(utmp1, u4));
+            } else {
+                w[o] = CZERO; w[vs + o] = CZERO; w[2 * vs + o] = CZERO; w[3 * vs + o] = CZERO;
+            }
+        }
+    }
+}
+
+/* pressure projection shared by proc4a.f:553-571 and proc4b.f:85-106 */
+static void project(orc_ctx *c, cx *u, int a, int y)
+{
+    int n = c->n, tot = c->xz_tot;
+    int x = c->ax[a], z = c->az[a];
+    size_t o = (size_t)a * n + y, vs = (size_t)tot * n;
+    double bk1 = c->b11 * c->kx[x];
+    double bk3 = c->b33 * c->kz[z];
+    double bkk3 = bk3 * c->kz[z];
+    double bk12 = bk1 * c->kx[x] + c->b22 * (c->ky[y] * c->ky[y]);
+    double den = bk12 + bkk3;
+    cx s = cadd(cadd(cscale(bk1, u[o]), cscale(c->b22 * c->ky[y], u[vs + o])), cscale(bk3, u[2 * vs + o]));
+    cx psi = cmk(-(s.re / den), -(s.im / den));
+    u[o] = cadd(u[o], cscale(c->kx[x], psi));
+    u[vs + o] = cadd(u[vs + o], cscale(c->ky[y], psi));
+    u[2 * vs + o] = cadd(u[2 * vs + o], cscale(c->kz[z], psi));
+}
+
+/* proc4a.f:418-486 (integrating factor, predictor) and :535-573 (projection).
+ * The mean mode (k=0) uses factor 1: the reference multiplies it by an
+ * unset element of facty, but both terms of that product are zero there. */
+static void proc4a(orc_ctx *c, cx *w, cx *un)
+{
+    int n = c->n, tot = c->xz_tot;
+    size_t vs = (size_t)tot * n;
+    #pragma omp parallel for schedule(static)
+    for (int a = 0; a < tot; a++) {
+        int x = c->ax[a], z = c->az[a];
+        for (int y = 0; y < n; y++) {
+            if (!mask_ok(c, a, y)) continue;
+            double f = (a == 0 && y == 0) ? 1.0 : c->xfac[x] * c->yfac[y] * c->zfac[z];
+            for (int i = 0; i < 3; i++) {
+                size_t o = i * vs + (size_t)a * n + y;
+                cx untemp = un[o];
+                un[o] = cscale(f, cadd(untemp, w[o]));
+                w[o] = cscale(f, cadd(untemp, cscale(2., w[o])));
+            }
+            if (a == 0 && y == 0) continue;
+            project(c, w, a, y);
+        }
+    }
+}
+
+/* proc4b.f:38-106 (corrector and projection), :183-191 (copy), :200-205
+ * (zero mean) */
+static void proc4b(orc_ctx *c, cx *w, cx *un)
+{
+    int n = c->n, tot = c->xz_tot;
+    size_t vs = (size_t)tot * n;
+    #pragma omp parallel for schedule(static)
+    for (int a = 0; a < tot; a++) {
+        for (int y = 0; y < n; y++) {
+            if (!mask_ok(c, a, y)) continue;
+            for (int i = 0; i < 3; i++) {
+                size_t o = i * vs + (size_t)a * n + y;
+                w[o] = cadd(un[o], w[o]);
+            }
+            if (a == 0 && y == 0) continue;
+            project(c, w, a, y);
+        }
+        for (int y = 0; y < n; y++) {
+            if (!mask_ok(c, a, y)) continue;
+            for (int i = 0; i < 3; i++) {
+                size_t o = i * vs + (size_t)a * n + y;
+                un[o] = w[o];
+            }
+        }
+    }
+    for (int i = 0; i < 3; i++) { w[i * vs] = CZERO; un[i * vs] = CZERO; }
+}
+
+/* One RK stage (timestep_module.f:70-481, CLEAN velocity path, nc = 0).
+ * The work array holds u (3 vars) on entry and the nonlinear slots (4 vars)
+ * after the forward transform; u keeps the result. */
+static int rk_stage(orc_ctx *c, int kstep)
+{
+    int n = c->n, tot = c->xz_tot;
+    int ks = kstep - 1;
+    size_t vs = (size_t)tot * n;
+    size_t np = (size_t)n * n * n;
+    phase_shift(c, c->u, 3, ks);
+    cx *w = (cx *)malloc(sizeof(cx) * 4 * vs);
+    memcpy(w, c->u, sizeof(cx) * 3 * vs);
+    double *p = (double *)malloc(sizeof(double) * 5 * np);
+    itransform(c, w, 3, p);
+    double vm = realspace(c, p, kstep == 1);
+    if (kstep == 1) c->velmax = vm;
+    transform(c, p, w);
+    free(p);
+    int err = 0;
+    if (kstep == 1) err = step_control(c);
+    wavespace(c, w, ks);
+    if (kstep == 1) proc4a(c, w, c->un);
+    else proc4b(c, w, c->un);
+    memcpy(c->u, w, sizeof(cx) * 3 * vs);
+    free(w);
+    return err;
+}
+
+/* One full RK2 step (main.f:392-463: shifts, then timestep).  Returns the
+ * step_control status (0 = ok). */
+int orc_step(orc_ctx *c)
+{
+    c->jstep += 1;
+    shifts(c);
+    int e1 = rk_stage(c, 1);
+    int e2 = rk_stage(c, 2);
+    c->status = e1 ? e1 : e2;
+    return c->status;
+}
+
+/* Stage driven with caller-provided shifts (for piecewise tests). */
+int orc_stage(orc_ctx *c, int kstep)
+{
+    return rk_stage(c, kstep);
+}
+
+/* Piecewise hooks for tests: the inverse transform of u (3 vars) into
+ * physical space p[3][y][z][x] (after the phase shift of stage kstep). */
+void orc_itransform_only(orc_ctx *c, int kstep, const double *ucyl, double *p)
+{
+    size_t vs = (size_t)c->xz_tot * c->n;
+    cx *w = (cx *)malloc(sizeof(cx) * 3 * vs);
+    memcpy(w, ucyl, sizeof(cx) * 3 * vs);
+    phase_shift(c, w, 3, kstep - 1);
+    itransform(c, w, 3, p);
+    free(w);
+}
+
+void orc_set_threads(int nt)
+{
+#ifdef _OPENMP
+    omp_set_num_threads(nt);
+#else
+    (void)nt;
+#endif
+}
+
+int orc_get_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* ------------------------------------------------------------------------ */
+/* Initial field: homogeneous/field.f:169-257 (random solenoidal field, the  */
+/* branch that draws its phases from ranu) followed by the conjugate        */
+/* symmetry of homogeneous/consym.f:35-73 (FRESH, single task).  The        */
+/* spectrum is E(k) = c0 k^4 exp(-2 (k/3)^2), c0 = 4/(sqrt(pi) 4.5^2.5), so */
+/* that the continuous integral of E is 3/2 (u' = 1).                       */
+/* ------------------------------------------------------------------------ */
+static double espec(double k)
+{
+    double c0 = 4.0 / (sqrt(M_PI) * pow(4.5, 2.5));
+    double q = k / 3.0;
+    return c0 * k * k * k * k * exp(-2.0 * q * q);
+}
+
+void orc_field_init(orc_ctx *c, int seed, double *out /* [3][xz_tot][n] complex */)
+{
+    int n = c->n, tot = c->xz_tot;
+    size_t vs = (size_t)tot * n;
+    cx *u = (cx *)out;
+    memset(u, 0, sizeof(cx) * 3 * vs);
+    orc_rng r; rng_init(&r, seed); rng_ranseq(&r, 1);
+    double pi = 4. * atan(1.);
+    double voljac = 1.0 * 1.0 * 1.0;   /* beta1*beta2*beta3 with unit box */
+    double twopi = 2. * pi;
+    double rpid = 1. / sqrt(twopi);
+    double s1 = sqrt(c->b11), s2 = sqrt(c->b22), s3 = sqrt(c->b33);
+    voljac = s1 * s2 * s3;
+    double s1d = 1. / s1, s2d = 1. / s2, s3d = 1. / s3;
+    for (int a = 0; a < tot; a++) {
+        int x = c->ax[a], z = c->az[a];
+        double k1u = s1 * c->kx[x];
+        double k3u = s3 * c->kz[z];
+        int yst = (a == 0) ? 1 : 0;
+        for (int y = yst; y < n; y++) {
+            if (!mask_ok(c, a, y)) continue;
+            double k2u = s2 * c->ky[y];
+            double kyzsq = k2u * k2u + k3u * k3u;
+            double k = sqrt(k1u * k1u + kyzsq);
+            double kd = 1. / k;
+            double ekx = espec(k) * voljac;
+            double ef = sqrt(ekx) * rpid * kd;
+            double theta1 = rng_ranu(&r);
+            double theta2 = rng_ranu(&r);
+            double phi = rng_ranu(&r);
+            double k12 = sqrt(k1u * k1u + k2u * k2u);
+            double angphi = twopi * phi;
+            double t1 = twopi * theta1, t2 = twopi * theta2;
+            cx e1 = cmk(cos(t1), sin(t1)), e2 = cmk(cos(t2), sin(t2));
+            cx alpha = cscale(cos(angphi), cscale(ef, e1));
+            cx beta = cscale(sin(angphi), cscale(ef, e2));
+            size_t o = (size_t)a * n + y;
+            if (k12 == 0.) {
+                u[o] = cscale(1.0 / s1, alpha);
+                u[o] = cmk(alpha.re / s1, alpha.im / s1);
+                u[vs + o] = cmk(beta.re / s2, beta.im / s2);
+                u[2 * vs + o] = CZERO;
+            } else {
+                cx ctmp1 = cscale(k, alpha);
+                cx ctmp2 = cscale(k3u, beta);
+                double rtmp = kd / k12;
+                u[o] = cscale(s1d, cscale(rtmp, cadd(cscale(k2u, ctmp1), cscale(k1u, ctmp2))));
+                u[vs + o] = cscale(s2d, cscale(rtmp, csub(cscale(k2u, ctmp2), cscale(k1u, ctmp1))));
+                cx b3 = cscale(s3d, cscale(kd, cscale(k12, beta)));
+                u[2 * vs + o] = cmk(-b3.re, -b3.im);
+            }
+        }
+    }
+    for (int i = 0; i < 3; i++) u[i * vs] = CZERO;
+    /* consym (FRESH): kx = 0 plane */
+    int kc0 = c->kc[0];
+    for (int i = 0; i < 3; i++) {
+        cx *ui = u + i * vs;
+        ui[0] = cmk(ui[0].re, 0.);
+        for (int y = n / 2 + 1; y < n; y++) ui[y] = cconj(ui[n - y]);
+        for (int j = kc0 + 1; j < 2 * kc0 + 1; j++) {
+            /* column j holds kz = j - (2 kc0 + 1) < 0; its mirror holds -kz */
+            int kz = j - (2 * kc0 + 1);
+            int jo = -kz;
+            ui[(size_t)j * n + 0] = cconj(ui[(size_t)jo * n + 0]);
+            for (int y = 1; y < n; y++) ui[(size_t)j * n + y] = cconj(ui[(size_t)jo * n + (n - y)]);
+        }
+    }
+}

@@ -1,0 +1,116 @@
+"""GPU parity: the sm_100a RK2 step against the FP64 oracle, through the
+C-ABI (psdns_gpu.Solver).
+
+Tolerances (relative L2 over the whole state, and per E(k) shell):
+  FP64 device state: 1e-11 (both sides are FP64; differences are FFT
+                     rounding order only)
+  FP32 device state: 2e-5 after 5 steps (FP32 FFTs, ~1e-7 per operation)
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def shell_spectrum(un, geo, n):
+    """E(k) per shell, ik = int(k + 1.5) (sptr.f:161-165), kx=0 plane once."""
+    col = geo["colstart"]
+    kk = lambda i: np.where(i > n // 2, i - n, i)
+    ky = kk(np.arange(n))
+    E = np.zeros(n)
+    for x in range(len(col) - 1):
+        tf = 1.0 if x == 0 else 2.0
+        for a in range(col[x], col[x + 1]):
+            z = geo["az"][a]
+            k = np.sqrt(x * x + ky ** 2 + kk(z) ** 2)
+            ik = (k + 1.5).astype(int)
+            e = 0.5 * tf * np.sum(np.abs(un[:, a, :]) ** 2, axis=0)
+            np.add.at(E, ik, e)
+    return E
+
+
+def run_pair(oracle_mod, gpu_mod, n, prec, steps, kshift=1, cfl=-1.0, dt=0.005, nu=0.01, seed=1234):
+    o = oracle_mod.Oracle(n, nu, cfl=cfl, dt=dt, kshift=kshift)
+    un0 = o.field_init(seed)
+    o.set_state(un0)
+    s = gpu_mod.Solver(n=n, precision=prec, viscos=nu, cfl=cfl, dt=dt, kshift=kshift,
+                       seed_input=o_seed_default())
+    s.set_state(un0)
+    infos = []
+    for _ in range(steps):
+        assert o.step() == 0
+        info = s.step()
+        assert info["status"] == 0
+        infos.append((o.scalars(), info))
+    u_o, un_o = o.get_state()
+    u_g = s.get_state(gpu_mod.FIELD_U)
+    un_g = s.get_state(gpu_mod.FIELD_UN)
+    geo = o.geometry()
+    o.close()
+    s.close()
+    return u_o, un_o, u_g, un_g, infos, geo
+
+
+def o_seed_default():
+    return 122929298
+
+
+@pytest.mark.parametrize("n", [16, 32, 64])
+def test_fp64_one_step(oracle_mod, gpu_mod, n):
+    u_o, un_o, u_g, un_g, infos, geo = run_pair(oracle_mod, gpu_mod, n, gpu_mod.PREC_FP64, 1)
+    so, sg = infos[0]
+    np.testing.assert_array_equal(sg["gsh1"], so["gsh"][:, 0])
+    assert abs(sg["velmax"] - so["velmax"]) <= 1e-12 * so["velmax"]
+    assert rel_l2(un_g, un_o) < 1e-11
+    assert rel_l2(u_g, u_o) < 1e-11
+
+
+def test_fp64_five_steps_adaptive_dt(oracle_mod, gpu_mod):
+    n = 32
+    u_o, un_o, u_g, un_g, infos, geo = run_pair(oracle_mod, gpu_mod, n, gpu_mod.PREC_FP64, 5, cfl=1.0)
+    for so, sg in infos:
+        assert abs(sg["dt"] - so["dt"]) <= 1e-12 * so["dt"]
+    assert rel_l2(un_g, un_o) < 1e-11
+    Eo, Eg = shell_spectrum(un_o, geo, n), shell_spectrum(un_g, geo, n)
+    m = Eo > 1e-30
+    assert np.max(np.abs(Eg[m] - Eo[m]) / Eo[m]) < 1e-10
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_fp32_five_steps(oracle_mod, gpu_mod, n):
+    u_o, un_o, u_g, un_g, infos, geo = run_pair(oracle_mod, gpu_mod, n, gpu_mod.PREC_FP32, 5)
+    err = rel_l2(un_g, un_o)
+    assert err < 2e-5, err
+    Eo, Eg = shell_spectrum(un_o, geo, n), shell_spectrum(un_g, geo, n)
+    m = Eo > 1e-8 * Eo.max()
+    assert np.max(np.abs(Eg[m] - Eo[m]) / Eo[m]) < 1e-4
+
+
+@pytest.mark.parametrize("kshift", [2, 3, 4])
+def test_shift_modes(oracle_mod, gpu_mod, kshift):
+    u_o, un_o, u_g, un_g, infos, geo = run_pair(oracle_mod, gpu_mod, 32, gpu_mod.PREC_FP64, 2, kshift=kshift)
+    assert rel_l2(un_g, un_o) < 1e-11
+
+
+def test_rk_stage_entry_point(oracle_mod, gpu_mod):
+    """psdns_gpu_rk_stage with driver-supplied shifts and dt."""
+    n = 32
+    o = oracle_mod.Oracle(n, 0.01, cfl=-1, dt=0.004, kshift=4)
+    un0 = o.field_init(99)
+    o.set_state(un0)
+    gsh = np.array([[0.1, 0.6], [0.3, 0.8], [0.45, 0.95]])
+    o.set_shifts(gsh)
+    o.stage(1)
+    o.stage(2)
+    s = gpu_mod.Solver(n=n, precision=gpu_mod.PREC_FP64, viscos=0.01, cfl=-1, dt=0.004, kshift=4)
+    s.set_state(un0)
+    vm = s.rk_stage(1, gsh, dt=0.004)
+    s.rk_stage(2, gsh)
+    assert abs(vm - o.scalars()["velmax"]) < 1e-12 * vm
+    _, un_o = o.get_state()
+    assert rel_l2(s.get_state(gpu_mod.FIELD_UN), un_o) < 1e-11
+    o.close(); s.close()

@@ -1,0 +1,142 @@
+"""CPU tests of the FP64 oracle: FFT against numpy, geometry against the
+reference's cylinder formulas, the LCG stream, and analytic properties of the
+initial field and of the RK2 step (no GPU)."""
+import numpy as np
+import pytest
+
+
+@pytest.mark.parametrize("n", [8, 16, 48, 64, 96, 128, 30])
+def test_fft_matches_numpy(oracle_mod, n):
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    np.testing.assert_allclose(oracle_mod.fft(x, -1), np.fft.fft(x), rtol=0, atol=1e-12 * n)
+    np.testing.assert_allclose(oracle_mod.fft(x, +1), np.fft.ifft(x) * n, rtol=0, atol=1e-12 * n)
+
+
+def test_fft_known_answers(oracle_mod):
+    n = 32
+    d = np.zeros(n, complex); d[0] = 1
+    np.testing.assert_allclose(oracle_mod.fft(d, -1), np.ones(n), atol=1e-15)
+    k0 = 5
+    tone = np.exp(2j * np.pi * k0 * np.arange(n) / n)
+    F = oracle_mod.fft(tone, -1)
+    expect = np.zeros(n, complex); expect[k0] = n
+    np.testing.assert_allclose(F, expect, atol=1e-12)
+
+
+# xz_tot for the grids quoted by the scope table (mpisetup.f:322-332)
+@pytest.mark.parametrize("n,kxn,xz_tot", [(16, 8, 96), (64, 31, 1465), (256, 121, 22995), (1024, 483, 366525)])
+def test_geometry_counts(oracle_mod, n, kxn, xz_tot):
+    o = oracle_mod.Oracle(n, 0.01, kshift=4)
+    assert (o.kxn, o.xz_tot) == (kxn, xz_tot)
+    g = o.geometry()
+    # each column x keeps n - 1 - 2 cut_z(x) kz values (mpisetup.f:332)
+    np.testing.assert_array_equal(np.diff(g["colstart"]), n - 1 - 2 * g["cut"])
+    o.close()
+
+
+def test_mask_matches_formula(oracle_mod):
+    n = 48
+    o = oracle_mod.Oracle(n, 0.01, kshift=4)
+    g = o.geometry()
+    col = g["colstart"]
+    kk = lambda i: i - n if i > n // 2 else i
+    for x in range(o.kxn):
+        for a in range(col[x], col[x + 1]):
+            z = g["az"][a]
+            for y in range(n):
+                sqk = (kk(y) / n) ** 2 + ((kk(z) / n) ** 2 + (x / n) ** 2)
+                inside = not (sqk > 2.0 / 9.0 or y == n // 2 or z == n // 2)
+                assert inside == (abs(kk(y)) <= g["kymax"][a] and y != n // 2)
+    o.close()
+
+
+def test_field_is_solenoidal_and_normalised(oracle_mod):
+    n = 32
+    o = oracle_mod.Oracle(n, 0.01, kshift=4)
+    g = o.geometry()
+    un = o.field_init(1234)
+    F = np.zeros((3, n, n, n // 2 + 1), complex)
+    for x in range(o.kxn):
+        for a in range(g["colstart"][x], g["colstart"][x + 1]):
+            F[:, :, g["az"][a], x] = un[:, a, :]
+    ky = np.fft.fftfreq(n, 1.0 / n)
+    kx = np.arange(n // 2 + 1)
+    div = kx[None, None, :] * F[0] + ky[:, None, None] * F[1] + ky[None, :, None] * F[2]
+    assert np.abs(div).max() < 1e-14
+    tf = np.where(kx == 0, 1.0, 2.0)
+    tke = 0.5 * np.sum(np.abs(F) ** 2 * tf)
+    assert abs(tke - 1.5) < 1e-12
+    # physical field is real: conjugate symmetry of the kx = 0 plane (consym.f)
+    p = np.fft.irfftn(F, s=(n, n, n), axes=(1, 2, 3))
+    back = np.fft.rfftn(p, axes=(1, 2, 3))
+    np.testing.assert_allclose(back, F, atol=1e-14)
+    o.close()
+
+
+def test_unforced_step_decays_energy_and_stays_solenoidal(oracle_mod):
+    n = 32
+    o = oracle_mod.Oracle(n, 0.01, cfl=-1, dt=0.005, kshift=1)
+    un = o.field_init(7)
+    o.set_state(un)
+    g = o.geometry()
+    kx = np.arange(n // 2 + 1)
+    ky = np.fft.fftfreq(n, 1.0 / n)
+    e_prev = 1.5
+    for _ in range(3):
+        assert o.step() == 0
+        _, un = o.get_state()
+        F = np.zeros((3, n, n, n // 2 + 1), complex)
+        for x in range(o.kxn):
+            for a in range(g["colstart"][x], g["colstart"][x + 1]):
+                F[:, :, g["az"][a], x] = un[:, a, :]
+        div = kx[None, None, :] * F[0] + ky[:, None, None] * F[1] + ky[None, :, None] * F[2]
+        assert np.abs(div).max() < 1e-13
+        tf = np.where(kx == 0, 1.0, 2.0)
+        e = 0.5 * np.sum(np.abs(F) ** 2 * tf)
+        assert e < e_prev
+        e_prev = e
+    o.close()
+
+
+def test_single_shear_mode_decays_viscously(oracle_mod):
+    """u = (sin y, 0, 0): the nonlinear term vanishes, so each RK2 step
+    multiplies the mode by exp(-nu k^2 dt) exactly (integrating factor)."""
+    n = 16
+    nu, dt = 0.05, 0.01
+    o = oracle_mod.Oracle(n, nu, cfl=-1, dt=dt, kshift=1)
+    un = np.zeros(o.state_shape(), complex)
+    # column a = 0 is (kx, kz) = (0, 0); sin y = (e^{iy} - e^{-iy}) / 2i
+    un[0, 0, 1] = -0.5j
+    un[0, 0, n - 1] = 0.5j
+    o.set_state(un)
+    for s in range(4):
+        o.step()
+    _, out = o.get_state()
+    f = np.exp(-nu * 4 * dt)
+    np.testing.assert_allclose(out[0, 0, 1], -0.5j * f, atol=1e-15)
+    np.testing.assert_allclose(out[0, 0, n - 1], 0.5j * f, atol=1e-15)
+    out[0, 0, 1] = out[0, 0, n - 1] = 0
+    assert np.abs(out).max() < 1e-15
+    o.close()
+
+
+def test_lcg_stream(oracle_mod):
+    """ranu.f: iseed = iseed*65539 mod 2^31 (32-bit wrap folded positive)."""
+    o = oracle_mod.Oracle(16, 0.01, cfl=-1, dt=0.005, kshift=2, seed_input=12345)
+    o.set_state(np.zeros(o.state_shape(), complex))
+    o.step()
+    g = o.scalars()["gsh"]
+    s = 12345
+    draws = []
+    for _ in range(6):
+        s = (s * 65539) % (1 << 32)
+        if s >= 1 << 31:
+            s -= 1 << 32
+        if s < 0:
+            s += 1 << 31
+        draws.append(s * 0.46566127e-9)
+    # kshift = 2: gsh(i,1) = ranu, gsh(i,2) = mod(gsh(i,1)+0.5, 1)
+    np.testing.assert_array_equal(g[:, 0], draws[:3])
+    np.testing.assert_array_equal(g[:, 1], np.fmod(np.array(draws[:3]) + 0.5, 1.0))
+    o.close()
