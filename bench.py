@@ -1,0 +1,312 @@
+#!/usr/bin/env python
+"""bench.py -- throughput of the PSDNS RK2 time step on B200.
+
+Workload: one periodic box of n^3 points (default 1024^3) with an FP32 device
+state, advanced by the RK2 step of PSDNS (both stages: phase shift, inverse
+transforms, products, forward transforms, wavespace closure, integrating
+factor update, projection).  The initial field is the seeded random solenoidal
+field of field.f with E(k) ~ k^4 exp(-2 (k/3)^2), u' = 1 (synthetic; no
+dataset is involved).
+
+`value` is points per second (Gpts/s = n^3 / step time) with the state
+resident in HBM; `e2e` is the same metric through the C-ABI with the state in
+pinned host memory, copied in and out every step.
+
+Multi-GPU: one independent box per GPU (replicas only; the single-box path
+has no data-path collective), timed as the max over ranks.
+
+`--impl reference` times the CPU restatement of the reference's step (the
+oracle, C/OpenMP on all host cores) on a bounded sample: one RK2 step of a
+256^3 box per timed step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "nasa-bluewater-psdns-benchmark-minsky_b200")
+sys.path.insert(0, PKG)
+sys.path.insert(0, ROOT)
+
+METRIC = "RK2 step throughput at 1024^3 (Gpts/s = N^3 / step time)"
+UNIT = "Gpts/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=1024)
+    ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-n", type=int, default=256)
+    return ap.parse_args()
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_oracle_rate(n, steps, warmup, threads):
+    """Oracle (FP64 C/OpenMP restatement of the reference step) on host cores."""
+    from oracle import oracle
+    oracle.build()
+    oracle.set_threads(threads)
+    o = oracle.Oracle(n, 0.01, cfl=-1.0, dt=0.001, kshift=1)
+    o.set_state(o.field_init(1234))
+    for _ in range(warmup):
+        o.step()
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        o.step()
+        ts.append(time.perf_counter() - t0)
+    o.close()
+    return ts
+
+
+def algorithmic_bytes(n, kxn, xz_tot, csz):
+    """Compulsory HBM bytes per launch of the five stage kernels (per-axis pass
+    model: each pass reads and writes its variables once, cylinder zero bands
+    are neither read nor written, the x chain keeps the physical field on chip).
+    C = xz_tot*n complex, Z = kxn*n^2 complex."""
+    C = xz_tot * n * csz
+    Z = kxn * n * n * csz
+    return {"k_yinv": 6 * C, "k_zinv": 3 * C + 3 * Z, "k_xchain": 8 * Z, "k_zfwd": 5 * Z + 4 * C,
+            "k_yfwd": 13 * C}, 2 * (26 * C + 16 * Z)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.dev), "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out = ""
+        sm, mx, reasons, n = [], [], set(), 0
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            n += 1
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": n}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = host_cores()
+    n = args.cpu_n
+    ts = cpu_oracle_rate(n, args.steps, args.warmup, cores)
+    t = sum(ts) / len(ts)
+    v = n ** 3 / t / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"RK2 step, {args.n}^3 box (timed on a bounded sample: one {n}^3 step per timed step)",
+                   "n": args.n, "sample_n": n},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"one full RK2 step of a {n}^3 box per timed step (FP64 C/OpenMP restatement "
+                                   f"of the reference, {cores} threads); Gpts/s = {n}^3/t"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import psdns_gpu as P
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    # the library uses the current device of the calling thread
+    n = args.n
+    prec = P.PREC_FP32 if args.prec == "fp32" else P.PREC_FP64
+    csz = 8 if prec == P.PREC_FP32 else 16
+    nu = 0.0028 * (512.0 / n) ** (4.0 / 3.0)
+    s = P.Solver(n=n, precision=prec, viscos=nu, cfl=3.77 / 2.0, dt=0.0, kshift=1)
+    s.field_init(1234 + rank)
+    stream = torch.cuda.ExternalStream(s.stream())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        s.step()
+    barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.4)
+    s.profile(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        info = s.step()
+    e1.record(stream)
+    e1.synchronize()
+    ms_total = e0.elapsed_time(e1)
+    kms, kcnt = s.kernel_times()
+    s.profile(False)
+    ck = clocks.stop()
+    barrier()
+    if dist is not None:
+        t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = world * n ** 3 / (ms_step * 1e-3) / 1e9
+
+    names = ["k_yinv", "k_zinv", "k_xchain", "k_zfwd", "k_yfwd"]
+    per_launch, step_bytes = algorithmic_bytes(n, s.kxn, s.xz_tot, csz)
+    dom = max(range(5), key=lambda i: kms[i])
+    avg_ms = kms[dom] / max(1, kcnt[dom])
+    achieved = per_launch[names[dom]] / (avg_ms * 1e-3) / 1e9
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak = json.load(open(peaks_path))["hbm_gbs"]
+        peak_src = "measured"
+    else:
+        peak = 6650.0
+        peak_src = "fallback"
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(tpath):
+        tj = json.load(open(tpath))
+        key = f"{names[dom]}_{args.prec}_{n}"
+        if key in tj:
+            traffic = tj[key]
+    kernel_table = {names[i]: {"ms_per_launch": kms[i] / max(1, kcnt[i]), "launches": int(kcnt[i]),
+                               "share": kms[i] / max(1e-12, sum(kms)),
+                               "algorithmic_bytes": per_launch[names[i]],
+                               "achieved_gbs": per_launch[names[i]] / (kms[i] / max(1, kcnt[i]) * 1e-3) / 1e9}
+                    for i in range(5)}
+
+    # end to end through the C-ABI: state (complex(8), reference layout) copied
+    # from pinned host memory and back every step
+    e2e = None
+    if not args.no_e2e:
+        nbytes = 3 * s.xz_tot * n * 16
+        try:
+            host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+            ptr = host.data_ptr()
+            s.get_state_ptr(ptr)
+            barrier()
+            f0 = torch.cuda.Event(enable_timing=True)
+            f1 = torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            for _ in range(args.e2e_steps):
+                s.set_state_ptr(ptr)
+                s.step()
+                s.get_state_ptr(ptr)
+            f1.record(stream)
+            f1.synchronize()
+            ems = f0.elapsed_time(f1) / args.e2e_steps
+            if dist is not None:
+                t = torch.tensor([ems], dtype=torch.float64, device="cuda")
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                ems = float(t.item())
+            e2e = {"value": world * n ** 3 / (ems * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                   "d2h_bytes_per_step": nbytes, "ms_per_step": ems, "steps": args.e2e_steps}
+            del host
+        except Exception as ex:  # pinned allocation may exceed host memory
+            e2e = {"value": None, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                   "error": str(ex)[:200]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cores = host_cores()
+        ts = cpu_oracle_rate(args.cpu_n, 1, 0, cores)
+        t = sum(ts) / len(ts)
+        cpu = {"value": args.cpu_n ** 3 / t / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"one RK2 step of a {args.cpu_n}^3 box (FP64 C/OpenMP restatement of the reference, "
+                         f"{cores} threads, {t:.2f} s); Gpts/s = {args.cpu_n}^3/t"}
+    s.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if prec == P.PREC_FP32 else "f64",
+            "data": "synthetic: seeded random solenoidal field, E(k)~k^4 exp(-2(k/3)^2), u'=1",
+            "config": {"workload": f"unforced RK2 step of one {n}^3 periodic box per GPU, "
+                                   f"{args.prec} state, kshift=1 phase shifts, adaptive dt (cfl=1.885)",
+                       "n": n, "precision": args.prec, "viscosity": nu, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (state >= 9 GB per variable set), no flush needed"},
+            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
+                         "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "step_achieved": step_bytes / (ms_step * 1e-3) / 1e9,
+                         "step_frac": step_bytes / (ms_step * 1e-3) / 1e9 / peak},
+            "kernels": kernel_table,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(sum(kcnt)),
+            "clocks": ck,
+            "last_step": {"dt": info["dt"], "velmax": info["velmax"], "courant": info["courant"]},
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

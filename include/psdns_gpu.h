@@ -86,6 +86,12 @@ int psdns_gpu_finalize(void *ctx);
  * array in the given layout (complex(8), 3+nc variables). */
 int psdns_gpu_set_state(void *ctx, const double *un, int32_t layout);
 
+/* Random solenoidal initial field on the device, un = u (replaces
+ * PSDNS/homogeneous/field.f:169-257 with PSDNS/homogeneous/consym.f:35-73,
+ * the ranu-phase branch).  Spectrum E(k) = c0 k^4 exp(-2 (k/3)^2) with
+ * integral 3/2 (u' = 1); seed starts the ranu stream (PSDNS/ranu.f). */
+int psdns_gpu_field_init(void *ctx, int32_t seed);
+
 /* Copy u or un back to a host array (complex(8), 3+nc variables). */
 int psdns_gpu_get_state(void *ctx, double *out, int32_t which, int32_t layout);
 
@@ -107,6 +113,20 @@ int psdns_gpu_rk_stage(void *ctx, int32_t kstep, const double *gsh, const double
 
 /* Run statistics: time, dt, velmax, jstep. */
 int psdns_gpu_get_time(void *ctx, double *out4);
+
+/* The CUDA stream (cudaStream_t) on which the context launches all its work,
+ * so that a caller can time or order work against it.  Plumbing; no
+ * counterpart in the reference. */
+int psdns_gpu_get_stream(void *ctx, void **stream);
+
+/* Per-kernel device timing with CUDA events on the context's stream
+ * (replaces the MPI_WTIME stage timers tt(1..10) of
+ * PSDNS/timestep_module.f:90-478).  enable != 0 starts (and zeroes) the
+ * accumulation; psdns_gpu_kernel_times returns, for the five stage kernels
+ * (y backward, z backward, x chain, z forward, y forward + update), the summed
+ * milliseconds ms[5] and launch counts launches[5]. */
+int psdns_gpu_profile(void *ctx, int32_t enable);
+int psdns_gpu_kernel_times(void *ctx, double *ms, int64_t *launches);
 
 /* Message of the last error on this thread ("" if none). */
 int psdns_gpu_last_error(char *buf, int32_t len);

@@ -18,6 +18,7 @@
 #include "psdns_gpu.h"
 #include "psdns_host.h"
 #include "stage_kernels.cuh"
+#include "field_init.cuh"
 
 namespace psdns {
 
@@ -151,7 +152,29 @@ struct Ctx {
   int jstep = 0;
   double time = 0, dt = 0, dt0 = 0, dt2 = 0, velmax = 0;
   int kfor = 0, k2fo = 0;
+  // per-kernel CUDA-event timing: [stage][kernel][begin/end]
+  bool prof = false;
+  cudaEvent_t ev[2][5][2] = {};
+  double prof_ms[5] = {0, 0, 0, 0, 0};
+  long long prof_n[5] = {0, 0, 0, 0, 0};
+  bool prof_pending[2] = {false, false};
 };
+
+static void prof_mark(Ctx& c, int stage, int k, int end) {
+  if (c.prof) cudaEventRecord(c.ev[stage][k][end], c.stream);
+}
+
+// fold the events of a finished stage into the totals (stream already synced)
+static void prof_collect(Ctx& c, int stage, int k0, int k1) {
+  if (!c.prof) return;
+  for (int k = k0; k < k1; k++) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c.ev[stage][k][0], c.ev[stage][k][1]) == cudaSuccess) {
+      c.prof_ms[k] += ms;
+      c.prof_n[k] += 1;
+    }
+  }
+}
 
 template <typename T> struct TabLayout {
   // offsets in bytes inside the stage-table block
@@ -239,22 +262,31 @@ template <typename T, int N> struct Impl {
     C* ub = (C*)c.d_ub;
     C* uz = (C*)c.d_uz;
     const int kxn = c.g.kxn;
+    const int s = kstep - 1;
     {
       constexpr int TH = Launch<T, N, TL::TB_I>::THREADS;
+      prof_mark(c, s, 0, 0);
       k_yinv<T, N><<<dim3(c.nab_i, 3), TH, sm1(), c.stream>>>(g, st, u, ub, tw);
+      prof_mark(c, s, 0, 1);
     }
     {
       constexpr int TH = Launch<T, N, TL::XT2>::THREADS;
+      prof_mark(c, s, 1, 0);
       k_zinv<T, N><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3), TH, sm2(), c.stream>>>(g, ub, uz, tw);
+      prof_mark(c, s, 1, 1);
     }
     {
       constexpr int TH = Launch<T, N, 2 * TL::TZ>::THREADS;
+      prof_mark(c, s, 2, 0);
       k_xchain<T, N><<<dim3(c.nzt, N), TH, sm3(), c.stream>>>(g, uz, tw, st.b11, st.b22, st.b33, c.d_velmax,
                                                                 kstep == 1 ? 1 : 0);
+      prof_mark(c, s, 2, 1);
     }
     {
       constexpr int TH = Launch<T, N, 2 * TL::XT4>::THREADS;
+      prof_mark(c, s, 3, 0);
       k_zfwd<T, N><<<dim3(N, (kxn + TL::XT4 - 1) / TL::XT4), TH, sm4(), c.stream>>>(g, uz, ub, tw, st.b11, st.b33);
+      prof_mark(c, s, 3, 1);
     }
     CK(cudaGetLastError());
     return 0;
@@ -265,12 +297,14 @@ template <typename T, int N> struct Impl {
     Geo g = make_geo(c);
     StageTables<T> st = make_tables<T>(c, kstep - 1);
     constexpr int TH = Launch<T, N, 4 * TL::TB_F>::THREADS;
+    prof_mark(c, kstep - 1, 4, 0);
     if (kstep == 1)
       k_yfwd<T, N, 1><<<c.nab_f, TH, sm5(), c.stream>>>(g, st, (const C*)c.d_ub, (C*)c.d_u, (C*)c.d_un,
                                                         (const C*)c.d_tw, c.d_efkz);
     else
       k_yfwd<T, N, 2><<<c.nab_f, TH, sm5(), c.stream>>>(g, st, (const C*)c.d_ub, (C*)c.d_u, (C*)c.d_un,
                                                         (const C*)c.d_tw, c.d_efkz);
+    prof_mark(c, kstep - 1, 4, 1);
     CK(cudaGetLastError());
     return 0;
   }
@@ -410,6 +444,7 @@ static int run_stage(Ctx& c, const Ops& o, int kstep, int* ctl_err) {
   if (kstep == 1) {
     CK(cudaMemcpyAsync(c.h_velmax, c.d_velmax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
+    prof_collect(c, 0, 0, 4);
     double vm;
     std::memcpy(&vm, c.h_velmax, sizeof vm);
     c.velmax = vm;
@@ -557,6 +592,10 @@ int psdns_gpu_finalize(void* ctx) {
                   c->d_ub, c->d_uz, c->d_forc, c->d_efkz, c->d_velmax};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  for (int s = 0; s < 2; s++)
+    for (int k = 0; k < 5; k++)
+      for (int e = 0; e < 2; e++)
+        if (c->ev[s][k][e]) cudaEventDestroy(c->ev[s][k][e]);
   if (c->h_tabs) cudaFreeHost(c->h_tabs);
   if (c->h_velmax) cudaFreeHost(c->h_velmax);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -622,6 +661,8 @@ int psdns_gpu_step(void* ctx, double* info) {
   if (run_stage(*c, o, 1, &ctl)) return 1;
   if (run_stage(*c, o, 2, &ctl)) return 1;
   CK(cudaStreamSynchronize(c->stream));
+  prof_collect(*c, 0, 4, 5);
+  prof_collect(*c, 1, 0, 5);
   if (info) {
     info[0] = c->dt;
     info[1] = c->time;
@@ -662,6 +703,76 @@ int psdns_gpu_rk_stage(void* ctx, int32_t kstep, const double* gsh, const double
   }
   if (o.stage_b(*c, kstep)) return 1;
   CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int psdns_gpu_field_init(void* ctx, int32_t seed) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return set_error("null context");
+  if (seed <= 0) return set_error("seed %d must be positive (ranu.f:33)", seed);
+  const Geometry& g = c->g;
+  const int n = c->n;
+  // offsets of each column's first draw (in modes) in the traversal order
+  std::vector<long long> off(g.xz_tot);
+  long long acc = 0;
+  for (int a = 0; a < g.xz_tot; a++) {
+    off[a] = acc;
+    const int km = std::min(g.kymax[a], n / 2 - 1);
+    long long cnt = km >= 0 ? 2LL * km + 1 : 0;
+    if (a == 0 && cnt > 0) cnt -= 1;   // the k = 0 mode draws nothing
+    acc += cnt;
+  }
+  long long* d_off = nullptr;
+  CK(cudaMalloc(&d_off, sizeof(long long) * g.xz_tot));
+  cudaError_t e = cudaMemcpy(d_off, off.data(), sizeof(long long) * g.xz_tot, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { cudaFree(d_off); return set_error("upload failed: %s", cudaGetErrorString(e)); }
+  Geo geo = make_geo(*c);
+  const double s1 = c->p.beta1, s2 = c->p.beta2, s3 = c->p.beta3;
+  const int kc0 = n / 2 - 1 - g.cut[0];
+  if (c->prec == PSDNS_PREC_FP64) {
+    k_field_init<double><<<148 * 8, 256, 0, c->stream>>>(geo, d_off, (uint32_t)seed, s1, s2, s3, (double2*)c->d_un,
+                                                         (double2*)c->d_u);
+    k_field_consym<double><<<148, 256, 0, c->stream>>>(n, kc0, g.xz_tot, (double2*)c->d_un, (double2*)c->d_u);
+  } else {
+    k_field_init<float><<<148 * 8, 256, 0, c->stream>>>(geo, d_off, (uint32_t)seed, s1, s2, s3, (float2*)c->d_un,
+                                                        (float2*)c->d_u);
+    k_field_consym<float><<<148, 256, 0, c->stream>>>(n, kc0, g.xz_tot, (float2*)c->d_un, (float2*)c->d_u);
+  }
+  e = cudaGetLastError();
+  cudaError_t e2 = cudaStreamSynchronize(c->stream);
+  cudaFree(d_off);
+  if (e != cudaSuccess || e2 != cudaSuccess)
+    return set_error("field init failed: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+  return 0;
+}
+
+int psdns_gpu_get_stream(void* ctx, void** stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !stream) return set_error("null argument");
+  *stream = (void*)c->stream;
+  return 0;
+}
+
+int psdns_gpu_profile(void* ctx, int32_t enable) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return set_error("null context");
+  if (enable && !c->ev[0][0][0]) {
+    for (int s = 0; s < 2; s++)
+      for (int k = 0; k < 5; k++)
+        for (int e = 0; e < 2; e++) CK(cudaEventCreate(&c->ev[s][k][e]));
+  }
+  c->prof = enable != 0;
+  for (int k = 0; k < 5; k++) { c->prof_ms[k] = 0; c->prof_n[k] = 0; }
+  return 0;
+}
+
+int psdns_gpu_kernel_times(void* ctx, double* ms, int64_t* launches) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return set_error("null context");
+  for (int k = 0; k < 5; k++) {
+    if (ms) ms[k] = c->prof_ms[k];
+    if (launches) launches[k] = c->prof_n[k];
+  }
   return 0;
 }
 

@@ -36,6 +36,10 @@ EXPORTS = (
     "psdns_gpu_rk_stage",
     "psdns_gpu_get_time",
     "psdns_gpu_last_error",
+    "psdns_gpu_field_init",
+    "psdns_gpu_get_stream",
+    "psdns_gpu_profile",
+    "psdns_gpu_kernel_times",
 )
 
 
@@ -82,6 +86,10 @@ def load():
     L.psdns_gpu_rk_stage.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_get_time.argtypes = [vp, dp]
     L.psdns_gpu_last_error.argtypes = [ctypes.c_char_p, ctypes.c_int32]
+    L.psdns_gpu_field_init.argtypes = [vp, ctypes.c_int32]
+    L.psdns_gpu_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
+    L.psdns_gpu_profile.argtypes = [vp, ctypes.c_int32]
+    L.psdns_gpu_kernel_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int64)]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     _LIB = L
@@ -192,6 +200,26 @@ class Solver:
         _check(load().psdns_gpu_rk_stage(self._ctx, int(kstep), _dp(g), _dp(dtv), None, _dp(vm)),
                "psdns_gpu_rk_stage")
         return vm[0]
+
+    def field_init(self, seed):
+        """Random solenoidal field (field.f restated) written to u and un on the device."""
+        _check(load().psdns_gpu_field_init(self._ctx, int(seed)), "field_init")
+
+    def stream(self):
+        """cudaStream_t (as int) on which the context launches its kernels."""
+        s = ctypes.c_void_p()
+        _check(load().psdns_gpu_get_stream(self._ctx, ctypes.byref(s)), "get_stream")
+        return s.value or 0
+
+    def profile(self, enable=True):
+        _check(load().psdns_gpu_profile(self._ctx, 1 if enable else 0), "profile")
+
+    def kernel_times(self):
+        ms = np.zeros(5, np.float64)
+        cnt = np.zeros(5, np.int64)
+        _check(load().psdns_gpu_kernel_times(self._ctx, _dp(ms), cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))),
+               "kernel_times")
+        return ms, cnt
 
     def time_info(self):
         out = np.zeros(4, np.float64)

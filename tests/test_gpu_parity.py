@@ -114,3 +114,17 @@ def test_rk_stage_entry_point(oracle_mod, gpu_mod):
     _, un_o = o.get_state()
     assert rel_l2(s.get_state(gpu_mod.FIELD_UN), un_o) < 1e-11
     o.close(); s.close()
+
+
+@pytest.mark.parametrize("prec,tol", [(1, 1e-13), (0, 1e-6)])
+def test_device_field_init_matches_oracle(oracle_mod, gpu_mod, prec, tol):
+    """field.f restated on the device (jump-ahead LCG) against the sequential oracle."""
+    n = 32
+    o = oracle_mod.Oracle(n, 0.01, kshift=4)
+    ref = o.field_init(2024)
+    s = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=-1, dt=0.005, kshift=4)
+    s.field_init(2024)
+    got = s.get_state(gpu_mod.FIELD_UN)
+    assert rel_l2(got, ref) < tol
+    np.testing.assert_array_equal(s.get_state(gpu_mod.FIELD_U), got)
+    o.close(); s.close()
