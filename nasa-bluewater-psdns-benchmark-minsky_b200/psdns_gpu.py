@@ -40,6 +40,7 @@ EXPORTS = (
     "psdns_gpu_get_stream",
     "psdns_gpu_profile",
     "psdns_gpu_kernel_times",
+    "psdns_gpu_rk_stage_noalloc",
 )
 
 
@@ -90,6 +91,7 @@ def load():
     L.psdns_gpu_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
     L.psdns_gpu_profile.argtypes = [vp, ctypes.c_int32]
     L.psdns_gpu_kernel_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int64)]
+    L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     _LIB = L
@@ -134,6 +136,24 @@ def geometry(n):
     ip = ctypes.POINTER(ctypes.c_int32)
     _check(load().psdns_gpu_geometry(n, None, None, cut.ctypes.data_as(ip), col.ctypes.data_as(ip)), "geometry")
     return {"kxn": kxn.value, "xz_tot": tot.value, "cut": cut, "colstart": col}
+
+
+NOALLOC_MAX_N = 64
+
+
+def rk_stage_noalloc(params, kstep, gsh, dt, u_ptr, un_ptr, stream=0):
+    """One RK stage on caller-owned device arrays with no device allocation
+    (psdns_gpu_rk_stage_noalloc).  u_ptr/un_ptr: device addresses of the YCYL
+    state in the params' precision; dt must be given at both stages.  Returns
+    velmax at stage 1."""
+    g = np.ascontiguousarray(np.asarray(gsh, np.float64).reshape(3, 2).T.reshape(-1))
+    dtv = np.array([dt], np.float64)
+    vm = np.zeros(1, np.float64)
+    _check(load().psdns_gpu_rk_stage_noalloc(ctypes.byref(params), int(kstep), _dp(g), _dp(dtv),
+                                             ctypes.c_void_p(u_ptr), ctypes.c_void_p(un_ptr), _dp(vm),
+                                             ctypes.c_void_p(stream)),
+           "psdns_gpu_rk_stage_noalloc")
+    return vm[0]
 
 
 class Solver:
