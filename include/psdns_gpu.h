@@ -111,6 +111,15 @@ int psdns_gpu_step(void *ctx, double *info);
 int psdns_gpu_rk_stage(void *ctx, int32_t kstep, const double *gsh, const double *dt,
                        const double *forcing, double *velmax_out);
 
+/* Eswaran-Pope forcing diagnostics of the last step (PSDNS/forcdt.f:18-41):
+ * efk[kfor] energy input per shell, eirate[3] per component, *erate total
+ * (each pointer may be NULL).  Error if the context is unforced. */
+int psdns_gpu_forcing_stats(void *ctx, double *efk, double *eirate, double *erate);
+
+/* The forcing table for(kfor,k2fo,k2fo,3) (complex(8), PSDNS/force.f:115-161)
+ * used by the last step, and its dimensions (param_set.f:33,37). */
+int psdns_gpu_forcing_table(void *ctx, double *table, int32_t *kfor, int32_t *k2fo);
+
 /* Run statistics: time, dt, velmax, jstep. */
 int psdns_gpu_get_time(void *ctx, double *out4);
 

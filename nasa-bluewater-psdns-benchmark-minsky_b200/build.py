@@ -9,7 +9,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = [os.path.join(HERE, "csrc", f) for f in ("psdns_api.cu", "stage_noalloc.cu")]
+SRC = [os.path.join(HERE, "csrc", f) for f in ("psdns_api.cu", "stage_noalloc.cu", "forcing.cpp")]
 OUT = os.path.join(HERE, "libpsdns_gpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

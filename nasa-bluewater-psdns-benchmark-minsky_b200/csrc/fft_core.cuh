@@ -231,6 +231,18 @@ template <typename T, int N> struct FFTPlan {
 __host__ __device__ __forceinline__ constexpr int pad32(int i) { return i + (i >> 5); }
 template <int N> struct LineLen { static constexpr int value = N + N / 32; };
 
+// Barrier among the threads that share a line.  When a line lives inside one
+// warp (P divides 32) a warp barrier suffices; otherwise the whole block
+// synchronises.
+template <int P>
+__device__ __forceinline__ void line_sync() {
+  if constexpr (P <= 32 && (32 % P) == 0) {
+    __syncwarp();
+  } else {
+    __syncthreads();
+  }
+}
+
 // One Stockham pass over nlines lines (rounds of LPR lines).
 template <typename C, int N, int R, int NS, int E, int P, int THREADS>
 __device__ __forceinline__ void fft_pass(C* buf, int nlines, int ls, const C* __restrict__ twp) {
@@ -257,7 +269,7 @@ __device__ __forceinline__ void fft_pass(C* buf, int nlines, int ls, const C* __
         dft_s<R, 1>(v + q * R);
       }
     }
-    __syncthreads();
+    line_sync<P>();
     if (act) {
 #pragma unroll
       for (int q = 0; q < NB; q++) {
@@ -268,7 +280,7 @@ __device__ __forceinline__ void fft_pass(C* buf, int nlines, int ls, const C* __
         for (int r = 0; r < R; r++) line[pad32(base + r * NS)] = v[q * R + r];
       }
     }
-    __syncthreads();
+    line_sync<P>();
   }
 }
 
@@ -290,6 +302,8 @@ template <typename T, int N, int THREADS>
 __device__ __forceinline__ void fft_lines(C2<T>* buf, int nlines, int ls, const C2<T>* tw) {
   static_assert(THREADS % FFTPlan<T, N>::P == 0, "THREADS must be a multiple of threads per line");
   fft_passes<T, N, THREADS, 0>(buf, nlines, ls, tw);
+  // results are read by other warps afterwards
+  __syncthreads();
 }
 
 // Host: build the twiddle table of FFTPlan<T,N> (pass p >= 1 table is

@@ -152,6 +152,10 @@ struct Ctx {
   int jstep = 0;
   double time = 0, dt = 0, dt0 = 0, dt2 = 0, velmax = 0;
   int kfor = 0, k2fo = 0;
+  EPForcing forcing;
+  void* h_forc = nullptr;          // pinned staging of the forcing table (device precision)
+  std::vector<double> efk_host;    // energy input per shell of the last step (forcdt.f)
+  double erate = 0, eirate[3] = {0, 0, 0};
   // per-kernel CUDA-event timing: [stage][kernel][begin/end]
   bool prof = false;
   cudaEvent_t ev[2][5][2] = {};
@@ -232,7 +236,7 @@ template <typename T, int N> struct Impl {
   static size_t sm1() { return TWB + sizeof(C) * TL::TB_I * L; }
   static size_t sm2() { return TWB + sizeof(C) * TL::XT2 * L; }
   static size_t sm3() { return TWB + sizeof(C) * 4 * (TL::TZ / 2) * L; }
-  static size_t sm4() { return TWB + sizeof(C) * 2 * TL::XT4 * L; }
+  static size_t sm4() { return TWB + sizeof(C) * 2 * TL::XT4 * TL::YT4 * L; }
   static size_t sm5() { return TWB + sizeof(C) * 4 * TL::TB_F * L; }
 
   static int setup() {
@@ -283,9 +287,9 @@ template <typename T, int N> struct Impl {
       prof_mark(c, s, 2, 1);
     }
     {
-      constexpr int TH = Launch<T, N, 2 * TL::XT4>::THREADS;
+      constexpr int TH = Launch<T, N, 2 * TL::XT4 * TL::YT4>::THREADS;
       prof_mark(c, s, 3, 0);
-      k_zfwd<T, N><<<dim3(N, (kxn + TL::XT4 - 1) / TL::XT4), TH, sm4(), c.stream>>>(g, uz, ub, tw, st.b11, st.b33);
+      k_zfwd<T, N><<<dim3(N / TL::YT4, (kxn + TL::XT4 - 1) / TL::XT4), TH, sm4(), c.stream>>>(g, uz, ub, tw, st.b11, st.b33);
       prof_mark(c, s, 3, 1);
     }
     CK(cudaGetLastError());
@@ -438,6 +442,38 @@ static int step_control(Ctx& c) {
   return err;
 }
 
+// for(kfor,k2fo,k2fo,3) complex double -> device precision -> d_forc
+static int upload_forcing(Ctx& c, const double* tab) {
+  const size_t nf = (size_t)c.kfor * c.k2fo * c.k2fo * 3;
+  if (c.prec == PSDNS_PREC_FP64) {
+    std::memcpy(c.h_forc, tab, nf * sizeof(double2));
+  } else {
+    float2* f = (float2*)c.h_forc;
+    for (size_t i = 0; i < nf; i++) f[i] = make_float2((float)tab[2 * i], (float)tab[2 * i + 1]);
+  }
+  CK(cudaMemcpyAsync(c.d_forc, c.h_forc, nf * c.csz, cudaMemcpyHostToDevice, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  return 0;
+}
+
+// forcdt.f:18-41: energy input per shell from efkz (device, FP64)
+static int collect_forcing_stats(Ctx& c) {
+  if (!(c.p.kforce > 0)) return 0;
+  std::vector<double> e(3 * (c.n / 2 + 2));
+  CK(cudaMemcpyAsync(e.data(), c.d_efkz, sizeof(double) * e.size(), cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  c.efk_host.assign(c.kfor, 0.0);
+  c.erate = 0;
+  c.eirate[0] = c.eirate[1] = c.eirate[2] = 0;
+  for (int k = 0; k < c.kfor; k++) {
+    const double e1 = e[3 * k] / c.dt, e2 = e[3 * k + 1] / c.dt, e3 = e[3 * k + 2] / c.dt;
+    c.efk_host[k] = .5 * (e1 + e2 + e3);
+    c.eirate[0] += e1; c.eirate[1] += e2; c.eirate[2] += e3;
+    c.erate += c.efk_host[k];
+  }
+  return 0;
+}
+
 static int run_stage(Ctx& c, const Ops& o, int kstep, int* ctl_err) {
   if (kstep == 1) CK(cudaMemsetAsync(c.d_velmax, 0, sizeof(unsigned long long), c.stream));
   if (o.stage_a(c, kstep)) return 1;
@@ -451,6 +487,12 @@ static int run_stage(Ctx& c, const Ops& o, int kstep, int* ctl_err) {
     *ctl_err = step_control(c);
     if (c.prec == PSDNS_PREC_FP64) fill_factor_tables<double>(c); else fill_factor_tables<float>(c);
     if (upload_tables(c)) return 1;
+    if (c.p.kforce > 0) {
+      // force.f, called after step at stage 1 (timestep_module.f:261-263)
+      c.forcing.step(c.rng, c.dt, 0);
+      if (upload_forcing(c, c.forcing.table.data())) return 1;
+      CK(cudaMemsetAsync(c.d_efkz, 0, sizeof(double) * 3 * (c.n / 2 + 2), c.stream));
+    }
   }
   if (o.stage_b(c, kstep)) return 1;
   return 0;
@@ -568,6 +610,9 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
 #undef ALLOC
   if (cudaMallocHost(&c->h_tabs, tabb) != cudaSuccess) return fail(set_error("cudaMallocHost"));
   if (cudaMallocHost((void**)&c->h_velmax, sizeof(unsigned long long)) != cudaSuccess) return fail(set_error("cudaMallocHost"));
+  if (cudaMallocHost(&c->h_forc, c->csz * std::max<size_t>(nfor, 1)) != cudaSuccess) return fail(set_error("cudaMallocHost"));
+  c->forcing.setup(c->kfor, n, p->kforce, p->tforce, p->epsfor, p->tfiuo, p->kranf1, p->kranf2,
+                   p->beta1 * p->beta1, p->beta2 * p->beta2, p->beta3 * p->beta3);
   std::memset(c->h_tabs, 0, tabb);
   if (cudaMemcpy(c->d_colstart, g.colstart.data(), sizeof(int) * (g.kxn + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(c->d_ax, g.ax.data(), sizeof(int) * g.xz_tot, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -598,6 +643,7 @@ int psdns_gpu_finalize(void* ctx) {
         if (c->ev[s][k][e]) cudaEventDestroy(c->ev[s][k][e]);
   if (c->h_tabs) cudaFreeHost(c->h_tabs);
   if (c->h_velmax) cudaFreeHost(c->h_velmax);
+  if (c->h_forc) cudaFreeHost(c->h_forc);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -663,6 +709,7 @@ int psdns_gpu_step(void* ctx, double* info) {
   CK(cudaStreamSynchronize(c->stream));
   prof_collect(*c, 0, 4, 5);
   prof_collect(*c, 1, 0, 5);
+  if (collect_forcing_stats(*c)) return 1;
   if (info) {
     info[0] = c->dt;
     info[1] = c->time;
@@ -681,7 +728,8 @@ int psdns_gpu_rk_stage(void* ctx, int32_t kstep, const double* gsh, const double
   Ctx* c = (Ctx*)ctx;
   if (!c || !gsh) return set_error("null argument");
   if (kstep != 1 && kstep != 2) return set_error("kstep must be 1 or 2");
-  if (forcing != nullptr) return set_error("forcing tables are not supported by this entry point yet");
+  if (forcing != nullptr && !(c->p.kforce > 0))
+    return set_error("a forcing table was passed but the context was created with kforce = 0");
   Ops o;
   if (!get_ops(c->prec, c->n, o)) return set_error("bad context");
   for (int i = 0; i < 3; i++) { c->gsh[i][0] = gsh[i]; c->gsh[i][1] = gsh[3 + i]; }
@@ -692,8 +740,19 @@ int psdns_gpu_rk_stage(void* ctx, int32_t kstep, const double* gsh, const double
     c->dt2 = c->dt / 2.;
     if (c->prec == PSDNS_PREC_FP64) fill_factor_tables<double>(*c); else fill_factor_tables<float>(*c);
     CK(cudaMemsetAsync(c->d_velmax, 0, sizeof(unsigned long long), c->stream));
+    if (c->p.kforce > 0) CK(cudaMemsetAsync(c->d_efkz, 0, sizeof(double) * 3 * (c->n / 2 + 2), c->stream));
   }
   if (upload_tables(*c)) return 1;
+  if (c->p.kforce > 0) {
+    // the driver passes this step's table (force.f); none means zero forcing
+    std::vector<double> zero;
+    const double* tab = forcing;
+    if (!tab) {
+      zero.assign((size_t)2 * c->kfor * c->k2fo * c->k2fo * 3, 0.0);
+      tab = zero.data();
+    }
+    if (kstep == 1 || forcing) { if (upload_forcing(*c, tab)) return 1; }
+  }
   if (o.stage_a(*c, kstep)) return 1;
   if (kstep == 1) {
     CK(cudaMemcpyAsync(c->h_velmax, c->d_velmax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
@@ -743,6 +802,25 @@ int psdns_gpu_field_init(void* ctx, int32_t seed) {
   cudaFree(d_off);
   if (e != cudaSuccess || e2 != cudaSuccess)
     return set_error("field init failed: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+  return 0;
+}
+
+int psdns_gpu_forcing_stats(void* ctx, double* efk, double* eirate, double* erate) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return set_error("null context");
+  if (!(c->p.kforce > 0)) return set_error("context is unforced (kforce = 0)");
+  if (efk) for (int k = 0; k < c->kfor; k++) efk[k] = k < (int)c->efk_host.size() ? c->efk_host[k] : 0.0;
+  if (eirate) for (int i = 0; i < 3; i++) eirate[i] = c->eirate[i];
+  if (erate) *erate = c->erate;
+  return 0;
+}
+
+int psdns_gpu_forcing_table(void* ctx, double* table, int32_t* kfor, int32_t* k2fo) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return set_error("null context");
+  if (kfor) *kfor = c->kfor;
+  if (k2fo) *k2fo = c->k2fo;
+  if (table) std::memcpy(table, c->forcing.table.data(), sizeof(double) * c->forcing.table.size());
   return 0;
 }
 

@@ -31,6 +31,31 @@ struct Rng {
   double ranu();
 };
 
+// PSDNS/rann2.f: Gaussian numbers by inversion of a 201-point table
+struct Rann2 {
+  std::vector<double> tab, dtab;   // 1-based
+  double p1 = 0;
+  int ntabm = 0;
+  bool ready = false;
+  void init();
+  void draw(Rng& r, double* x, int n);
+};
+
+// Eswaran-Pope forcing (PSDNS/force.f, vfuo.f, vfiuo.f, raniuo.f)
+struct EPForcing {
+  int kfor = 0, k2fo = 0, nrproc = 0, n = 0, kranf1 = 5, kranf2 = 5;
+  double kforce = 0, tforce = 0, epsfor = 0, tfiuo = 0, b11 = 1, b22 = 1, b33 = 1;
+  double t1 = 0, t2 = 0, siga = 0;
+  bool first = true;
+  std::vector<double> suo, svo, velinc, w1, w2;
+  std::vector<double> table;   // for(kfor,k2fo,k2fo,3), interleaved complex
+  Rann2 g;
+  void setup(int kfor, int nx, double kforce, double tforce, double epsfor, double tfiuo, int kranf1, int kranf2,
+             double b11, double b22, double b33);
+  void raniuo(Rng& r, double dt);
+  void step(Rng& r, double dt, int istart);
+};
+
 int set_error(const char* fmt, ...);
 
 }  // namespace psdns

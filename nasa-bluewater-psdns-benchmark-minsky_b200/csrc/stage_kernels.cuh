@@ -50,8 +50,8 @@ template <typename T> struct StageTables {
 // TB_F = columns per K5 block, TZ = z lines per K3 tile (32 B runs),
 // XT2/XT4 = x lines per K2/K4 block.
 template <typename T> struct Tiles;
-template <> struct Tiles<float> { static constexpr int TB_I = 8, TB_F = 4, TZ = 4, XT2 = 8, XT4 = 4; };
-template <> struct Tiles<double> { static constexpr int TB_I = 4, TB_F = 2, TZ = 2, XT2 = 4, XT4 = 2; };
+template <> struct Tiles<float> { static constexpr int TB_I = 8, TB_F = 4, TZ = 4, XT2 = 8, XT4 = 4, YT4 = 1; };
+template <> struct Tiles<double> { static constexpr int TB_I = 4, TB_F = 2, TZ = 2, XT2 = 4, XT4 = 2, YT4 = 1; };
 
 template <int N> __device__ __forceinline__ int kwave(int i) { return i > N / 2 ? i - N : i; }
 
@@ -269,26 +269,39 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
 // 1 = uv, 2 = d/dx(uw)+d/dz(w^2-v^2), 3 = vw (y derivatives added in K5).
 // ---------------------------------------------------------------------------
 template <typename T, int N>
-__device__ __forceinline__ void zfwd_load(const Geo& g, const C2<T>* __restrict__ uz, int slot, int y,
+__device__ __forceinline__ void zfwd_load(const Geo& g, const C2<T>* __restrict__ uz, int slot, int y0, int ny,
                                           int x0, int nl, C2<T>* buf, int L) {
+  // lines l = yy*nl + xl, rows y0+yy, columns x0+xl
   constexpr int TZ = Tiles<T>::TZ;
-  const size_t vbase = ((size_t)slot * N + y) * g.nzt;
-  for (int e = threadIdx.x; e < nl * N; e += blockDim.x) {
-    const int zt = e / (nl * TZ), rem = e % (nl * TZ), l = rem / TZ, zz = rem % TZ;
-    buf[l * L + pad32(zt * TZ + zz)] = uz[((vbase + zt) * g.kxn + x0 + l) * TZ + zz];
+  for (int yy = 0; yy < ny; yy++) {
+    const size_t vbase = ((size_t)slot * N + y0 + yy) * g.nzt;
+    C2<T>* b = buf + yy * nl * L;
+    for (int e = threadIdx.x; e < nl * N; e += blockDim.x) {
+      const int zt = e / (nl * TZ), rem = e % (nl * TZ), l = rem / TZ, zz = rem % TZ;
+      b[l * L + pad32(zt * TZ + zz)] = uz[((vbase + zt) * g.kxn + x0 + l) * TZ + zz];
+    }
   }
 }
 
 template <typename T, int N, int MODE>
 __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const C2<T>* s1, int L,
-                                           C2<T>* __restrict__ ub, int slot, int y, int x0, int x1,
+                                           C2<T>* __restrict__ ub, int slot, int y0, int ny, int x0, int x1,
                                            T b11, T b33) {
+  // the ny rows of one block column are adjacent in ub: write them together
   using C = C2<T>;
   constexpr int TB = Tiles<T>::TB_F;
+  const int nl = x1 - x0;
   const int abeg = __ldg(g.colstart + x0), aend = __ldg(g.colstart + x1);
+  const int as = abeg - (abeg % TB);                      // first block boundary
+  const int cnt = ((aend - as + TB - 1) / TB) * TB * ny;  // whole blocks x rows
   C* dst = ub + (size_t)slot * g.nab_f * N * TB;
-  for (int a = abeg + threadIdx.x; a < aend; a += blockDim.x) {
-    const int x = __ldg(g.ax + a), z = __ldg(g.az + a), l = x - x0;
+  for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+    // e -> (block q, row yy, column a): the ny rows of a block are adjacent
+    // in memory, so consecutive threads write consecutive addresses
+    const int q = e / (TB * ny), r = e % (TB * ny);
+    const int yy = r / TB, a = as + q * TB + r % TB;
+    if (a < abeg || a >= aend) continue;
+    const int x = __ldg(g.ax + a), z = __ldg(g.az + a), l = yy * nl + (x - x0);
     const int i = l * L + pad32(z);
     C out;
     if constexpr (MODE == 0) {          // i kx P1 + i b33 kz P5   (s1 = P1, s0 = P5)
@@ -304,56 +317,58 @@ __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const 
     } else {
       out = s1[i];
     }
-    dst[((size_t)(a / TB) * N + y) * TB + (a % TB)] = out;
+    dst[((size_t)(a / TB) * N + y0 + yy) * TB + (a % TB)] = out;
   }
 }
 
 template <typename T, int N>
-__global__ void __launch_bounds__(Launch<T, N, 2 * Tiles<T>::XT4>::THREADS)
+__global__ void __launch_bounds__(Launch<T, N, 2 * Tiles<T>::XT4 * Tiles<T>::YT4>::THREADS)
 k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>* __restrict__ tw_g,
        T b11, T b33) {
+  // grid (n / YT4, ceil(kxn / XT4)): YT4 adjacent y rows x XT4 x lines
   using C = C2<T>;
-  constexpr int XT = Tiles<T>::XT4;
-  constexpr int THREADS = Launch<T, N, 2 * XT>::THREADS;
+  constexpr int XT = Tiles<T>::XT4, YT = Tiles<T>::YT4, NLT = XT * YT;
+  constexpr int THREADS = Launch<T, N, 2 * NLT>::THREADS;
   constexpr int L = LS<N>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   C* s0 = tw + FFTPlan<T, N>::TWSIZE;
-  C* s1 = s0 + XT * L;
+  C* s1 = s0 + NLT * L;
   load_twiddles<T, N>(tw, tw_g);
-  const int y = blockIdx.x, x0 = blockIdx.y * XT;
+  const int y0 = blockIdx.x * YT, x0 = blockIdx.y * XT;
   const int x1 = min(x0 + XT, g.kxn);
   const int nl = x1 - x0;
+  const int nt = nl * YT;
   // round 1: P5 -> s0, P1 -> s1
-  zfwd_load<T, N>(g, uz, 4, y, x0, nl, s0, L);
-  zfwd_load<T, N>(g, uz, 0, y, x0, nl, s1, L);
+  zfwd_load<T, N>(g, uz, 4, y0, YT, x0, nl, s0, L);
+  zfwd_load<T, N>(g, uz, 0, y0, YT, x0, nl, s1, L);
   __syncthreads();
   if (nl == XT) {
-    fft_lines<T, N, THREADS>(s0, 2 * XT, L, tw);
+    fft_lines<T, N, THREADS>(s0, 2 * NLT, L, tw);
   } else {
-    fft_lines<T, N, THREADS>(s0, nl, L, tw);
-    fft_lines<T, N, THREADS>(s1, nl, L, tw);
+    fft_lines<T, N, THREADS>(s0, nt, L, tw);
+    fft_lines<T, N, THREADS>(s1, nt, L, tw);
   }
-  zfwd_store<T, N, 0>(g, s0, s1, L, ub, 0, y, x0, x1, b11, b33);
+  zfwd_store<T, N, 0>(g, s0, s1, L, ub, 0, y0, YT, x0, x1, b11, b33);
   __syncthreads();
   // round 2: P3 -> s1
-  zfwd_load<T, N>(g, uz, 2, y, x0, nl, s1, L);
+  zfwd_load<T, N>(g, uz, 2, y0, YT, x0, nl, s1, L);
   __syncthreads();
-  fft_lines<T, N, THREADS>(s1, nl, L, tw);
-  zfwd_store<T, N, 1>(g, s0, s1, L, ub, 2, y, x0, x1, b11, b33);
+  fft_lines<T, N, THREADS>(s1, nt, L, tw);
+  zfwd_store<T, N, 1>(g, s0, s1, L, ub, 2, y0, YT, x0, x1, b11, b33);
   __syncthreads();
   // round 3: P2 -> s0, P4 -> s1
-  zfwd_load<T, N>(g, uz, 1, y, x0, nl, s0, L);
-  zfwd_load<T, N>(g, uz, 3, y, x0, nl, s1, L);
+  zfwd_load<T, N>(g, uz, 1, y0, YT, x0, nl, s0, L);
+  zfwd_load<T, N>(g, uz, 3, y0, YT, x0, nl, s1, L);
   __syncthreads();
   if (nl == XT) {
-    fft_lines<T, N, THREADS>(s0, 2 * XT, L, tw);
+    fft_lines<T, N, THREADS>(s0, 2 * NLT, L, tw);
   } else {
-    fft_lines<T, N, THREADS>(s0, nl, L, tw);
-    fft_lines<T, N, THREADS>(s1, nl, L, tw);
+    fft_lines<T, N, THREADS>(s0, nt, L, tw);
+    fft_lines<T, N, THREADS>(s1, nt, L, tw);
   }
-  zfwd_store<T, N, 2>(g, s0, s1, L, ub, 1, y, x0, x1, b11, b33);
-  zfwd_store<T, N, 3>(g, s0, s1, L, ub, 3, y, x0, x1, b11, b33);
+  zfwd_store<T, N, 2>(g, s0, s1, L, ub, 1, y0, YT, x0, x1, b11, b33);
+  zfwd_store<T, N, 3>(g, s0, s1, L, ub, 3, y0, YT, x0, x1, b11, b33);
 }
 
 // ---------------------------------------------------------------------------

@@ -197,8 +197,8 @@ static int run(const psdns_params* prm, int kstep, const double* gsh, double dt,
         geo, uz, twd, stb.b11, stb.b22, stb.b33, vmx, kstep == 1 ? 1 : 0);
   }
   {
-    constexpr int TH = Launch<T, N, 2 * TL::XT4>::THREADS;
-    k_zfwd<T, N><<<dim3(N, (kxn + TL::XT4 - 1) / TL::XT4), TH, TWB + sizeof(C) * 2 * TL::XT4 * L, st>>>(
+    constexpr int TH = Launch<T, N, 2 * TL::XT4 * TL::YT4>::THREADS;
+    k_zfwd<T, N><<<dim3(N / TL::YT4, (kxn + TL::XT4 - 1) / TL::XT4), TH, TWB + sizeof(C) * 2 * TL::XT4 * TL::YT4 * L, st>>>(
         geo, uz, ub, twd, stb.b11, stb.b33);
   }
   {

@@ -41,6 +41,8 @@ EXPORTS = (
     "psdns_gpu_profile",
     "psdns_gpu_kernel_times",
     "psdns_gpu_rk_stage_noalloc",
+    "psdns_gpu_forcing_stats",
+    "psdns_gpu_forcing_table",
 )
 
 
@@ -91,6 +93,8 @@ def load():
     L.psdns_gpu_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
     L.psdns_gpu_profile.argtypes = [vp, ctypes.c_int32]
     L.psdns_gpu_kernel_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int64)]
+    L.psdns_gpu_forcing_stats.argtypes = [vp, dp, dp, dp]
+    L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
@@ -240,6 +244,25 @@ class Solver:
         _check(load().psdns_gpu_kernel_times(self._ctx, _dp(ms), cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))),
                "kernel_times")
         return ms, cnt
+
+    def forcing_table(self):
+        """for(kfor,k2fo,k2fo,3) of the last step as an array [3][k2fo][k2fo][kfor]."""
+        kf = ctypes.c_int32()
+        k2 = ctypes.c_int32()
+        _check(load().psdns_gpu_forcing_table(self._ctx, None, ctypes.byref(kf), ctypes.byref(k2)), "forcing_table")
+        tab = np.zeros(kf.value * k2.value * k2.value * 3, np.complex128)
+        _check(load().psdns_gpu_forcing_table(self._ctx, _dp(tab.view(np.float64)), None, None), "forcing_table")
+        return tab.reshape(3, k2.value, k2.value, kf.value)
+
+    def forcing_stats(self):
+        """Energy input of the last step (forcdt.f): efk per shell, eirate[3], erate."""
+        kf = ctypes.c_int32()
+        _check(load().psdns_gpu_forcing_table(self._ctx, None, ctypes.byref(kf), None), "forcing_table")
+        efk = np.zeros(kf.value, np.float64)
+        eir = np.zeros(3, np.float64)
+        er = np.zeros(1, np.float64)
+        _check(load().psdns_gpu_forcing_stats(self._ctx, _dp(efk), _dp(eir), _dp(er)), "forcing_stats")
+        return {"efk": efk, "eirate": eir, "erate": er[0]}
 
     def time_info(self):
         out = np.zeros(4, np.float64)

@@ -50,6 +50,10 @@ def lib():
         L.orc_fft.argtypes = [dp, ctypes.c_int, ctypes.c_int]
         L.orc_field_init.argtypes = [vp, ctypes.c_int, dp]
         L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_set_forcing.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_int, ctypes.c_int]
+        L.orc_get_forcing.argtypes = [vp, dp, dp]
+        L.orc_rann2.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int]
         L.orc_get_threads.restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -141,6 +145,26 @@ class Oracle:
 
     def stage(self, kstep):
         return lib().orc_stage(self._c, int(kstep))
+
+    def set_forcing(self, kforce, tforce, epsfor, tfiuo=0.0, kranf1=5, kranf2=5):
+        """Eswaran-Pope forcing (force.f) with the reference's RNG sequences."""
+        lib().orc_set_forcing(self._c, kforce, tforce, epsfor, tfiuo, kranf1, kranf2)
+        bmin = 1.0
+        self.kfor = int(kforce / bmin + 1.5)
+        self.k2fo = 2 * self.kfor - 1
+
+    def forcing(self):
+        """(for(kfor,k2fo,k2fo,3) as a Fortran-ordered complex array, efkz[kfor,3])."""
+        nf = self.kfor * self.k2fo * self.k2fo * 3
+        tab = np.zeros(nf, np.complex128)
+        ef = np.zeros(3 * self.kfor, np.float64)
+        lib().orc_get_forcing(self._c, _dp(tab.view(np.float64)), _dp(ef))
+        return tab.reshape(3, self.k2fo, self.k2fo, self.kfor), ef.reshape(self.kfor, 3)
+
+    def rann2(self, seq, n):
+        x = np.zeros(n, np.float64)
+        lib().orc_rann2(self._c, int(seq), _dp(x), int(n))
+        return x
 
     def itransform(self, ucyl, kstep=1):
         a = np.ascontiguousarray(ucyl, dtype=np.complex128)

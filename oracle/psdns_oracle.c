@@ -178,6 +178,15 @@ typedef struct {
     cx *u, *un;            /* [3][xz_tot][n] */
     fft_tw tw;
     int status;
+    /* Eswaran-Pope forcing (force.f, vfuo.f, vfiuo.f, raniuo.f, rann2.f) */
+    double kforce, tforce, epsfor, tfiuo;
+    int kranf1, kranf2, kfor, k2fo, nrproc, ffirst;
+    double t1, t2, siga;
+    double *suo, *svo, *velinc, *w1, *w2;
+    cx *forc;              /* for(kfor,k2fo,k2fo,3) */
+    double *efkz;          /* efkz(k,i), k = 1..kfor */
+    double g_tab[202], g_dtab[202], g_p1;
+    int g_ready;
 } orc_ctx;
 
 static int mask_ok(const orc_ctx *c, int a, int y)
@@ -278,6 +287,7 @@ void orc_destroy(orc_ctx *c)
     free(c->ax); free(c->az); free(c->kymax); free(c->u); free(c->un);
     free(c->sx); free(c->sy); free(c->sz); free(c->xfac); free(c->yfac); free(c->zfac);
     free(c->tw.w);
+    free(c->suo); free(c->svo); free(c->velinc); free(c->w1); free(c->w2); free(c->forc); free(c->efkz);
     free(c);
 }
 
@@ -624,6 +634,8 @@ static void wavespace(orc_ctx *c, cx *w, int ks)
     }
 }
 
+static void add_forcing(orc_ctx *c, cx *w, int stage1);
+
 /* pressure projection shared by proc4a.f:553-571 and proc4b.f:85-106 */
 static void project(orc_ctx *c, cx *u, int a, int y)
 {
@@ -665,6 +677,7 @@ static void proc4a(orc_ctx *c, cx *w, cx *un)
             project(c, w, a, y);
         }
     }
+    add_forcing(c, w, 1);
 }
 
 /* proc4b.f:38-106 (corrector and projection), :183-191 (copy), :200-205
@@ -684,6 +697,10 @@ static void proc4b(orc_ctx *c, cx *w, cx *un)
             if (a == 0 && y == 0) continue;
             project(c, w, a, y);
         }
+    }
+    add_forcing(c, w, 0);
+    #pragma omp parallel for schedule(static)
+    for (int a = 0; a < tot; a++) {
         for (int y = 0; y < n; y++) {
             if (!mask_ok(c, a, y)) continue;
             for (int i = 0; i < 3; i++) {
@@ -693,6 +710,265 @@ static void proc4b(orc_ctx *c, cx *w, cx *un)
         }
     }
     for (int i = 0; i < 3; i++) { w[i * vs] = CZERO; un[i * vs] = CZERO; }
+}
+
+
+/* ------------------------------------------------------------------------ */
+/* Eswaran-Pope forcing                                                     */
+/* ------------------------------------------------------------------------ */
+/* rann2.f:238-254 */
+static double erf_as(double x)
+{
+    double p = .3275911, a1 = .254829592, a2 = -.284496736, a3 = 1.421413741, a4 = -1.453152027, a5 = 1.061405429;
+    double t = 1. / (1. + p * fabs(x));
+    double q = t * (a1 + t * (a2 + t * (a3 + t * (a4 + t * a5))));
+    double e = 1. - q * exp(-x * x);
+    if (x < 0.) e = -e;
+    return e;
+}
+
+/* rann2.f:149-226: inverse-distribution table of the standard normal */
+static void rann2_init(orc_ctx *c)
+{
+    const int ntab = 201, ntabm = 200, ntabmm = 199, ntsq = 201 * 201, ntabh = 100;
+    double pi = 3.1415927, rtpii = 0.3989423, rti = 0.7071068;
+    double *tab = c->g_tab, *dtab = c->g_dtab;
+    double dy = 1. / (double)ntabm;
+    double p3 = ntsq * 5.800e-6 - ntab * 4.35160e-3 - 1.7006542;
+    double p2 = ntsq * 6.035e-6 - ntab * 4.46257e-3 - 1.8738435;
+    double p1 = ntabm * exp(-p2 * p2 / 2.) / sqrt(2. * pi);
+    double xmin = 2. * pi * p1 * p1 * 1.e-14;
+    xmin = -log(xmin);
+    xmin = -sqrt(xmin);
+    double xmax = -xmin;
+    c->g_p1 = p1;
+    tab[1] = xmin; tab[2] = p2; tab[3] = p3;
+    tab[ntab] = xmax; tab[ntabm] = -p2; tab[ntabmm] = -p3;
+    double y = 2. * dy;
+    double xx = tab[3] + dy * (xmax - xmin);
+    for (int i = 4; i <= ntabh; i++) {
+        y = y + dy;
+        double xxmin = tab[i - 1], xxmax = xmax;
+        for (int iter = 1; iter <= 50; iter++) {
+            double yy = 0.5 * (1. + erf_as(rti * xx));
+            double err = yy - y;
+            if (fabs(err) < 1.e-6) break;
+            if (err > 0.) xxmax = xx;
+            if (err < 0.) xxmin = xx;
+            double fd = rtpii * exp(-0.5 * xx * xx);
+            xx = xx + err / (fd > 1.e-10 ? fd : 1.e-10);
+            if (xx <= xxmin || xx >= xxmax) xx = 0.5 * (xxmin + xxmax);
+        }
+        tab[i] = xx;
+    }
+    for (int i = 1; i <= ntabh; i++) tab[ntab - i + 1] = -tab[i];
+    tab[ntabh + 1] = 0.;
+    for (int i = 1; i <= ntabm; i++) dtab[i] = tab[i + 1] - tab[i];
+    c->g_ready = 1;
+}
+
+/* rann2.f:114-143 with ranu2.f/vrand.f as the uniform source (the ranu LCG) */
+static void rann2(orc_ctx *c, double *x, int n)
+{
+    if (!c->g_ready) rann2_init(c);
+    const int ntabm = 200;
+    double pi = 3.1415927, azer = 1.e-20, p1 = c->g_p1;
+    for (int j = 0; j < n; j++) x[j] = rng_ranu(&c->rng);
+    for (int j = 0; j < n; j++) {
+        double y = x[j] * ntabm + 1;
+        int i = (int)y;
+        if (i == 1) {
+            double y1 = x[j];
+            y1 = 2. * pi * p1 * p1 * y1 * y1;
+            if (y1 <= 0.) y1 = azer;
+            x[j] = -sqrt(-log(y1));
+        } else if (i == ntabm) {
+            double y1 = 1. - x[j];
+            y1 = 2. * pi * p1 * p1 * y1 * y1;
+            x[j] = sqrt(-log(y1));
+        } else {
+            y = y - i;
+            x[j] = c->g_tab[i] + y * c->g_dtab[i];
+        }
+    }
+}
+
+void orc_set_forcing(orc_ctx *c, double kforce, double tforce, double epsfor, double tfiuo, int kranf1, int kranf2)
+{
+    c->kforce = kforce; c->tforce = tforce; c->epsfor = epsfor; c->tfiuo = tfiuo;
+    c->kranf1 = kranf1; c->kranf2 = kranf2;
+    double bmin = sqrt(c->b11) < sqrt(c->b22) + sqrt(c->b33) ? sqrt(c->b11) : sqrt(c->b22) + sqrt(c->b33);
+    c->kfor = (int)(kforce / bmin + 1.5);                 /* param_set.f:33 */
+    c->k2fo = 2 * c->kfor - 1;
+    c->nrproc = 4 * c->kfor * c->k2fo * c->k2fo;          /* param_set.f:87 */
+    c->ffirst = 1;
+    c->suo = (double *)calloc((size_t)c->nrproc, sizeof(double));
+    c->svo = (double *)calloc((size_t)c->nrproc, sizeof(double));
+    c->velinc = (double *)calloc((size_t)c->nrproc, sizeof(double));
+    c->w1 = (double *)calloc((size_t)c->nrproc, sizeof(double));
+    c->w2 = (double *)calloc((size_t)c->nrproc, sizeof(double));
+    c->forc = (cx *)calloc((size_t)c->kfor * c->k2fo * c->k2fo * 3, sizeof(cx));
+    c->efkz = (double *)calloc((size_t)3 * (c->kfor + 2), sizeof(double));
+}
+
+/* raniuo.f:56-109 */
+static void raniuo(orc_ctx *c, double dtv)
+{
+    int n = c->nrproc;
+    if (c->t1 <= 0. || c->t2 <= 0.) return;
+    double diff = fabs(c->t1 / c->t2 - 1.);
+    if (diff < 0.05) c->t1 = 0.95 * c->t2;
+    if (dtv < 0.) {
+        double rr = c->t1 / (c->t1 + c->t2), be = sqrt(rr), ga = sqrt(1. - rr);
+        rann2(c, c->w1, n);
+        rann2(c, c->w2, n);
+        for (int i = 0; i < n; i++) { c->suo[i] = c->w1[i]; c->svo[i] = be * c->w1[i] + ga * c->w2[i]; }
+        return;
+    }
+    double om1 = 1. / c->t1, om2 = 1. / c->t2, s = om1 + om2, d = om2 - om1;
+    double a = exp(-om1 * dtv), b = exp(-om2 * dtv), cc = (a - b) / d;
+    double sco = cc * sqrt(s * om2), r = sqrt(om2 / s);
+    double uu = 1. - a * a;
+    double vv = 1. - b * b + 4. * om1 * om2 * b * cc / d - om2 * s * (a * a - b * b) / (d * d);
+    double uv = r * (1. - a * b - s * a * cc);
+    double al = sqrt(uu), be = uv / al;
+    double g2 = vv - be * be;
+    double ga = sqrt(g2 > 0. ? g2 : 0.);
+    rann2(c, c->w1, n);
+    rann2(c, c->w2, n);
+    for (int i = 0; i < n; i++) {
+        c->svo[i] = b * c->svo[i] + sco * c->suo[i] + be * c->w1[i] + ga * c->w2[i];
+        c->suo[i] = a * c->suo[i] + al * c->w1[i];
+    }
+}
+
+/* force.f:60-166 with vfuo.f:25-55 / vfiuo.f:33-57 */
+static void force(orc_ctx *c)
+{
+    if (c->kforce == 0.) return;
+    int n = c->nrproc, kfor = c->kfor, k2fo = c->k2fo, nn = c->n;
+    double dt = c->dt;
+    if (c->tforce * c->tfiuo == 0.) {
+        if (c->ffirst) {
+            c->ffirst = 0;
+            rng_ranseq(&c->rng, c->kranf1);
+            rann2(c, c->suo, n);
+        }
+        double exp1 = 0.;
+        if (c->tforce > 0.05 * dt) exp1 = exp(-dt / c->tforce);
+        double exp2 = exp1 * exp1;
+        double rana = sqrt(1. - exp2);
+        double ranua = sqrt(c->epsfor * c->tforce) * ((1. - exp1) * (1. - exp1)) / sqrt(1. - exp2);
+        double ranub = (c->epsfor * (2. * dt + c->tforce * (-3. + 4. * exp1 - exp2)) - ranua * ranua);
+        ranub = sqrt(ranub > 0. ? ranub : 0.);
+        double ranud = sqrt(c->epsfor * c->tforce) * (1. - exp1);
+        rng_ranseq(&c->rng, c->kranf2);
+        rann2(c, c->w1, n);
+        rann2(c, c->w2, n);
+        for (int i = 0; i < n; i++) {
+            c->velinc[i] = ranud * c->suo[i] + ranua * c->w1[i] + ranub * c->w2[i];
+            c->suo[i] = exp1 * c->suo[i] + rana * c->w1[i];
+        }
+    } else {
+        if (c->ffirst) {
+            c->ffirst = 0;
+            double q = sqrt(1. - 4. * fabs(c->tfiuo) * fabs(c->tfiuo));
+            c->t1 = 0.5 * c->tforce * (1. + q);
+            c->t2 = 0.5 * c->tforce * (1. - q);
+            c->siga = sqrt(c->epsfor / c->tforce);
+            if (c->tfiuo > 0.) { rng_ranseq(&c->rng, c->kranf1); raniuo(c, -1.); }
+        }
+        rng_ranseq(&c->rng, c->kranf2);
+        raniuo(c, dt);
+        double fmult = c->siga * dt;
+        for (int i = 0; i < n; i++) c->velinc[i] = c->svo[i] * fmult;
+    }
+    double s1 = sqrt(c->b11), s2 = sqrt(c->b22), s3 = sqrt(c->b33);
+#define FOR(x, y, z, i) c->forc[((((size_t)(i) - 1) * k2fo + ((z) - 1)) * k2fo + ((y) - 1)) * kfor + ((x) - 1)]
+    for (int z = 1; z <= k2fo; z++)
+        for (int y = 1; y <= k2fo; y++) {
+            int iy = y + (y / (kfor + 1)) * (nn - k2fo), iz = z + (z / (kfor + 1)) * (nn - k2fo);
+            double k2u = s2 * c->ky[iy - 1], k3u = s3 * c->kz[iz - 1];
+            for (int x = 1; x <= kfor; x++) {
+                size_t o = 2 * ((size_t)(x - 1) + (size_t)kfor * ((y - 1) + (size_t)k2fo * (z - 1)));
+                cx alpha = cmk(c->velinc[2 * o], c->velinc[2 * o + 1]);
+                cx beta = cmk(c->velinc[2 * o + 2], c->velinc[2 * o + 3]);
+                double k1u = s1 * c->kx[x - 1];
+                double k = sqrt(k1u * k1u + k2u * k2u + k3u * k3u);
+                double k12 = sqrt(k1u * k1u + k2u * k2u);
+                if (k > c->kforce || k == 0.) {
+                    FOR(x, y, z, 1) = CZERO; FOR(x, y, z, 2) = CZERO; FOR(x, y, z, 3) = CZERO;
+                } else if (k12 == 0.) {
+                    FOR(x, y, z, 1) = cmk(alpha.re / s1, alpha.im / s1);
+                    FOR(x, y, z, 2) = cmk(beta.re / s2, beta.im / s2);
+                    FOR(x, y, z, 3) = CZERO;
+                } else {
+                    double d1 = k * k12 * s1, d2 = k * k12 * s2, d3 = k * s3;
+                    cx t1 = cadd(cscale(k2u, cscale(k, alpha)), cscale(k3u, cscale(k1u, beta)));
+                    cx t2 = csub(cscale(k3u, cscale(k2u, beta)), cscale(k1u, cscale(k, alpha)));
+                    cx t3 = cscale(k12, beta);
+                    FOR(x, y, z, 1) = cmk(t1.re / d1, t1.im / d1);
+                    FOR(x, y, z, 2) = cmk(t2.re / d2, t2.im / d2);
+                    FOR(x, y, z, 3) = cmk(-(t3.re / d3), -(t3.im / d3));
+                }
+            }
+        }
+    for (int i = 1; i <= 3; i++) {
+        for (int y = kfor + 1; y <= k2fo; y++) FOR(1, y, 1, i) = cconj(FOR(1, k2fo + 2 - y, 1, i));
+        for (int z = kfor + 1; z <= k2fo; z++) {
+            FOR(1, 1, z, i) = cconj(FOR(1, 1, k2fo + 2 - z, i));
+            for (int y = 2; y <= k2fo; y++) FOR(1, y, z, i) = cconj(FOR(1, k2fo + 2 - y, k2fo + 2 - z, i));
+        }
+    }
+#undef FOR
+}
+
+/* the forcing addition of proc4a.f:588-651 (stage 1, with efkz and the
+ * |k| <= kforce test) and proc4b.f:118-163 (stage 2) */
+static void add_forcing(orc_ctx *c, cx *w, int stage1)
+{
+    if (c->kforce == 0.) return;
+    int n = c->n, tot = c->xz_tot, kfor = c->kfor, k2fo = c->k2fo;
+    size_t vs = (size_t)tot * n;
+    if (stage1) memset(c->efkz, 0, sizeof(double) * 3 * (kfor + 2));
+    for (int a = 0; a < tot; a++) {
+        int x = c->ax[a], z = c->az[a];   /* 0-based */
+        int zz = z + 1, iz;
+        if (zz <= kfor) iz = zz; else if (zz >= n + 2 - kfor) iz = zz - n + k2fo; else iz = 0;
+        if (iz == 0 || x + 1 > kfor) continue;
+        for (int i = 0; i < 3; i++)
+            for (int y = 0; y < n; y++) {
+                if (!mask_ok(c, a, y)) continue;
+                int yy = y + 1, iy;
+                if (yy <= kfor) iy = yy; else if (yy >= n + 2 - kfor) iy = yy - n + k2fo; else iy = 0;
+                if (iy == 0) continue;
+                cx f = c->forc[(((size_t)i * k2fo + (iz - 1)) * k2fo + (iy - 1)) * kfor + x];
+                size_t o = i * vs + (size_t)a * n + y;
+                if (stage1) {
+                    double rks = c->kx[x] * c->kx[x] * c->b11 + c->ky[y] * c->ky[y] * c->b22 + c->kz[z] * c->kz[z] * c->b33;
+                    if (!(rks <= c->kforce * c->kforce)) continue;
+                    int k = (int)(sqrt(rks) + 1.5);
+                    double term = w[o].re * f.re + w[o].im * f.im;
+                    double tfact = (x == 0) ? 1. : 2.;
+                    double ssq = i == 0 ? c->b11 : (i == 1 ? c->b22 : c->b33);
+                    c->efkz[(k - 1) * 3 + i] += 2. * term * tfact * ssq;
+                }
+                w[o] = cadd(w[o], f);
+            }
+    }
+}
+
+void orc_get_forcing(orc_ctx *c, double *table, double *efkz)
+{
+    if (table) memcpy(table, c->forc, sizeof(cx) * (size_t)c->kfor * c->k2fo * c->k2fo * 3);
+    if (efkz) memcpy(efkz, c->efkz, sizeof(double) * 3 * (size_t)c->kfor);
+}
+
+/* Gaussian numbers of rann2 from the given LCG sequence (tests) */
+void orc_rann2(orc_ctx *c, int seq, double *x, int n)
+{
+    rng_ranseq(&c->rng, seq);
+    rann2(c, x, n);
 }
 
 /* One RK stage (timestep_module.f:70-481, CLEAN velocity path, nc = 0).
@@ -714,7 +990,7 @@ static int rk_stage(orc_ctx *c, int kstep)
     transform(c, p, w);
     free(p);
     int err = 0;
-    if (kstep == 1) err = step_control(c);
+    if (kstep == 1) { err = step_control(c); force(c); }
     wavespace(c, w, ks);
     if (kstep == 1) proc4a(c, w, c->un);
     else proc4b(c, w, c->un);

@@ -128,3 +128,40 @@ def test_device_field_init_matches_oracle(oracle_mod, gpu_mod, prec, tol):
     assert rel_l2(got, ref) < tol
     np.testing.assert_array_equal(s.get_state(gpu_mod.FIELD_U), got)
     o.close(); s.close()
+
+
+@pytest.mark.parametrize("tfiuo,cfl", [(0.0, -1.0), (0.4, -1.0), (0.0, np.pi), (0.4, np.pi)])
+def test_forced_steps_match_oracle(oracle_mod, gpu_mod, tfiuo, cfl):
+    """Eswaran-Pope forcing (force.f with vfuo.f, or vfiuo.f + raniuo.f), FP64
+    device state.  With a fixed dt the forcing table depends only on the RNG
+    path and must be bit-identical; with adaptive dt (cfl = pi, Courant number
+    0.5) it also depends on dt = cfl/velmax, whose device value differs from
+    the oracle's in the last bits, so the table is compared to 1e-11."""
+    n, nu = 32, 0.02
+    kforce, tforce = 2.99, 0.5
+    epsfor = 0.1 / (4.0 * (4.0 * np.pi / 3.0) * kforce ** 3)
+    dt = 0.004 if cfl < 0 else 0.0
+    o = oracle_mod.Oracle(n, nu, cfl=cfl, dt=dt, kshift=1)
+    o.set_forcing(kforce, tforce, epsfor, tfiuo)
+    un0 = o.field_init(77)
+    o.set_state(un0)
+    s = gpu_mod.Solver(n=n, precision=gpu_mod.PREC_FP64, viscos=nu, cfl=cfl, dt=dt, kshift=1,
+                       kforce=kforce, tforce=tforce, epsfor=epsfor, tfiuo=tfiuo)
+    s.set_state(un0)
+    for step in range(3):
+        o.step()
+        info = s.step()
+        so = o.scalars()
+        assert abs(info["dt"] - so["dt"]) <= 1e-12 * so["dt"]
+        tab_o, ef_o = o.forcing()
+        tab_g = s.forcing_table()
+        if cfl < 0:
+            np.testing.assert_array_equal(tab_g, tab_o)
+        else:
+            np.testing.assert_allclose(tab_g, tab_o, rtol=1e-11, atol=1e-11 * np.abs(tab_o).max())
+        st = s.forcing_stats()
+        efk_o = 0.5 * ef_o.sum(axis=1) / so["dt"]
+        np.testing.assert_allclose(st["efk"], efk_o, rtol=1e-9, atol=1e-15)
+    _, un_o = o.get_state()
+    assert rel_l2(s.get_state(gpu_mod.FIELD_UN), un_o) < 1e-11
+    o.close(); s.close()

@@ -140,3 +140,37 @@ def test_lcg_stream(oracle_mod):
     np.testing.assert_array_equal(g[:, 0], draws[:3])
     np.testing.assert_array_equal(g[:, 1], np.fmod(np.array(draws[:3]) + 0.5, 1.0))
     o.close()
+
+
+def test_rann2_moments(oracle_mod):
+    """rann2.f's table is tuned for variance 1 and flatness 3 within about 1%
+    (rann2.f:68-75); odd moments vanish by the table's symmetry."""
+    o = oracle_mod.Oracle(16, 0.01, kshift=4, seed_input=122929298)
+    x = o.rann2(5, 400000)
+    assert abs(x.mean()) < 5e-3
+    assert abs(x.var() - 1.0) < 0.02
+    assert abs(np.mean(x ** 4) / x.var() ** 2 - 3.0) < 0.06
+    o.close()
+
+
+def test_forcing_table_is_solenoidal_and_limited_to_kforce(oracle_mod):
+    n = 32
+    o = oracle_mod.Oracle(n, 0.01, cfl=-1, dt=0.005, kshift=4)
+    kforce = 2.99
+    o.set_forcing(kforce, 0.5, 2e-4, 0.0)
+    o.set_state(o.field_init(3))
+    o.step()
+    tab, ef = o.forcing()
+    kf, k2 = o.kfor, o.k2fo
+    kw = lambda i: i if i < kf else i - k2
+    for z in range(k2):
+        for y in range(k2):
+            for x in range(kf):
+                k = np.array([x, kw(y), kw(z)], float)
+                f = tab[:, z, y, x]
+                if np.linalg.norm(k) > kforce or np.linalg.norm(k) == 0:
+                    assert np.all(f == 0)
+                else:
+                    assert abs(np.dot(k, f)) < 1e-14 * (1 + np.abs(f).max())
+    assert np.abs(tab).max() > 0
+    o.close()
