@@ -111,6 +111,15 @@ int psdns_gpu_step(void *ctx, double *info);
 int psdns_gpu_rk_stage(void *ctx, int32_t kstep, const double *gsh, const double *dt,
                        const double *forcing, double *velmax_out);
 
+/* Shell spectra in FP64 (replaces PSDNS/homogeneous/sptr.f:139-400 for the
+ * velocity): shells ik = int(|k| + 1.5), n of them (mxyz, comsp_set.f:14).
+ * which = PSDNS_FIELD_UN (as sptr(un,...)) or PSDNS_FIELD_U.  Outputs (each
+ * may be NULL): ek[n] = E(k), dk[n] = D(k) (2 nu k^2 E, shell 1 zeroed as in
+ * sptr.f:355-357), eijk[n*6] = sum tfact Re(u_i u_j*) per shell for ij = 11,
+ * 12, 13, 22, 23, 33, stats[7] = tke, epsilon, skewness (sptr.f:365),
+ * Kolmogorov length, velocity and time, integral scale (sptr.f:387-390). */
+int psdns_gpu_spectra(void *ctx, int32_t which, double *ek, double *dk, double *eijk, double *stats);
+
 /* Eswaran-Pope forcing diagnostics of the last step (PSDNS/forcdt.f:18-41):
  * efk[kfor] energy input per shell, eirate[3] per component, *erate total
  * (each pointer may be NULL).  Error if the context is unforced. */

@@ -1,0 +1,56 @@
+// spectra.cuh -- FP64 shell spectra of the velocity state on the device.
+//
+// Restates homogeneous/sptr.f:139-193 (per-mode products tfact*Re(u_i u_j*)
+// binned by shell ik = int(|k| + 1.5), dissipation and skewness moments scaled
+// by 2 nu, :235-237) and the derived statistics of :350-400 (E(k), D(k), TKE,
+// epsilon, spectral derivative skewness, Kolmogorov scales, integral scale).
+// All accumulation is FP64 whatever the state precision: each block keeps
+// shell histograms in shared memory (FP64 shared atomics) and adds them to
+// the global sums once.
+#pragma once
+#include "stage_kernels.cuh"
+
+namespace psdns {
+
+// per shell: E_ij (6: 11,12,13,22,23,33), D_ii sum, S_ii sum, ekk
+constexpr int kSpecVals = 9;
+
+template <typename T>
+__global__ void k_spectra(Geo g, const C2<T>* __restrict__ un, double b11, double b22, double b33,
+                          int nshell, double* __restrict__ out) {
+  extern __shared__ double hist[];   // [nshell][kSpecVals]
+  const int n = g.n;
+  for (int i = threadIdx.x; i < nshell * kSpecVals; i += blockDim.x) hist[i] = 0.0;
+  __syncthreads();
+  const size_t vs = (size_t)g.xz_tot * n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < vs; i += (size_t)gridDim.x * blockDim.x) {
+    const int a = (int)(i / n), y = (int)(i % n);
+    if (!mask_ok(g, a, y, n)) continue;
+    const int x = __ldg(g.ax + a), z = __ldg(g.az + a);
+    const double kx = x, ky = y > n / 2 ? y - n : y, kz = z > n / 2 ? z - n : z;
+    const double tf = x == 0 ? 1.0 : 2.0;
+    // sptr.f:85-97: Nyquist rows contribute no wavenumber (masked anyway)
+    const double rk2 = b11 * kx * kx + b22 * ky * ky + b33 * kz * kz;
+    const int ik = (int)(sqrt(rk2) + 1.5) - 1;
+    if (ik < 0 || ik >= nshell) continue;
+    const C2<T> u1 = un[i], u2 = un[vs + i], u3 = un[2 * vs + i];
+    const double a1 = u1.x, c1 = u1.y, a2 = u2.x, c2 = u2.y, a3 = u3.x, c3 = u3.y;
+    const double e11 = tf * (a1 * a1 + c1 * c1), e22 = tf * (a2 * a2 + c2 * c2), e33 = tf * (a3 * a3 + c3 * c3);
+    double* h = hist + ik * kSpecVals;
+    atomicAdd(h + 0, e11);
+    atomicAdd(h + 1, tf * (a1 * a2 + c1 * c2));
+    atomicAdd(h + 2, tf * (a1 * a3 + c1 * c3));
+    atomicAdd(h + 3, e22);
+    atomicAdd(h + 4, tf * (a2 * a3 + c2 * c3));
+    atomicAdd(h + 5, e33);
+    const double tr = e11 + e22 + e33;
+    atomicAdd(h + 6, rk2 * tr);
+    atomicAdd(h + 7, rk2 * rk2 * tr);
+    if (rk2 != 0.) atomicAdd(h + 8, (e11 * b11 + e22 * b22 + e33 * b33) / sqrt(rk2));
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nshell * kSpecVals; i += blockDim.x)
+    if (hist[i] != 0.0) atomicAdd(out + i, hist[i]);
+}
+
+}  // namespace psdns

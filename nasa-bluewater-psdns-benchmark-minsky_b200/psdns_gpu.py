@@ -42,6 +42,7 @@ EXPORTS = (
     "psdns_gpu_kernel_times",
     "psdns_gpu_rk_stage_noalloc",
     "psdns_gpu_forcing_stats",
+    "psdns_gpu_spectra",
     "psdns_gpu_forcing_table",
 )
 
@@ -94,6 +95,7 @@ def load():
     L.psdns_gpu_profile.argtypes = [vp, ctypes.c_int32]
     L.psdns_gpu_kernel_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int64)]
     L.psdns_gpu_forcing_stats.argtypes = [vp, dp, dp, dp]
+    L.psdns_gpu_spectra.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
     for name in EXPORTS:
@@ -244,6 +246,13 @@ class Solver:
         _check(load().psdns_gpu_kernel_times(self._ctx, _dp(ms), cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))),
                "kernel_times")
         return ms, cnt
+
+    def spectra(self, which=FIELD_UN):
+        """FP64 shell spectra (sptr.f): (ek[n], dk[n], eijk[n,6], stats dict)."""
+        n = self.n
+        ek = np.zeros(n); dk = np.zeros(n); e6 = np.zeros(n * 6); st = np.zeros(7)
+        _check(load().psdns_gpu_spectra(self._ctx, int(which), _dp(ek), _dp(dk), _dp(e6), _dp(st)), "spectra")
+        return ek, dk, e6.reshape(n, 6), dict(zip(["tke", "eps", "skew", "klen", "kvel", "ktime", "ekl"], st))
 
     def forcing_table(self):
         """for(kfor,k2fo,k2fo,3) of the last step as an array [3][k2fo][k2fo][kfor]."""

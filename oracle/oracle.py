@@ -55,6 +55,7 @@ def lib():
         L.orc_get_forcing.argtypes = [vp, dp, dp]
         L.orc_rann2.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int]
         L.orc_get_threads.restype = ctypes.c_int
+        L.orc_spectra.argtypes = [vp, ctypes.c_int, dp, dp, dp, dp]
         _LIB = L
     return _LIB
 
@@ -160,6 +161,13 @@ class Oracle:
         ef = np.zeros(3 * self.kfor, np.float64)
         lib().orc_get_forcing(self._c, _dp(tab.view(np.float64)), _dp(ef))
         return tab.reshape(3, self.k2fo, self.k2fo, self.kfor), ef.reshape(self.kfor, 3)
+
+    def spectra(self, which=1):
+        """sptr.f restated: (ek[n], dk[n], eijk[n,6], stats dict) of un (which=1) or u."""
+        n = self.n
+        ek = np.zeros(n); dk = np.zeros(n); e6 = np.zeros(n * 6); st = np.zeros(7)
+        lib().orc_spectra(self._c, int(which), _dp(ek), _dp(dk), _dp(e6), _dp(st))
+        return ek, dk, e6.reshape(n, 6), dict(zip(["tke", "eps", "skew", "klen", "kvel", "ktime", "ekl"], st))
 
     def rann2(self, seq, n):
         x = np.zeros(n, np.float64)

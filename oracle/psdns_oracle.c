@@ -1130,3 +1130,73 @@ void orc_field_init(orc_ctx *c, int seed, double *out /* [3][xz_tot][n] complex 
         }
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Shell spectra: homogeneous/sptr.f:139-193 (sums), :235-237 (2 nu),       */
+/* :350-400 (ek, dk, tke, epslon, skew, Kolmogorov scales, integral scale). */
+/* which = 0: u, 1: un.  ek, dk: [n]; stats: [7].                           */
+/* ------------------------------------------------------------------------ */
+void orc_spectra(orc_ctx *c, int which, double *ek, double *dk, double *eijk, double *stats)
+{
+    int n = c->n, tot = c->xz_tot, ns = n;
+    size_t vs = (size_t)tot * n;
+    const cx *u = which == 0 ? c->u : c->un;
+    double *e6 = (double *)calloc((size_t)ns * 6, sizeof(double));
+    double *d1 = (double *)calloc((size_t)ns, sizeof(double));
+    double *s1 = (double *)calloc((size_t)ns, sizeof(double));
+    double *ekk = (double *)calloc((size_t)ns, sizeof(double));
+    for (int a = 0; a < tot; a++) {
+        int x = c->ax[a], z = c->az[a];
+        double tfact = (x == 0) ? 1. : 2.;
+        for (int y = 0; y < n; y++) {
+            if (!mask_ok(c, a, y)) continue;
+            double kx2 = c->b11 * c->kx[x] * c->kx[x];
+            double ky2 = (y == n / 2) ? 0. : c->b22 * c->ky[y] * c->ky[y];
+            double kz2 = (z == n / 2) ? 0. : c->b33 * c->kz[z] * c->kz[z];
+            double rk2 = kx2 + ky2 + kz2;
+            int ik = (int)(sqrt(rk2) + 1.5);
+            if (ik > ns) continue;
+            cx v[3];
+            for (int i = 0; i < 3; i++) v[i] = u[i * vs + (size_t)a * n + y];
+            int ij = 0;
+            for (int i = 0; i < 3; i++)
+                for (int j = i; j < 3; j++) {
+                    double uiuj = v[i].re * v[j].re + v[i].im * v[j].im;
+                    double term = tfact * uiuj;
+                    e6[(ik - 1) * 6 + ij] += term;
+                    if (i == j) {
+                        d1[ik - 1] += rk2 * term;
+                        s1[ik - 1] += rk2 * term * rk2;
+                        double ssq = i == 0 ? c->b11 : (i == 1 ? c->b22 : c->b33);
+                        if (rk2 != 0.) ekk[ik - 1] += term / sqrt(rk2) * ssq;
+                    }
+                    ij++;
+                }
+        }
+    }
+    double nu = c->viscos, tke = 0, eps = 0, skew = 0, ekl = 0;
+    for (int k = 0; k < ns; k++) {
+        double e = (e6[k * 6 + 0] + e6[k * 6 + 3] + e6[k * 6 + 5]) * 0.5;
+        double d = (2 * nu * d1[k]) * 0.5;
+        double sk = (2 * nu * s1[k]) * 0.5;
+        if (k == 0) { e = 0; d = 0; }
+        if (ek) ek[k] = e;
+        if (dk) dk[k] = d;
+        if (eijk) for (int j = 0; j < 6; j++) eijk[k * 6 + j] = e6[k * 6 + j];
+        tke += e; eps += d; skew += sk;
+        if (k < n / 2) ekl += ekk[k] / 2.;
+    }
+    double pi = 4. * atan(1.), klen = 0, kvel = 0, ktime = 0;
+    if (eps > 0) {
+        skew = 2. / 35. * pow(15. * nu / eps, 1.5) * skew;
+        klen = pow(nu * nu * nu / eps, .25);
+        kvel = pow(nu * eps, .25);
+        ktime = pow(nu / eps, .5);
+    }
+    ekl = 1.5 * pi / (2 * tke) * ekl;
+    if (stats) {
+        stats[0] = tke; stats[1] = eps; stats[2] = skew; stats[3] = klen; stats[4] = kvel; stats[5] = ktime;
+        stats[6] = ekl;
+    }
+    free(e6); free(d1); free(s1); free(ekk);
+}

@@ -165,3 +165,25 @@ def test_forced_steps_match_oracle(oracle_mod, gpu_mod, tfiuo, cfl):
     _, un_o = o.get_state()
     assert rel_l2(s.get_state(gpu_mod.FIELD_UN), un_o) < 1e-11
     o.close(); s.close()
+
+
+@pytest.mark.parametrize("prec,tol", [(1, 1e-12), (0, 1e-5)])
+def test_spectra_match_oracle(oracle_mod, gpu_mod, prec, tol):
+    """FP64 shell sums on the device (sptr.f) against the oracle after 2 steps."""
+    n, nu = 32, 0.01
+    o = oracle_mod.Oracle(n, nu, cfl=-1, dt=0.005, kshift=1)
+    un0 = o.field_init(5)
+    o.set_state(un0)
+    s = gpu_mod.Solver(n=n, precision=prec, viscos=nu, cfl=-1, dt=0.005, kshift=1)
+    s.set_state(un0)
+    for _ in range(2):
+        o.step()
+        s.step()
+    ek_o, dk_o, e6_o, st_o = o.spectra(1)
+    ek_g, dk_g, e6_g, st_g = s.spectra(gpu_mod.FIELD_UN)
+    m = ek_o > 1e-10 * ek_o.max()
+    np.testing.assert_allclose(ek_g[m], ek_o[m], rtol=tol)
+    np.testing.assert_allclose(dk_g[m], dk_o[m], rtol=tol)
+    for k in ("tke", "eps", "skew", "klen", "ekl"):
+        assert abs(st_g[k] - st_o[k]) <= tol * abs(st_o[k]), k
+    o.close(); s.close()

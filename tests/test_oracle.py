@@ -174,3 +174,30 @@ def test_forcing_table_is_solenoidal_and_limited_to_kforce(oracle_mod):
                     assert abs(np.dot(k, f)) < 1e-14 * (1 + np.abs(f).max())
     assert np.abs(tab).max() > 0
     o.close()
+
+
+def test_spectra_against_numpy(oracle_mod):
+    """sptr.f restated: E(k) per shell int(|k|+1.5), epsilon = 2 nu sum k^2 E."""
+    n, nu = 32, 0.01
+    o = oracle_mod.Oracle(n, nu, kshift=4)
+    g = o.geometry()
+    un = o.field_init(11)
+    o.set_state(un)
+    ek, dk, e6, st = o.spectra(1)
+    F = np.zeros((3, n, n, n // 2 + 1), complex)
+    for x in range(o.kxn):
+        for a in range(g["colstart"][x], g["colstart"][x + 1]):
+            F[:, :, g["az"][a], x] = un[:, a, :]
+    ky = np.fft.fftfreq(n, 1.0 / n)
+    kx = np.arange(n // 2 + 1)
+    K2 = kx[None, None, :] ** 2 + ky[:, None, None] ** 2 + ky[None, :, None] ** 2
+    tf = np.where(kx == 0, 1.0, 2.0)[None, None, :]
+    e = 0.5 * tf * np.sum(np.abs(F) ** 2, axis=0)
+    ik = (np.sqrt(K2) + 1.5).astype(int) - 1
+    E = np.bincount(ik.ravel(), weights=e.ravel(), minlength=n)[:n]
+    E[0] = 0
+    np.testing.assert_allclose(ek, E, rtol=1e-12, atol=1e-15)
+    assert abs(st["tke"] - 1.5) < 1e-12
+    eps = 2 * nu * np.sum(K2 * e)
+    assert abs(st["eps"] - eps) < 1e-12 * eps
+    o.close()
