@@ -111,6 +111,20 @@ int psdns_gpu_step(void *ctx, double *info);
 int psdns_gpu_rk_stage(void *ctx, int32_t kstep, const double *gsh, const double *dt,
                        const double *forcing, double *velmax_out);
 
+/* Lagrangian particles (replaces the LAG_LOCAL hooks: partin positions in,
+ * partsp.f RK2 with spcal_local.f cubic-spline interpolation).  pos is
+ * column-major (np,3) = pp(np,1:3): FP64 positions in grid units, grid plane
+ * i (1-based) at 1 + (i-1) + gsh(.,1) (PSDNS/hooks/LAG_LOCAL/partsp.f:44-51).
+ * Each psdns_gpu_step then advances them at stage 1 with the spline of the
+ * stage-1 velocity field, lagging the Eulerian field by one step
+ * (partsp.f:231-299,405-412); the first step only interpolates velocities.
+ * set replaces any previous particles; np = 0 removes them. */
+int psdns_gpu_particles_set(void *ctx, int64_t np, const double *pos);
+
+/* Positions pp(np,1:3) and velocities pp(np,4:6), column-major (np,3) each
+ * (either may be NULL). */
+int psdns_gpu_particles_get(void *ctx, double *pos, double *vel);
+
 /* Shell spectra in FP64 (replaces PSDNS/homogeneous/sptr.f:139-400 for the
  * velocity): shells ik = int(|k| + 1.5), n of them (mxyz, comsp_set.f:14).
  * which = PSDNS_FIELD_UN (as sptr(un,...)) or PSDNS_FIELD_U.  Outputs (each

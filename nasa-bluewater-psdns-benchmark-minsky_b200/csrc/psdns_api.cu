@@ -154,6 +154,12 @@ struct Ctx {
   double time = 0, dt = 0, dt0 = 0, dt2 = 0, velmax = 0;
   int kfor = 0, k2fo = 0;
   EPForcing forcing;
+  // Lagrangian particles (positions/velocities FP64, spline coefficients in
+  // the state precision, interleaved as 4-vectors [y][z][x])
+  long long np = 0;
+  double *d_pos = nullptr, *d_vel = nullptr;
+  void *d_bs = nullptr, *d_spf = nullptr;
+  bool part_first = true;
   void* h_forc = nullptr;          // pinned staging of the forcing table (device precision)
   std::vector<double> efk_host;    // energy input per shell of the last step (forcdt.f)
   double erate = 0, eirate[3] = {0, 0, 0};
@@ -223,6 +229,7 @@ static StageTables<T> make_tables(const Ctx& c, int ks) {
   st.b22 = (T)(c.p.beta2 * c.p.beta2);
   st.b33 = (T)(c.p.beta3 * c.p.beta3);
   st.norm = (T)(c.dt2 / c.n / c.n);
+  st.spf = (const T*)c.d_spf;
   return st;
 }
 
@@ -247,6 +254,38 @@ template <typename T, int N> struct Impl {
     CK(cudaFuncSetAttribute(k_zfwd<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm4()));
     CK(cudaFuncSetAttribute(k_yfwd<T, N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
     CK(cudaFuncSetAttribute(k_yfwd<T, N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
+    CK(cudaFuncSetAttribute(k_yinv<T, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1()));
+    CK(cudaFuncSetAttribute(k_xspline<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxs()));
+    return 0;
+  }
+
+  static size_t smxs() { return TWB + sizeof(C) * 3 * (TL::TZ / 2) * L; }
+
+  // particles at stage 1 (lagpart.f -> partsp.f): spline coefficients of the
+  // stage-1 field on the predictor grid, then the particle RK2 step with the
+  // previous step's dt (realspace is called before step, timestep_module.f)
+  static int particles(Ctx& c) {
+    Geo g = make_geo(c);
+    StageTables<T> st = make_tables<T>(c, 0);
+    const C* tw = (const C*)c.d_tw;
+    C* ub = (C*)c.d_ub;
+    C* uz = (C*)c.d_uz;
+    const int kxn = c.g.kxn;
+    k_yinv<T, N, true><<<dim3(c.nab_i, 3), Launch<T, N, TL::TB_I>::THREADS, sm1(), c.stream>>>(g, st, (const C*)c.d_u,
+                                                                                               ub, tw);
+    k_zinv<T, N><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3), Launch<T, N, TL::XT2>::THREADS, sm2(), c.stream>>>(
+        g, ub, uz, tw);
+    using V4 = typename V4T<T>::type;
+    k_xspline<T, N><<<dim3(c.nzt, N), Launch<T, N, 2 * TL::TZ>::THREADS, smxs(), c.stream>>>(g, uz, (V4*)c.d_bs, tw);
+    const double pi = 4. * std::atan(1.);
+    const double ps = 1.0;
+    const double fact = ((((0.5 * c.dt) / 2.) / pi) * (double)N) * ps;   // rk_advpos.f:31-32
+    const long long groups = (c.np + 15) / 16;
+    const int blocks = (int)std::min<long long>((groups + 15) / 16, 148LL * 16);
+    k_particles<T><<<blocks, 256, 0, c.stream>>>((const V4*)c.d_bs, N, c.np, c.d_pos, c.d_vel, c.gsh[0][0],
+                                                 c.gsh[1][0], c.gsh[2][0], fact, fact, c.part_first ? 1 : 0);
+    CK(cudaGetLastError());
+    c.part_first = false;
     return 0;
   }
 
@@ -320,10 +359,12 @@ struct Ops {
   int (*twiddles)(Ctx&);
   int (*stage_a)(Ctx&, int);
   int (*stage_b)(Ctx&, int);
+  int (*particles)(Ctx&);
 };
 
 template <typename T, int N> static Ops ops_for() {
-  return Ops{&Impl<T, N>::setup, &Impl<T, N>::twiddles, &Impl<T, N>::stage_a, &Impl<T, N>::stage_b};
+  return Ops{&Impl<T, N>::setup, &Impl<T, N>::twiddles, &Impl<T, N>::stage_a, &Impl<T, N>::stage_b,
+             &Impl<T, N>::particles};
 }
 
 static bool get_ops(int prec, int n, Ops& o) {
@@ -476,6 +517,7 @@ static int collect_forcing_stats(Ctx& c) {
 }
 
 static int run_stage(Ctx& c, const Ops& o, int kstep, int* ctl_err) {
+  if (kstep == 1 && c.np > 0 && o.particles(c)) return 1;
   if (kstep == 1) CK(cudaMemsetAsync(c.d_velmax, 0, sizeof(unsigned long long), c.stream));
   if (o.stage_a(c, kstep)) return 1;
   if (kstep == 1) {
@@ -609,6 +651,7 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
   ALLOC(c->d_forc, c->csz * std::max<size_t>(nfor, 1));
   ALLOC(c->d_efkz, sizeof(double) * 3 * (n / 2 + 2));
 #undef ALLOC
+#define ALLOC2(ptr, bytes) if (cudaMalloc((void**)&(ptr), (bytes)) != cudaSuccess) return fail(set_error("cudaMalloc of %zu bytes failed", (size_t)(bytes)))
   if (cudaMallocHost(&c->h_tabs, tabb) != cudaSuccess) return fail(set_error("cudaMallocHost"));
   if (cudaMallocHost((void**)&c->h_velmax, sizeof(unsigned long long)) != cudaSuccess) return fail(set_error("cudaMallocHost"));
   if (cudaMallocHost(&c->h_forc, c->csz * std::max<size_t>(nfor, 1)) != cudaSuccess) return fail(set_error("cudaMallocHost"));
@@ -621,6 +664,22 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
       cudaMemcpy(c->d_kymax, g.kymax.data(), sizeof(int) * g.xz_tot, cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(set_error("geometry upload failed"));
   if (o.twiddles(*c)) return fail(1);
+  {
+    // cubic B-spline symbol per axis: 6 / (4 + 2 cos(2 pi k / n))
+    const size_t ns = (size_t)(n / 2 + 1) + 2 * n;
+    std::vector<double> f(ns);
+    const double pi = 4. * std::atan(1.);
+    for (int x = 0; x <= n / 2; x++) f[x] = 6. / (4. + 2. * std::cos(2. * pi * x / n));
+    for (int y = 0; y < n; y++) f[n / 2 + 1 + y] = 6. / (4. + 2. * std::cos(2. * pi * g.ky[y] / n));
+    for (int z = 0; z < n; z++) f[n / 2 + 1 + n + z] = 6. / (4. + 2. * std::cos(2. * pi * g.kz[z] / n));
+    const size_t rsz = dbl ? sizeof(double) : sizeof(float);
+    ALLOC2(c->d_spf, rsz * ns);
+    std::vector<float> ff(ns);
+    for (size_t i = 0; i < ns; i++) ff[i] = (float)f[i];
+    if (cudaMemcpy(c->d_spf, dbl ? (const void*)f.data() : (const void*)ff.data(), rsz * ns,
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(set_error("prefilter upload failed"));
+  }
   if (cudaMemset(c->d_u, 0, c->csz * c->st_elems) != cudaSuccess ||
       cudaMemset(c->d_un, 0, c->csz * c->st_elems) != cudaSuccess ||
       cudaMemset(c->d_forc, 0, c->csz * std::max<size_t>(nfor, 1)) != cudaSuccess ||
@@ -635,7 +694,7 @@ int psdns_gpu_finalize(void* ctx) {
   if (!c) return 0;
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->d_colstart, c->d_ax, c->d_az, c->d_kymax, c->d_tw, c->d_tabs, c->d_u, c->d_un,
-                  c->d_ub, c->d_uz, c->d_forc, c->d_efkz, c->d_velmax};
+                  c->d_ub, c->d_uz, c->d_forc, c->d_efkz, c->d_velmax, c->d_pos, c->d_vel, c->d_bs, c->d_spf};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (int s = 0; s < 2; s++)
@@ -803,6 +862,41 @@ int psdns_gpu_field_init(void* ctx, int32_t seed) {
   cudaFree(d_off);
   if (e != cudaSuccess || e2 != cudaSuccess)
     return set_error("field init failed: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+  return 0;
+}
+
+int psdns_gpu_particles_set(void* ctx, int64_t np, const double* pos) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return set_error("null context");
+  if (np < 0) return set_error("negative particle count");
+  if (np > 0 && !pos) return set_error("null positions");
+  if (c->d_pos) { cudaFree(c->d_pos); c->d_pos = nullptr; }
+  if (c->d_vel) { cudaFree(c->d_vel); c->d_vel = nullptr; }
+  c->np = 0;
+  if (np == 0) return 0;
+  const size_t n3 = (size_t)c->n * c->n * c->n;
+  const size_t bsb = n3 * 4 * (c->prec == PSDNS_PREC_FP64 ? sizeof(double) : sizeof(float));
+  size_t freeb = 0, totb = 0;
+  CK(cudaMemGetInfo(&freeb, &totb));
+  const size_t need = (c->d_bs ? 0 : bsb) + sizeof(double) * 6 * (size_t)np;
+  if (need + (size_t)256 * 1024 * 1024 > freeb)
+    return set_error("particles need %.2f GB of device memory, %.2f GB free", need / 1e9, freeb / 1e9);
+  if (!c->d_bs) CK(cudaMalloc(&c->d_bs, bsb));
+  CK(cudaMalloc((void**)&c->d_pos, sizeof(double) * 3 * (size_t)np));
+  CK(cudaMalloc((void**)&c->d_vel, sizeof(double) * 3 * (size_t)np));
+  CK(cudaMemcpy(c->d_pos, pos, sizeof(double) * 3 * (size_t)np, cudaMemcpyHostToDevice));
+  CK(cudaMemset(c->d_vel, 0, sizeof(double) * 3 * (size_t)np));
+  c->np = np;
+  c->part_first = true;
+  return 0;
+}
+
+int psdns_gpu_particles_get(void* ctx, double* pos, double* vel) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return set_error("null context");
+  if (c->np == 0) return set_error("no particles");
+  if (pos) CK(cudaMemcpy(pos, c->d_pos, sizeof(double) * 3 * (size_t)c->np, cudaMemcpyDeviceToHost));
+  if (vel) CK(cudaMemcpy(vel, c->d_vel, sizeof(double) * 3 * (size_t)c->np, cudaMemcpyDeviceToHost));
   return 0;
 }
 

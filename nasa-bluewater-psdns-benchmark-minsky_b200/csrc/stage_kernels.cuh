@@ -44,6 +44,7 @@ template <typename T> struct StageTables {
   double kforce2;    // kforce^2
   T b11, b22, b33;
   T norm;            // dt2/ny/nz
+  const T* spf;      // spline prefilter 6/(4+2cos(2 pi k/n)): [n/2+1] x, [n] y, [n] z
 };
 
 // per-precision tile sizes: TB_I = columns per K1 block (64 B segments),
@@ -81,10 +82,14 @@ template <int N> struct LS { static constexpr int value = N + N / 32 + 4; };
 // K1: phase shift + mask + y backward FFT, transposed store to ub (TB_I block)
 // grid (ceil(xz_tot/TB_I), 3); one block = one ub block of TB_I columns
 // ---------------------------------------------------------------------------
-template <typename T, int N>
+template <typename T, int N, bool SPL = false>
 __global__ void __launch_bounds__(Launch<T, N, Tiles<T>::TB_I>::THREADS)
 k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict__ ub,
        const C2<T>* __restrict__ tw_g) {
+  // SPL: also divide by the cubic B-spline symbol, (4 + 2 cos(2 pi k/n))/6 per
+  // axis, so that the backward transform yields the periodic spline
+  // coefficients of the shifted-grid field (the circulant tridiagonal systems
+  // that splx.f/splz_m.f/sply.f solve in physical space)
   using C = C2<T>;
   constexpr int TB = Tiles<T>::TB_I;
   constexpr int THREADS = Launch<T, N, TB>::THREADS;
@@ -103,6 +108,11 @@ k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict_
       C sxz = cmul(__ldg(st.sx + __ldg(g.ax + a)), __ldg(st.sz + __ldg(g.az + a)));
       C sh = cmul(__ldg(st.sy + y), sxz);
       val = cmul(u[v * vs + (size_t)a * N + y], sh);
+      if constexpr (SPL) {
+        const T f = __ldg(st.spf + __ldg(g.ax + a)) * __ldg(st.spf + (N / 2 + 1) + y) *
+                    __ldg(st.spf + (N / 2 + 1) + N + __ldg(g.az + a));
+        val = cscale(f, val);
+      }
     }
     buf[l * L + pad32(y)] = cconj(val);
   }
@@ -502,6 +512,151 @@ k_yfwd(Geo g, StageTables<T> st, const C2<T>* __restrict__ ub, C2<T>* __restrict
     }
     u[o] = u1; u[vs + o] = u2; u[2 * vs + o] = u3;
     un[o] = n1; un[vs + o] = n2; un[2 * vs + o] = n3;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Spline coefficients: backward x transform of the prefiltered field (pairs
+// of z lines as in K3) and store of (c_u, c_v, c_w, 0) per grid point into
+// bs[y][z][x] (vector of 4).  grid (nzt, n).
+// ---------------------------------------------------------------------------
+template <typename T> struct V4T;
+template <> struct V4T<float> { using type = float4; };
+template <> struct V4T<double> { using type = double4; };
+
+template <typename T, int N>
+__global__ void __launch_bounds__(Launch<T, N, 2 * Tiles<T>::TZ>::THREADS)
+k_xspline(Geo g, const C2<T>* __restrict__ uz, typename V4T<T>::type* __restrict__ bs,
+          const C2<T>* __restrict__ tw_g) {
+  using C = C2<T>;
+  using V4 = typename V4T<T>::type;
+  constexpr int TZ = Tiles<T>::TZ, NPAIR = TZ / 2;
+  constexpr int THREADS = Launch<T, N, 2 * TZ>::THREADS;
+  constexpr int L = LS<N>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* bufU = tw + FFTPlan<T, N>::TWSIZE;
+  load_twiddles<T, N>(tw, tw_g);
+  const int zt = blockIdx.x, y = blockIdx.y;
+  const int kxn = g.kxn;
+  const int nz0 = N - 2 * kxn + 1;
+  for (int e = threadIdx.x; e < 3 * NPAIR * nz0; e += THREADS)
+    bufU[(e / nz0) * L + pad32(kxn + e % nz0)] = cmk<C>(0, 0);
+  for (int e = threadIdx.x; e < 3 * kxn * NPAIR; e += THREADS) {
+    const int v = e / (kxn * NPAIR), rem = e % (kxn * NPAIR), x = rem / NPAIR, p = rem % NPAIR;
+    const C* src = uz + ((((size_t)v * N + y) * g.nzt + zt) * kxn + x) * TZ + 2 * p;
+    const C A = src[0], B = src[1];
+    C* line = bufU + (v * NPAIR + p) * L;
+    if (x == 0) {
+      line[pad32(0)] = cmk<C>(A.x, -B.x);
+    } else {
+      line[pad32(x)] = cmk<C>(A.x - B.y, -(A.y + B.x));
+      line[pad32(N - x)] = cmk<C>(A.x + B.y, -(B.x - A.y));
+    }
+  }
+  __syncthreads();
+  fft_lines<T, N, THREADS>(bufU, 3 * NPAIR, L, tw);
+  // buffer = conj(a + i b): line z = 2p is re, line 2p+1 is -im
+  for (int e = threadIdx.x; e < TZ * N; e += THREADS) {
+    const int zz = e / N, x = e % N, p = zz / 2;
+    const int i = p * L + pad32(x);
+    const C U = bufU[i], V = bufU[NPAIR * L + i], W = bufU[2 * NPAIR * L + i];
+    V4 c;
+    if (zz & 1) { c.x = -U.y; c.y = -V.y; c.z = -W.y; } else { c.x = U.x; c.y = V.x; c.z = W.x; }
+    c.w = 0;
+    bs[((size_t)y * N + zt * TZ + zz) * N + x] = c;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Lagrangian particles: one Heun (RK2) step with two cubic-spline
+// interpolations (partsp.f:231-299,405-412, rk_advpos.f:29-37,65-72,
+// spcal_local.f:118-367).  Positions are FP64 in grid units (grid plane i at
+// 1 + (i-1) + gsh(.,1), partsp.f:44-51).  Sixteen lanes share a particle:
+// lane r gathers the 4 x-points of row (y, z) = (r/4, r%4) of the 4x4x4
+// stencil, and the partial sums are reduced with warp shuffles.
+// first != 0: interpolate only (first step, partsp.f:206).
+// ---------------------------------------------------------------------------
+template <typename V4>
+__device__ __forceinline__ void spline_weights(double pos, double gfn, int n, int& ib, double w[4]) {
+  // spcal_local.f:175-181, :211-231
+  const double px1 = pos - gfn;
+  const double px = px1 - (double)n;
+  const double fl = floor(px);
+  long long ipx = (long long)fl;
+  long long jpx = ipx;
+  if (ipx < 0) jpx = ipx + 1000LL * n;
+  const long long jloc = jpx % n;
+  const double bfp = ((double)jloc + px) - (double)ipx;
+  ib = (int)bfp;
+  const double t = bfp - ib;
+  const double d6 = 1. / 6., tt = 2. / 3.;
+  const double ym = 1. - t, yms = ym * ym;
+  w[0] = ym * yms * d6;
+  w[1] = tt + 0.5 * t * (yms - 1.);
+  w[3] = t * t * t * d6;
+  w[2] = 1. - w[0] - w[1] - w[3];
+}
+
+template <typename V4>
+__device__ __forceinline__ void spline_interp(const V4* __restrict__ bs, int n, const double p[3],
+                                              const double gfn[3], int lane16, unsigned mask16, double out[3]) {
+  int ib[3];
+  double wx[4], wy[4], wz[4];
+  spline_weights<V4>(p[0], gfn[0], n, ib[0], wx);
+  spline_weights<V4>(p[1], gfn[1], n, ib[1], wy);
+  spline_weights<V4>(p[2], gfn[2], n, ib[2], wz);
+  const int jy = lane16 >> 2, jz = lane16 & 3;
+  // bs index ib+k (k = 1..4) holds grid point ib+k-2 (splx.f:29-35)
+  const int yy = (ib[1] + jy - 1 + n) % n, zz = (ib[2] + jz - 1 + n) % n;
+  const V4* row = bs + ((size_t)yy * n + zz) * n;
+  double sx = 0, sy = 0, sz = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int xx = (ib[0] + k - 1 + n) % n;
+    const V4 c = row[xx];
+    sx += wx[k] * (double)c.x;
+    sy += wx[k] * (double)c.y;
+    sz += wx[k] * (double)c.z;
+  }
+  const double wyz = wy[jy] * wz[jz];
+  sx *= wyz; sy *= wyz; sz *= wyz;
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) {
+    sx += __shfl_xor_sync(mask16, sx, o, 16);
+    sy += __shfl_xor_sync(mask16, sy, o, 16);
+    sz += __shfl_xor_sync(mask16, sz, o, 16);
+  }
+  out[0] = sx; out[1] = sy; out[2] = sz;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_particles(const typename V4T<T>::type* __restrict__ bs, int n, long long np,
+                                                   double* __restrict__ pos, double* __restrict__ vel, double g1,
+                                                   double g2, double g3, double fact1, double fact2, int first) {
+  const int lane16 = threadIdx.x & 15;
+  const unsigned mask16 = 0xffffu << (threadIdx.x & 16);
+  const long long groups = (long long)gridDim.x * (blockDim.x / 16);
+  const double gfn[3] = {g1 + 1., g2 + 1., g3 + 1.};
+  for (long long m = (long long)blockIdx.x * (blockDim.x / 16) + (threadIdx.x >> 4); m < np; m += groups) {
+    double x[3] = {pos[m], pos[np + m], pos[2 * np + m]};
+    double v[3];
+    if (first) {
+      spline_interp(bs, n, x, gfn, lane16, mask16, v);
+    } else {
+      // rk_advpos(1,.5,.5): pp7 = x + fact1 v, x = pp7 + fact2 v
+      double u0[3] = {vel[m], vel[np + m], vel[2 * np + m]};
+      double h[3], xs[3], vs[3];
+      for (int k = 0; k < 3; k++) { h[k] = x[k] + fact1 * u0[k]; xs[k] = h[k] + fact2 * u0[k]; }
+      spline_interp(bs, n, xs, gfn, lane16, mask16, vs);
+      // rk_advpos(2,0,.5): x = pp7 + fact2 v*
+      for (int k = 0; k < 3; k++) x[k] = h[k] + fact2 * vs[k];
+      spline_interp(bs, n, x, gfn, lane16, mask16, v);
+    }
+    if (lane16 == 0) {
+      pos[m] = x[0]; pos[np + m] = x[1]; pos[2 * np + m] = x[2];
+      vel[m] = v[0]; vel[np + m] = v[1]; vel[2 * np + m] = v[2];
+    }
   }
 }
 

@@ -43,6 +43,8 @@ EXPORTS = (
     "psdns_gpu_rk_stage_noalloc",
     "psdns_gpu_forcing_stats",
     "psdns_gpu_spectra",
+    "psdns_gpu_particles_set",
+    "psdns_gpu_particles_get",
     "psdns_gpu_forcing_table",
 )
 
@@ -95,6 +97,8 @@ def load():
     L.psdns_gpu_profile.argtypes = [vp, ctypes.c_int32]
     L.psdns_gpu_kernel_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int64)]
     L.psdns_gpu_forcing_stats.argtypes = [vp, dp, dp, dp]
+    L.psdns_gpu_particles_set.argtypes = [vp, ctypes.c_int64, dp]
+    L.psdns_gpu_particles_get.argtypes = [vp, dp, dp]
     L.psdns_gpu_spectra.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
@@ -246,6 +250,18 @@ class Solver:
         _check(load().psdns_gpu_kernel_times(self._ctx, _dp(ms), cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))),
                "kernel_times")
         return ms, cnt
+
+    def particles_set(self, pos):
+        """pos: (np, 3) FP64 positions in grid units (pp(np,1:3))."""
+        a = np.asfortranarray(np.asarray(pos, np.float64))
+        flat = np.ascontiguousarray(a.T)   # (3, np): column-major (np,3)
+        self._np = flat.shape[1]
+        _check(load().psdns_gpu_particles_set(self._ctx, self._np, _dp(flat)), "particles_set")
+
+    def particles_get(self):
+        pos = np.zeros((3, self._np)); vel = np.zeros((3, self._np))
+        _check(load().psdns_gpu_particles_get(self._ctx, _dp(pos), _dp(vel)), "particles_get")
+        return pos.T.copy(), vel.T.copy()
 
     def spectra(self, which=FIELD_UN):
         """FP64 shell spectra (sptr.f): (ek[n], dk[n], eijk[n,6], stats dict)."""

@@ -56,6 +56,8 @@ def lib():
         L.orc_rann2.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int]
         L.orc_get_threads.restype = ctypes.c_int
         L.orc_spectra.argtypes = [vp, ctypes.c_int, dp, dp, dp, dp]
+        L.orc_particles_set.argtypes = [vp, ctypes.c_long, dp]
+        L.orc_particles_get.argtypes = [vp, dp, dp]
         _LIB = L
     return _LIB
 
@@ -168,6 +170,17 @@ class Oracle:
         ek = np.zeros(n); dk = np.zeros(n); e6 = np.zeros(n * 6); st = np.zeros(7)
         lib().orc_spectra(self._c, int(which), _dp(ek), _dp(dk), _dp(e6), _dp(st))
         return ek, dk, e6.reshape(n, 6), dict(zip(["tke", "eps", "skew", "klen", "kvel", "ktime", "ekl"], st))
+
+    def particles_set(self, pos):
+        """pos: (np, 3) positions in grid units (pp(np,1:3))."""
+        flat = np.ascontiguousarray(np.asarray(pos, np.float64).T)
+        self._np = flat.shape[1]
+        lib().orc_particles_set(self._c, self._np, _dp(flat))
+
+    def particles_get(self):
+        pos = np.zeros((3, self._np)); vel = np.zeros((3, self._np))
+        lib().orc_particles_get(self._c, _dp(pos), _dp(vel))
+        return pos.T.copy(), vel.T.copy()
 
     def rann2(self, seq, n):
         x = np.zeros(n, np.float64)

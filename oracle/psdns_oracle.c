@@ -187,6 +187,10 @@ typedef struct {
     double *efkz;          /* efkz(k,i), k = 1..kfor */
     double g_tab[202], g_dtab[202], g_p1;
     int g_ready;
+    /* particles: pp(np,1:3) positions, pp(np,4:6) velocities (column-major) */
+    long np;
+    double *pp;            /* [9][np] */
+    int part_first;
 } orc_ctx;
 
 static int mask_ok(const orc_ctx *c, int a, int y)
@@ -287,6 +291,7 @@ void orc_destroy(orc_ctx *c)
     free(c->ax); free(c->az); free(c->kymax); free(c->u); free(c->un);
     free(c->sx); free(c->sy); free(c->sz); free(c->xfac); free(c->yfac); free(c->zfac);
     free(c->tw.w);
+    free(c->pp);
     free(c->suo); free(c->svo); free(c->velinc); free(c->w1); free(c->w2); free(c->forc); free(c->efkz);
     free(c);
 }
@@ -971,6 +976,173 @@ void orc_rann2(orc_ctx *c, int seq, double *x, int n)
     rann2(c, x, n);
 }
 
+
+/* ------------------------------------------------------------------------ */
+/* Lagrangian particles (LAG_LOCAL)                                         */
+/* ------------------------------------------------------------------------ */
+/* solsp1.f:21-40: factors of the periodic [1 4 1] system */
+static void solsp1(int n, double *p, double *q, double *t, double *d)
+{
+    double *s = (double *)malloc(sizeof(double) * (size_t)(n + 1));
+    q[0] = 0.;
+    for (int i = 1; i <= n; i++) { p[i] = q[i - 1] + 4.; q[i] = -1. / p[i]; }
+    s[0] = 1.;
+    for (int i = 1; i <= n; i++) s[i] = -s[i - 1] / p[i];
+    t[n] = 1.;
+    for (int i = n - 1; i >= 1; i--) t[i] = q[i] * t[i + 1] + s[i];
+    *d = 1. / (t[1] + t[n - 1] + 4.);
+    for (int i = 1; i <= n; i++) p[i] = 1. / p[i];
+    free(s);
+}
+
+/* splx.f:20-40 on one line: f[1..n] (1-based) -> b[1..n+3]; scale multiplies
+ * the input (splz_m.f:31 uses 216) */
+static void spl_line(int n, const double *p, const double *q, const double *t, double d, const double *f,
+                     double scale, double *u, double *v, double *b)
+{
+    u[0] = 0.; v[n] = 0.;
+    for (int x = 1; x <= n; x++) u[x] = (f[x] * scale - u[x - 1]) * p[x];
+    for (int x = n - 1; x >= 1; x--) v[x] = q[x] * v[x + 1] + u[x];
+    b[n + 1] = d * (f[n] * scale - v[1] - v[n - 1]);
+    for (int x = n - 1; x >= 1; x--) b[x + 1] = t[x] * b[n + 1] + v[x];
+    b[1] = b[n + 1]; b[n + 2] = b[2]; b[n + 3] = b[3];
+}
+
+/* spxyz_m.f: x sweep, z sweep (x216), y sweep of one variable.
+ * in: f[y][z][x] (0-based, n^3); out: bs[y+1][z+1][x+1] over (n+3)^3, index
+ * j in 1..n+3 holding grid point j-2 (mod n) */
+static void spline3(orc_ctx *c, const double *f, double *bs)
+{
+    int n = c->n, nb = n + 3;
+    double *p = malloc(sizeof(double) * (n + 1)), *q = malloc(sizeof(double) * (n + 1)), *t = malloc(sizeof(double) * (n + 1));
+    double d;
+    solsp1(n, p, q, t, &d);
+    double *A = calloc((size_t)nb * nb * nb, sizeof(double));   /* after x: [y][z][xb] */
+    #pragma omp parallel
+    {
+        double *fl = malloc(sizeof(double) * (n + 4)), *u = malloc(sizeof(double) * (n + 4)),
+               *v = malloc(sizeof(double) * (n + 4)), *b = malloc(sizeof(double) * (n + 4));
+        #pragma omp for collapse(2)
+        for (int y = 0; y < n; y++)
+            for (int z = 0; z < n; z++) {
+                for (int x = 0; x < n; x++) fl[x + 1] = f[((size_t)y * n + z) * n + x];
+                spl_line(n, p, q, t, d, fl, 1.0, u, v, b);
+                for (int xb = 1; xb <= nb; xb++) A[(((size_t)(y + 1)) * nb + (z + 1)) * nb + xb - 1] = b[xb];
+            }
+        /* z sweep (x216) for every x index of the padded x dimension */
+        #pragma omp for collapse(2)
+        for (int y = 0; y < n; y++)
+            for (int xb = 0; xb < nb; xb++) {
+                for (int z = 0; z < n; z++) fl[z + 1] = A[(((size_t)(y + 1)) * nb + (z + 1)) * nb + xb];
+                spl_line(n, p, q, t, d, fl, 216., u, v, b);
+                for (int zb = 1; zb <= nb; zb++) A[(((size_t)(y + 1)) * nb + (zb - 1)) * nb + xb] = b[zb];
+            }
+        /* y sweep */
+        #pragma omp for collapse(2)
+        for (int zb = 0; zb < nb; zb++)
+            for (int xb = 0; xb < nb; xb++) {
+                for (int y = 0; y < n; y++) fl[y + 1] = A[(((size_t)(y + 1)) * nb + zb) * nb + xb];
+                spl_line(n, p, q, t, d, fl, 1.0, u, v, b);
+                for (int yb = 1; yb <= nb; yb++) bs[(((size_t)(yb - 1)) * nb + zb) * nb + xb] = b[yb];
+            }
+        free(fl); free(u); free(v); free(b);
+    }
+    free(A); free(p); free(q); free(t);
+}
+
+/* spcal_local.f:175-231: cell index and basis functions along one axis */
+static void bweights(double pos, double gfn, int n, int *ib, double w[4])
+{
+    double px1 = pos - gfn;
+    double px = px1 - (double)n;
+    long ipx = (long)floor(px);
+    long jpx = ipx;
+    if (ipx < 0) jpx = ipx + 1000L * n;
+    long jloc = jpx % n;
+    double bfp = (double)jloc + px - (double)ipx;
+    *ib = (int)bfp;
+    double t = bfp - *ib, d6 = 1. / 6., tt = 2. / 3.;
+    double ym = 1. - t, yms = ym * ym;
+    w[0] = ym * yms * d6;
+    w[1] = tt + 0.5 * t * (yms - 1.);
+    w[3] = t * t * t * d6;
+    w[2] = 1. - w[0] - w[1] - w[3];
+}
+
+/* spcal_local.f:234-367: sum of the 4x4x4 stencil; bs index kk = ib+k,
+ * folded by nb (n+3) */
+static double binterp(const double *bs, int n, const double p[3], const double gfn[3])
+{
+    int nb = n + 3, ib[3];
+    double w[3][4];
+    for (int j = 0; j < 3; j++) bweights(p[j], gfn[j], n, &ib[j], w[j]);
+    double sum = 0.;
+    for (int k = 1; k <= 4; k++) {
+        int kz = ib[2] + k; if (kz > nb) kz -= nb;
+        for (int jj = 1; jj <= 4; jj++) {
+            int ky = ib[1] + jj; if (ky > nb) ky -= nb;
+            for (int i = 1; i <= 4; i++) {
+                int kx = ib[0] + i; if (kx > nb) kx -= nb;
+                sum += bs[(((size_t)(ky - 1)) * nb + (kz - 1)) * nb + (kx - 1)] * w[0][i - 1] * w[1][jj - 1] * w[2][k - 1];
+            }
+        }
+    }
+    return sum;
+}
+
+void orc_particles_set(orc_ctx *c, long np, const double *pos)
+{
+    free(c->pp);
+    c->np = np;
+    c->pp = calloc((size_t)9 * np, sizeof(double));
+    memcpy(c->pp, pos, sizeof(double) * 3 * (size_t)np);
+    c->part_first = 1;
+}
+
+void orc_particles_get(orc_ctx *c, double *pos, double *vel)
+{
+    if (pos) memcpy(pos, c->pp, sizeof(double) * 3 * (size_t)c->np);
+    if (vel) memcpy(vel, c->pp + 3 * (size_t)c->np, sizeof(double) * 3 * (size_t)c->np);
+}
+
+/* partsp.f:231-299,405-412 with rk_advpos.f and rk_part.f: p[0..2] is the
+ * stage-1 physical velocity on the predictor grid; dt is the previous step's */
+static void particles_stage1(orc_ctx *c, const double *p)
+{
+    int n = c->n, nb = n + 3;
+    long np = c->np;
+    size_t n3 = (size_t)n * n * n, nb3 = (size_t)nb * nb * nb;
+    double *bs = malloc(sizeof(double) * 3 * nb3);
+    for (int v = 0; v < 3; v++) spline3(c, p + v * n3, bs + v * nb3);
+    double gfn[3] = {c->gsh[0][0] + 1., c->gsh[1][0] + 1., c->gsh[2][0] + 1.};
+    double pi = 4. * atan(1.);
+    double *pp = c->pp;
+    if (c->part_first) {
+        #pragma omp parallel for
+        for (long m = 0; m < np; m++) {
+            double x[3] = {pp[m], pp[np + m], pp[2 * np + m]};
+            for (int v = 0; v < 3; v++) pp[(3 + v) * np + m] = binterp(bs + v * nb3, n, x, gfn);
+        }
+        c->part_first = 0;
+    } else {
+        double fact1 = 0.5 * c->dt / 2. / pi * n * 1.0;
+        double fact2 = fact1;
+        #pragma omp parallel for
+        for (long m = 0; m < np; m++) {
+            double x[3], h[3], xs[3], vs[3];
+            for (int k = 0; k < 3; k++) {
+                h[k] = pp[k * np + m] + fact1 * pp[(3 + k) * np + m];     /* pp(,7:9) */
+                xs[k] = h[k] + fact2 * pp[(3 + k) * np + m];
+            }
+            for (int v = 0; v < 3; v++) vs[v] = binterp(bs + v * nb3, n, xs, gfn);
+            for (int k = 0; k < 3; k++) x[k] = h[k] + fact2 * vs[k];
+            for (int k = 0; k < 3; k++) pp[k * np + m] = x[k];
+            for (int v = 0; v < 3; v++) pp[(3 + v) * np + m] = binterp(bs + v * nb3, n, x, gfn);
+        }
+    }
+    free(bs);
+}
+
 /* One RK stage (timestep_module.f:70-481, CLEAN velocity path, nc = 0).
  * The work array holds u (3 vars) on entry and the nonlinear slots (4 vars)
  * after the forward transform; u keeps the result. */
@@ -985,6 +1157,7 @@ static int rk_stage(orc_ctx *c, int kstep)
     memcpy(w, c->u, sizeof(cx) * 3 * vs);
     double *p = (double *)malloc(sizeof(double) * 5 * np);
     itransform(c, w, 3, p);
+    if (kstep == 1 && c->np > 0) particles_stage1(c, p);   /* realspace -> lagpart */
     double vm = realspace(c, p, kstep == 1);
     if (kstep == 1) c->velmax = vm;
     transform(c, p, w);

@@ -201,3 +201,47 @@ def test_spectra_against_numpy(oracle_mod):
     eps = 2 * nu * np.sum(K2 * e)
     assert abs(st["eps"] - eps) < 1e-12 * eps
     o.close()
+
+
+def test_spline_interpolates_grid_values_exactly(oracle_mod):
+    """The periodic cubic spline (solsp1/splx/splz_m/sply sweeps) passes
+    through the grid values: particles placed on grid points get the field
+    values there (first step interpolates only)."""
+    n = 16
+    o = oracle_mod.Oracle(n, 0.01, cfl=-1, dt=0.01, kshift=4)
+    un = o.field_init(21)
+    o.set_state(un)
+    o.set_shifts(np.zeros((3, 2)))   # kshift = 4: the step uses zero shifts too
+    p = o.itransform(un, 1)          # physical u on the (unshifted) grid [v][y][z][x]
+    rng = np.random.default_rng(1)
+    idx = rng.integers(0, n, size=(40, 3))
+    pos = 1.0 + idx.astype(float)    # grid plane i at 1 + (i-1) (partsp.f:44-51)
+    o.particles_set(pos)
+    o.step()
+    _, vel = o.particles_get()
+    expect = np.stack([p[v][idx[:, 1], idx[:, 2], idx[:, 0]] for v in range(3)], axis=1)
+    np.testing.assert_allclose(vel, expect, atol=1e-12)
+    o.close()
+
+
+def test_particle_heun_step_in_uniform_flow(oracle_mod):
+    """u = (U, 0, 0) constant (the kx=0,ky=0,kz=0 mode is zeroed by the
+    solver, so use a long-wave field instead): positions advance by
+    dt N/(2 pi) (u0 + u*)/2 (rk_advpos.f)."""
+    n = 16
+    o = oracle_mod.Oracle(n, 0.0, cfl=-1, dt=0.01, kshift=4)
+    un = np.zeros(o.state_shape(), complex)
+    un[1, 0, 1] = 0.5            # v = cos(y) (solenoidal)
+    un[1, 0, n - 1] = 0.5
+    o.set_state(un)
+    pos = np.array([[1.0, 1.0, 1.0], [5.5, 3.25, 7.0]])
+    o.particles_set(pos)
+    o.step()
+    _, v0 = o.particles_get()
+    o.step()
+    p1, v1 = o.particles_get()
+    f = 0.01 * n / (2 * np.pi)
+    # the y displacement is dt N/2pi * mean of the two interpolated velocities
+    assert np.all(np.abs(p1[:, 1] - pos[:, 1]) > 0)
+    np.testing.assert_allclose(p1[:, 0], pos[:, 0], atol=1e-14)
+    o.close()
