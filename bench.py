@@ -1,12 +1,15 @@
 #!/usr/bin/env python
 """bench.py -- throughput of the PSDNS RK2 time step on B200.
 
-Workload: one periodic box of n^3 points (default 1024^3) with an FP32 device
-state, advanced by the RK2 step of PSDNS (both stages: phase shift, inverse
-transforms, products, forward transforms, wavespace closure, integrating
-factor update, projection).  The initial field is the seeded random solenoidal
-field of field.f with E(k) ~ k^4 exp(-2 (k/3)^2), u' = 1 (synthetic; no
-dataset is involved).
+Workload: the forced 1024^3 box with an FP32 device state, advanced by the
+RK2 step of PSDNS (both stages: phase shift, inverse transforms, products,
+forward transforms, wavespace closure, integrating factor update, projection),
+with Eswaran-Pope forcing on shells |k| < 3 (tforce = 0.5, epsilon target
+0.1), viscosity from kmax*eta = 1.5, adaptive dt at Courant number 0.5
+(cfl = pi) and 2^24 Lagrangian particles (FP64 positions, FP32 spline
+coefficients).  The initial field is the seeded random solenoidal field of
+field.f with E(k) ~ k^4 exp(-2 (k/3)^2), u' = 1, and particles start
+uniformly at random (seeded); all data is synthetic.
 
 `value` is points per second (Gpts/s = n^3 / step time) with the state
 resident in HBM; `e2e` is the same metric through the C-ABI with the state in
@@ -48,6 +51,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-n", type=int, default=256)
+    ap.add_argument("--particles", type=int, default=1 << 24)
+    ap.add_argument("--unforced", action="store_true")
     return ap.parse_args()
 
 
@@ -180,9 +185,20 @@ def main():
     n = args.n
     prec = P.PREC_FP32 if args.prec == "fp32" else P.PREC_FP64
     csz = 8 if prec == P.PREC_FP32 else 16
-    nu = 0.0028 * (512.0 / n) ** (4.0 / 3.0)
-    s = P.Solver(n=n, precision=prec, viscos=nu, cfl=3.77 / 2.0, dt=0.0, kshift=1)
+    import math
+    import numpy as np
+    eps_target = 0.1
+    kmax = math.sqrt(2.0) * n / 3.0
+    nu = (1.5 / kmax) ** (4.0 / 3.0) * eps_target ** (1.0 / 3.0)   # kmax*eta = 1.5
+    kforce = 0.0 if args.unforced else 2.99                          # shells |k| < 3
+    epsfor = eps_target / (4.0 * (4.0 * math.pi / 3.0) * 3.0 ** 3)   # epfor_param.f: eps/(4 N_f)
+    s = P.Solver(n=n, precision=prec, viscos=nu, cfl=math.pi, dt=0.0, kshift=1,
+                 kforce=kforce, tforce=0.5, epsfor=epsfor, tfiuo=0.0)
     s.field_init(1234 + rank)
+    npart = args.particles
+    if npart > 0:
+        rng = np.random.default_rng(4321 + rank)
+        s.particles_set(1.0 + rng.random((npart, 3)) * n)
     stream = torch.cuda.ExternalStream(s.stream())
 
     def barrier():
@@ -216,9 +232,22 @@ def main():
     ms_step = ms_total / args.steps
     value = world * n ** 3 / (ms_step * 1e-3) / 1e9
 
-    names = ["k_yinv", "k_zinv", "k_xchain", "k_zfwd", "k_yfwd"]
+    names = ["k_yinv", "k_zinv", "k_xchain", "k_zfwd", "k_yfwd", "particles"]
     per_launch, step_bytes = algorithmic_bytes(n, s.kxn, s.xz_tot, csz)
-    dom = max(range(5), key=lambda i: kms[i])
+    if npart > 0:
+        # particle phase: one extra 3-variable backward chain (9C + 6Z), the
+        # spline coefficients written once (3 values per point), two stencil
+        # gathers (min of the whole coefficient field and 64 points x 3 values
+        # per particle) and FP64 positions/velocities read and written
+        C = s.xz_tot * n * csz
+        Z = s.kxn * n * n * csz
+        rsz = csz // 2
+        coef = 3 * n ** 3 * rsz
+        per_launch["particles"] = 9 * C + 6 * Z + coef + 2 * min(coef, npart * 64 * 3 * rsz) + npart * 12 * 8
+        step_bytes += per_launch["particles"]
+    else:
+        per_launch["particles"] = 0
+    dom = max(range(5), key=lambda i: kms[i])   # dominant stage kernel
     avg_ms = kms[dom] / max(1, kcnt[dom])
     achieved = per_launch[names[dom]] / (avg_ms * 1e-3) / 1e9
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -239,7 +268,7 @@ def main():
                                "share": kms[i] / max(1e-12, sum(kms)),
                                "algorithmic_bytes": per_launch[names[i]],
                                "achieved_gbs": per_launch[names[i]] / (kms[i] / max(1, kcnt[i]) * 1e-3) / 1e9}
-                    for i in range(5)}
+                    for i in range(6) if kcnt[i] > 0}
 
     # end to end through the C-ABI: state (complex(8), reference layout) copied
     # from pinned host memory and back every step
@@ -287,9 +316,11 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if prec == P.PREC_FP32 else "f64",
             "data": "synthetic: seeded random solenoidal field, E(k)~k^4 exp(-2(k/3)^2), u'=1",
-            "config": {"workload": f"unforced RK2 step of one {n}^3 periodic box per GPU, "
-                                   f"{args.prec} state, kshift=1 phase shifts, adaptive dt (cfl=1.885)",
-                       "n": n, "precision": args.prec, "viscosity": nu, "parallelism": f"replicas x{world}",
+            "config": {"workload": f"{'unforced' if kforce == 0 else 'forced'} RK2 step of one {n}^3 periodic box "
+                                   f"per GPU, {args.prec} state, kshift=1 phase shifts, cfl=pi (Courant 0.5), "
+                                   f"{npart} particles",
+                       "n": n, "precision": args.prec, "viscosity": nu, "kforce": kforce, "tforce": 0.5,
+                       "epsfor": epsfor, "particles": npart, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (state >= 9 GB per variable set), no flush needed"},
             "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
                          "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
@@ -298,7 +329,7 @@ def main():
             "kernels": kernel_table,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": int(sum(kcnt)),
+            "gpu_launches": int(sum(kcnt[:5]) + 4 * kcnt[5]),
             "clocks": ck,
             "last_step": {"dt": info["dt"], "velmax": info["velmax"], "courant": info["courant"]},
         }

@@ -155,8 +155,9 @@ int psdns_gpu_get_stream(void *ctx, void **stream);
  * (replaces the MPI_WTIME stage timers tt(1..10) of
  * PSDNS/timestep_module.f:90-478).  enable != 0 starts (and zeroes) the
  * accumulation; psdns_gpu_kernel_times returns, for the five stage kernels
- * (y backward, z backward, x chain, z forward, y forward + update), the summed
- * milliseconds ms[5] and launch counts launches[5]. */
+ * (y backward, z backward, x chain, z forward, y forward + update) and the
+ * particle phase (spline transform + particle step, 4 launches), the summed
+ * milliseconds ms[6] and counts launches[6]. */
 int psdns_gpu_profile(void *ctx, int32_t enable);
 int psdns_gpu_kernel_times(void *ctx, double *ms, int64_t *launches);
 

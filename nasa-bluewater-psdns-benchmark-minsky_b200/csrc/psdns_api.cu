@@ -165,9 +165,9 @@ struct Ctx {
   double erate = 0, eirate[3] = {0, 0, 0};
   // per-kernel CUDA-event timing: [stage][kernel][begin/end]
   bool prof = false;
-  cudaEvent_t ev[2][5][2] = {};
-  double prof_ms[5] = {0, 0, 0, 0, 0};
-  long long prof_n[5] = {0, 0, 0, 0, 0};
+  cudaEvent_t ev[2][6][2] = {};
+  double prof_ms[6] = {0, 0, 0, 0, 0, 0};
+  long long prof_n[6] = {0, 0, 0, 0, 0, 0};
   bool prof_pending[2] = {false, false};
 };
 
@@ -271,6 +271,7 @@ template <typename T, int N> struct Impl {
     C* ub = (C*)c.d_ub;
     C* uz = (C*)c.d_uz;
     const int kxn = c.g.kxn;
+    prof_mark(c, 0, 5, 0);
     k_yinv<T, N, true><<<dim3(c.nab_i, 3), Launch<T, N, TL::TB_I>::THREADS, sm1(), c.stream>>>(g, st, (const C*)c.d_u,
                                                                                                ub, tw);
     k_zinv<T, N><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3), Launch<T, N, TL::XT2>::THREADS, sm2(), c.stream>>>(
@@ -284,6 +285,7 @@ template <typename T, int N> struct Impl {
     const int blocks = (int)std::min<long long>((groups + 15) / 16, 148LL * 16);
     k_particles<T><<<blocks, 256, 0, c.stream>>>((const V4*)c.d_bs, N, c.np, c.d_pos, c.d_vel, c.gsh[0][0],
                                                  c.gsh[1][0], c.gsh[2][0], fact, fact, c.part_first ? 1 : 0);
+    prof_mark(c, 0, 5, 1);
     CK(cudaGetLastError());
     c.part_first = false;
     return 0;
@@ -524,6 +526,7 @@ static int run_stage(Ctx& c, const Ops& o, int kstep, int* ctl_err) {
     CK(cudaMemcpyAsync(c.h_velmax, c.d_velmax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
     prof_collect(c, 0, 0, 4);
+    if (c.np > 0) prof_collect(c, 0, 5, 6);
     double vm;
     std::memcpy(&vm, c.h_velmax, sizeof vm);
     c.velmax = vm;
@@ -698,7 +701,7 @@ int psdns_gpu_finalize(void* ctx) {
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (int s = 0; s < 2; s++)
-    for (int k = 0; k < 5; k++)
+    for (int k = 0; k < 6; k++)
       for (int e = 0; e < 2; e++)
         if (c->ev[s][k][e]) cudaEventDestroy(c->ev[s][k][e]);
   if (c->h_tabs) cudaFreeHost(c->h_tabs);
@@ -988,18 +991,18 @@ int psdns_gpu_profile(void* ctx, int32_t enable) {
   if (!c) return set_error("null context");
   if (enable && !c->ev[0][0][0]) {
     for (int s = 0; s < 2; s++)
-      for (int k = 0; k < 5; k++)
+      for (int k = 0; k < 6; k++)
         for (int e = 0; e < 2; e++) CK(cudaEventCreate(&c->ev[s][k][e]));
   }
   c->prof = enable != 0;
-  for (int k = 0; k < 5; k++) { c->prof_ms[k] = 0; c->prof_n[k] = 0; }
+  for (int k = 0; k < 6; k++) { c->prof_ms[k] = 0; c->prof_n[k] = 0; }
   return 0;
 }
 
 int psdns_gpu_kernel_times(void* ctx, double* ms, int64_t* launches) {
   Ctx* c = (Ctx*)ctx;
   if (!c) return set_error("null context");
-  for (int k = 0; k < 5; k++) {
+  for (int k = 0; k < 6; k++) {
     if (ms) ms[k] = c->prof_ms[k];
     if (launches) launches[k] = c->prof_n[k];
   }

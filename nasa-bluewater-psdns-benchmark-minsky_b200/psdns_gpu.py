@@ -245,8 +245,8 @@ class Solver:
         _check(load().psdns_gpu_profile(self._ctx, 1 if enable else 0), "profile")
 
     def kernel_times(self):
-        ms = np.zeros(5, np.float64)
-        cnt = np.zeros(5, np.int64)
+        ms = np.zeros(6, np.float64)
+        cnt = np.zeros(6, np.int64)
         _check(load().psdns_gpu_kernel_times(self._ctx, _dp(ms), cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))),
                "kernel_times")
         return ms, cnt
