@@ -1,0 +1,87 @@
+! psdns_gpu_mod.f90 -- Fortran 2003 interface to libpsdns_gpu (include/psdns_gpu.h).
+!
+! A PSDNS driver USEs this module and calls the C-ABI through iso_c_binding;
+! no Fortran compiler exists in the build container, so this file is shipped
+! for the driver build (link with -lpsdns_gpu).
+module psdns_gpu_mod
+  use iso_c_binding
+  implicit none
+
+  integer(c_int32_t), parameter :: PSDNS_PREC_FP32 = 0, PSDNS_PREC_FP64 = 1
+  integer(c_int32_t), parameter :: PSDNS_LAYOUT_YCYL = 0
+  integer(c_int32_t), parameter :: PSDNS_FIELD_U = 0, PSDNS_FIELD_UN = 1
+
+  type, bind(c) :: psdns_params
+    integer(c_int32_t) :: nx, ny, nz, nc, precision, kshift, ksran, seed_input
+    integer(c_int32_t) :: kranf1, kranf2
+    integer(c_int32_t) :: reserved_i(6)
+    real(c_double) :: viscos, beta1, beta2, beta3, cfl, dt
+    real(c_double) :: kforce, tforce, epsfor, tfiuo, pr
+    real(c_double) :: grad(3)
+    real(c_double) :: reserved_d(8)
+  end type psdns_params
+
+  interface
+    integer(c_int) function psdns_gpu_default_params(p) bind(c, name='psdns_gpu_default_params')
+      import :: c_int, psdns_params
+      type(psdns_params), intent(inout) :: p
+    end function
+    integer(c_int) function psdns_gpu_init(p, ctx) bind(c, name='psdns_gpu_init')
+      import :: c_int, c_ptr, psdns_params
+      type(psdns_params), intent(in) :: p
+      type(c_ptr), intent(out) :: ctx
+    end function
+    integer(c_int) function psdns_gpu_finalize(ctx) bind(c, name='psdns_gpu_finalize')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function psdns_gpu_set_state(ctx, un, layout) bind(c, name='psdns_gpu_set_state')
+      import :: c_int, c_ptr, c_double_complex, c_int32_t
+      type(c_ptr), value :: ctx
+      complex(c_double_complex), intent(in) :: un(*)
+      integer(c_int32_t), value :: layout
+    end function
+    integer(c_int) function psdns_gpu_get_state(ctx, out, which, layout) bind(c, name='psdns_gpu_get_state')
+      import :: c_int, c_ptr, c_double_complex, c_int32_t
+      type(c_ptr), value :: ctx
+      complex(c_double_complex), intent(out) :: out(*)
+      integer(c_int32_t), value :: which, layout
+    end function
+    integer(c_int) function psdns_gpu_step(ctx, info) bind(c, name='psdns_gpu_step')
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(out) :: info(8)
+    end function
+    integer(c_int) function psdns_gpu_rk_stage(ctx, kstep, gsh, dt, forcing, velmax) bind(c, name='psdns_gpu_rk_stage')
+      import :: c_int, c_ptr, c_double, c_int32_t
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: kstep
+      real(c_double), intent(in) :: gsh(3, 2)
+      real(c_double), intent(in) :: dt
+      type(c_ptr), value :: forcing       ! c_loc(for) or c_null_ptr
+      real(c_double), intent(out) :: velmax
+    end function
+    integer(c_int) function psdns_gpu_spectra(ctx, which, ek, dk, eijk, stats) bind(c, name='psdns_gpu_spectra')
+      import :: c_int, c_ptr, c_double, c_int32_t
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: which
+      real(c_double), intent(out) :: ek(*), dk(*), eijk(*), stats(7)
+    end function
+    integer(c_int) function psdns_gpu_particles_set(ctx, np, pos) bind(c, name='psdns_gpu_particles_set')
+      import :: c_int, c_ptr, c_double, c_int64_t
+      type(c_ptr), value :: ctx
+      integer(c_int64_t), value :: np
+      real(c_double), intent(in) :: pos(*)
+    end function
+    integer(c_int) function psdns_gpu_particles_get(ctx, pos, vel) bind(c, name='psdns_gpu_particles_get')
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(out) :: pos(*), vel(*)
+    end function
+    integer(c_int) function psdns_gpu_last_error(buf, len) bind(c, name='psdns_gpu_last_error')
+      import :: c_int, c_char, c_int32_t
+      character(kind=c_char), intent(out) :: buf(*)
+      integer(c_int32_t), value :: len
+    end function
+  end interface
+end module psdns_gpu_mod
