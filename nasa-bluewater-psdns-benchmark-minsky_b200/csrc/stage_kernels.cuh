@@ -155,9 +155,9 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
   __syncthreads();
   fft_lines<T, N, THREADS>(buf, nl, L, tw);
   const size_t vbase = ((size_t)v * N + y) * g.nzt;
-  for (int e = threadIdx.x; e < nl * N; e += THREADS) {
-    const int zt = e / (nl * TZ), rem = e % (nl * TZ), l = rem / TZ, zz = rem % TZ;
-    uz[((vbase + zt) * g.kxn + x0 + l) * TZ + zz] = cconj(buf[l * L + pad32(zt * TZ + zz)]);
+  for (int e = threadIdx.x; e < XT * N; e += THREADS) {
+    const int zt = e / (XT * TZ), rem = e % (XT * TZ), l = rem / TZ, zz = rem % TZ;
+    if (l < nl) uz[((vbase + zt) * g.kxn + x0 + l) * TZ + zz] = cconj(buf[l * L + pad32(zt * TZ + zz)]);
   }
 }
 
@@ -177,8 +177,10 @@ __device__ __forceinline__ void xchain_store(const Geo& g, const C2<T>* buf, int
   using C = C2<T>;
   constexpr int TZ = Tiles<T>::TZ, NPAIR = TZ / 2;
   const int kxn = g.kxn;
-  for (int e = threadIdx.x; e < nbuf * kxn * NPAIR; e += blockDim.x) {
-    const int b = e / (kxn * NPAIR), rem = e % (kxn * NPAIR), x = rem / NPAIR, p = rem % NPAIR;
+  // thread -> fixed pair p, x strided by blockDim/NPAIR (no runtime division)
+  const int p = threadIdx.x % NPAIR, x0 = threadIdx.x / NPAIR, xs = blockDim.x / NPAIR;
+  for (int b = 0; b < nbuf; b++)
+  for (int x = x0; x < kxn; x += xs) {
     const C* line = buf + (b * NPAIR + p) * L;
     const C Y = line[pad32(x)];
     const C Yn = line[pad32(x == 0 ? 0 : N - x)];
@@ -208,14 +210,17 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
   const int zt = blockIdx.x, y = blockIdx.y;
   const int kxn = g.kxn;
   // zero the band kx in [kxn, n-kxn] (includes the Nyquist column)
-  const int nz0 = N - 2 * kxn + 1;
-  for (int e = threadIdx.x; e < 3 * NPAIR * nz0; e += THREADS)
-    bufU[(e / nz0) * L + pad32(kxn + e % nz0)] = cmk<C>(0, 0);
+  for (int e = threadIdx.x; e < 3 * NPAIR * N; e += THREADS) {
+    const int k = e % N;
+    if (k >= kxn && k <= N - kxn) bufU[(e / N) * L + pad32(k)] = cmk<C>(0, 0);
+  }
   // pack two real lines per complex line: Z(k) = A(k) + i B(k), with the
   // Hermitian extension and the imaginary part of the kx=0 term dropped;
   // stored conjugated (backward transform by conjugation)
-  for (int e = threadIdx.x; e < 3 * kxn * NPAIR; e += THREADS) {
-    const int v = e / (kxn * NPAIR), rem = e % (kxn * NPAIR), x = rem / NPAIR, p = rem % NPAIR;
+  const int pth = threadIdx.x % NPAIR, xth = threadIdx.x / NPAIR, xst = THREADS / NPAIR;
+  for (int v = 0; v < 3; v++)
+  for (int x = xth; x < kxn; x += xst) {
+    const int p = pth;
     const C* src = uz + ((((size_t)v * N + y) * g.nzt + zt) * kxn + x) * TZ + 2 * p;
     const C A = src[0], B = src[1];
     C* line = bufU + (v * NPAIR + p) * L;
@@ -295,8 +300,9 @@ __device__ __forceinline__ void zfwd_load(const Geo& g, const C2<T>* __restrict_
 
 template <typename T, int N, int MODE>
 __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const C2<T>* s1, int L,
-                                           C2<T>* __restrict__ ub, int slot, int y0, int ny, int x0, int x1,
+                                           C2<T>* __restrict__ ub, int slot, int y0, int /*ny*/, int x0, int x1,
                                            T b11, T b33) {
+  constexpr int ny = Tiles<T>::YT4;
   // the ny rows of one block column are adjacent in ub: write them together
   using C = C2<T>;
   constexpr int TB = Tiles<T>::TB_F;
@@ -392,9 +398,10 @@ __device__ __forceinline__ void project3(C2<T>& u1, C2<T>& u2, C2<T>& u3, T kx, 
   const T bk1 = b11 * kx, bk3 = b33 * kz, bkk3 = bk3 * kz;
   const T bk12 = bk1 * kx + b22 * (ky * ky);
   const T den = bk12 + bkk3;
+  const T rden = T(1) / den;
   const T c2 = b22 * ky;
   const C s = cmk<C>(bk1 * u1.x + c2 * u2.x + bk3 * u3.x, bk1 * u1.y + c2 * u2.y + bk3 * u3.y);
-  const C psi = cmk<C>(-(s.x / den), -(s.y / den));
+  const C psi = cmk<C>(-(s.x * rden), -(s.y * rden));
   u1 = cmk<C>(u1.x + kx * psi.x, u1.y + kx * psi.y);
   u2 = cmk<C>(u2.x + ky * psi.x, u2.y + ky * psi.y);
   u3 = cmk<C>(u3.x + kz * psi.x, u3.y + kz * psi.y);
@@ -539,11 +546,14 @@ k_xspline(Geo g, const C2<T>* __restrict__ uz, typename V4T<T>::type* __restrict
   load_twiddles<T, N>(tw, tw_g);
   const int zt = blockIdx.x, y = blockIdx.y;
   const int kxn = g.kxn;
-  const int nz0 = N - 2 * kxn + 1;
-  for (int e = threadIdx.x; e < 3 * NPAIR * nz0; e += THREADS)
-    bufU[(e / nz0) * L + pad32(kxn + e % nz0)] = cmk<C>(0, 0);
-  for (int e = threadIdx.x; e < 3 * kxn * NPAIR; e += THREADS) {
-    const int v = e / (kxn * NPAIR), rem = e % (kxn * NPAIR), x = rem / NPAIR, p = rem % NPAIR;
+  for (int e = threadIdx.x; e < 3 * NPAIR * N; e += THREADS) {
+    const int k = e % N;
+    if (k >= kxn && k <= N - kxn) bufU[(e / N) * L + pad32(k)] = cmk<C>(0, 0);
+  }
+  const int pth = threadIdx.x % NPAIR, xth = threadIdx.x / NPAIR, xst = THREADS / NPAIR;
+  for (int v = 0; v < 3; v++)
+  for (int x = xth; x < kxn; x += xst) {
+    const int p = pth;
     const C* src = uz + ((((size_t)v * N + y) * g.nzt + zt) * kxn + x) * TZ + 2 * p;
     const C A = src[0], B = src[1];
     C* line = bufU + (v * NPAIR + p) * L;
