@@ -137,6 +137,7 @@ struct Ctx {
   psdns_params p;
   Geometry g;
   int n, prec, nzt, nab_i, nab_f;
+  int nc = 0, nv = 3;   // passive scalars and stored variables (3 + nc)
   size_t csz;  // sizeof complex element on device
   int *d_colstart = nullptr, *d_ax = nullptr, *d_az = nullptr, *d_kymax = nullptr;
   void *d_tw = nullptr, *d_tabs = nullptr, *d_u = nullptr, *d_un = nullptr, *d_ub = nullptr, *d_uz = nullptr;
@@ -189,7 +190,7 @@ static void prof_collect(Ctx& c, int stage, int k0, int k1) {
 
 template <typename T> struct TabLayout {
   // offsets in bytes inside the stage-table block
-  size_t sx[2], sy[2], sz[2], xf, yf, zf, total;
+  size_t sx[2], sy[2], sz[2], xf, yf, zf, xd, yd, zd, total;
   explicit TabLayout(int n) {
     const size_t c = sizeof(C2<T>), r = sizeof(T);
     size_t o = 0;
@@ -199,6 +200,9 @@ template <typename T> struct TabLayout {
     xf = o; o += r * (n / 2 + 1);
     yf = o; o += r * n;
     zf = o; o += r * n;
+    xd = o; o += r * (n / 2 + 1);
+    yd = o; o += r * n;
+    zd = o; o += r * n;
     total = (o + 255) & ~size_t(255);
   }
 };
@@ -222,6 +226,9 @@ static StageTables<T> make_tables(const Ctx& c, int ks) {
   st.xfac = (const T*)(b + L.xf);
   st.yfac = (const T*)(b + L.yf);
   st.zfac = (const T*)(b + L.zf);
+  st.xdif = (const T*)(b + L.xd);
+  st.ydif = (const T*)(b + L.yd);
+  st.zdif = (const T*)(b + L.zd);
   st.forc = (c.p.kforce > 0) ? (const C2<T>*)c.d_forc : nullptr;
   st.kfor = c.kfor; st.k2fo = c.k2fo;
   st.kforce2 = c.p.kforce * c.p.kforce;
@@ -234,26 +241,28 @@ static StageTables<T> make_tables(const Ctx& c, int ks) {
 }
 
 // ---------------------------------------------------------------------------
-// per-(precision, n) kernel launch sequence
+// per-(precision, n, nc) kernel launch sequence
 // ---------------------------------------------------------------------------
-template <typename T, int N> struct Impl {
+template <typename T, int N, int NC> struct Impl {
   using C = C2<T>;
   using TL = Tiles<T>;
   static constexpr int L = LS<N>::value;
   static constexpr size_t TWB = sizeof(C) * FFTPlan<T, N>::TWSIZE;
   static size_t sm1() { return TWB + sizeof(C) * TL::TB_I * L; }
   static size_t sm2() { return TWB + sizeof(C) * TL::XT2 * L; }
-  static size_t sm3() { return TWB + sizeof(C) * 4 * (TL::TZ / 2) * L; }
+  static size_t sm3() { return TWB + sizeof(C) * (NC ? 6 : 4) * (TL::TZ / 2) * L; }
   static size_t sm4() { return TWB + sizeof(C) * 2 * TL::XT4 * TL::YT4 * L; }
-  static size_t sm5() { return TWB + sizeof(C) * 4 * TL::TB_F * L; }
+  static size_t sm5() { return TWB + sizeof(C) * (4 + NC) * TL::TB_F * L; }
 
   static int setup() {
-    CK(cudaFuncSetAttribute(k_yinv<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1()));
+    CK(cudaFuncSetAttribute(k_yinv<T, N, false, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1()));
+    CK(cudaFuncSetAttribute(k_zinv<T, N, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2()));
+    CK(cudaFuncSetAttribute(k_xchain<T, N, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3()));
+    CK(cudaFuncSetAttribute(k_zfwd<T, N, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm4()));
+    CK(cudaFuncSetAttribute(k_yfwd<T, N, 1, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
+    CK(cudaFuncSetAttribute(k_yfwd<T, N, 2, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
+    // the particle path transforms the velocity only (NC = 0 instances)
     CK(cudaFuncSetAttribute(k_zinv<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2()));
-    CK(cudaFuncSetAttribute(k_xchain<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3()));
-    CK(cudaFuncSetAttribute(k_zfwd<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm4()));
-    CK(cudaFuncSetAttribute(k_yfwd<T, N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
-    CK(cudaFuncSetAttribute(k_yfwd<T, N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
     CK(cudaFuncSetAttribute(k_yinv<T, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1()));
     CK(cudaFuncSetAttribute(k_xspline<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxs()));
     return 0;
@@ -312,26 +321,31 @@ template <typename T, int N> struct Impl {
     {
       constexpr int TH = Launch<T, N, TL::TB_I>::THREADS;
       prof_mark(c, s, 0, 0);
-      k_yinv<T, N><<<dim3(c.nab_i, 3), TH, sm1(), c.stream>>>(g, st, u, ub, tw);
+      k_yinv<T, N, false, NC><<<dim3(c.nab_i, 3 + 2 * NC), TH, sm1(), c.stream>>>(g, st, u, ub, tw);
       prof_mark(c, s, 0, 1);
     }
     {
       constexpr int TH = Launch<T, N, TL::XT2>::THREADS;
       prof_mark(c, s, 1, 0);
-      k_zinv<T, N><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3), TH, sm2(), c.stream>>>(g, ub, uz, tw);
+      k_zinv<T, N, NC><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3 + 3 * NC), TH, sm2(), c.stream>>>(
+          g, ub, uz, tw, st.b11, st.b33);
       prof_mark(c, s, 1, 1);
     }
     {
       constexpr int TH = Launch<T, N, 2 * TL::TZ>::THREADS;
       prof_mark(c, s, 2, 0);
-      k_xchain<T, N><<<dim3(c.nzt, N), TH, sm3(), c.stream>>>(g, uz, tw, st.b11, st.b22, st.b33, c.d_velmax,
-                                                                kstep == 1 ? 1 : 0);
+      // mean-gradient coefficients cb = beta * grad (init.f:42-45)
+      const T cb1 = (T)(c.p.beta1 * c.p.grad[0]), cb2 = (T)(c.p.beta2 * c.p.grad[1]),
+              cb3 = (T)(c.p.beta3 * c.p.grad[2]);
+      k_xchain<T, N, NC><<<dim3(c.nzt, N), TH, sm3(), c.stream>>>(g, uz, tw, st.b11, st.b22, st.b33, c.d_velmax,
+                                                                    kstep == 1 ? 1 : 0, cb1, cb2, cb3);
       prof_mark(c, s, 2, 1);
     }
     {
       constexpr int TH = Launch<T, N, 2 * TL::XT4 * TL::YT4>::THREADS;
       prof_mark(c, s, 3, 0);
-      k_zfwd<T, N><<<dim3(N / TL::YT4, (kxn + TL::XT4 - 1) / TL::XT4), TH, sm4(), c.stream>>>(g, uz, ub, tw, st.b11, st.b33);
+      k_zfwd<T, N, NC><<<dim3(N / TL::YT4, (kxn + TL::XT4 - 1) / TL::XT4), TH, sm4(), c.stream>>>(g, uz, ub, tw,
+                                                                                                   st.b11, st.b33);
       prof_mark(c, s, 3, 1);
     }
     CK(cudaGetLastError());
@@ -342,13 +356,13 @@ template <typename T, int N> struct Impl {
   static int stage_b(Ctx& c, int kstep) {
     Geo g = make_geo(c);
     StageTables<T> st = make_tables<T>(c, kstep - 1);
-    constexpr int TH = Launch<T, N, 4 * TL::TB_F>::THREADS;
+    constexpr int TH = Launch<T, N, (4 + NC) * TL::TB_F>::THREADS;
     prof_mark(c, kstep - 1, 4, 0);
     if (kstep == 1)
-      k_yfwd<T, N, 1><<<c.nab_f, TH, sm5(), c.stream>>>(g, st, (const C*)c.d_ub, (C*)c.d_u, (C*)c.d_un,
+      k_yfwd<T, N, 1, NC><<<c.nab_f, TH, sm5(), c.stream>>>(g, st, (const C*)c.d_ub, (C*)c.d_u, (C*)c.d_un,
                                                         (const C*)c.d_tw, c.d_efkz);
     else
-      k_yfwd<T, N, 2><<<c.nab_f, TH, sm5(), c.stream>>>(g, st, (const C*)c.d_ub, (C*)c.d_u, (C*)c.d_un,
+      k_yfwd<T, N, 2, NC><<<c.nab_f, TH, sm5(), c.stream>>>(g, st, (const C*)c.d_ub, (C*)c.d_u, (C*)c.d_un,
                                                         (const C*)c.d_tw, c.d_efkz);
     prof_mark(c, kstep - 1, 4, 1);
     CK(cudaGetLastError());
@@ -364,15 +378,20 @@ struct Ops {
   int (*particles)(Ctx&);
 };
 
-template <typename T, int N> static Ops ops_for() {
-  return Ops{&Impl<T, N>::setup, &Impl<T, N>::twiddles, &Impl<T, N>::stage_a, &Impl<T, N>::stage_b,
-             &Impl<T, N>::particles};
+template <typename T, int N, int NC> static Ops ops_for() {
+  using I = Impl<T, N, NC>;
+  return Ops{&I::setup, &I::twiddles, &I::stage_a, &I::stage_b, &I::particles};
 }
 
-static bool get_ops(int prec, int n, Ops& o) {
-#define PSDNS_CASE(NN)                                                    \
-  case NN:                                                                \
-    o = (prec == PSDNS_PREC_FP64) ? ops_for<double, NN>() : ops_for<float, NN>(); \
+template <int N> static Ops ops_n(int prec, int nc) {
+  if (prec == PSDNS_PREC_FP64) return nc ? ops_for<double, N, 1>() : ops_for<double, N, 0>();
+  return nc ? ops_for<float, N, 1>() : ops_for<float, N, 0>();
+}
+
+static bool get_ops(int prec, int n, int nc, Ops& o) {
+#define PSDNS_CASE(NN)    \
+  case NN:                \
+    o = ops_n<NN>(prec, nc); \
     return true;
   switch (n) {
     PSDNS_CASE(16)
@@ -455,6 +474,19 @@ static void fill_factor_tables(Ctx& c) {
   for (int y = 0; y < n; y++) yf[y] = (T)std::exp(-(nu * (c.g.ky[y] * c.g.ky[y]) * term));
   term = b33 * c.dt;
   for (int z = 0; z < n; z++) zf[z] = (T)std::exp(-(nu * (c.g.kz[z] * c.g.kz[z]) * term));
+  if (c.nc > 0) {
+    // scalar factors xfac**(1/pr) from the FP64 velocity factors (step.f:387-407)
+    T* xd = (T*)(b + L.xd);
+    T* yd = (T*)(b + L.yd);
+    T* zd = (T*)(b + L.zd);
+    const double ipr = 1. / c.p.pr;
+    term = b11 * c.dt;
+    for (int x = 0; x <= n / 2; x++) xd[x] = (T)std::pow(std::exp(-(nu * (c.g.kx[x] * c.g.kx[x]) * term)), ipr);
+    term = b22 * c.dt;
+    for (int y = 0; y < n; y++) yd[y] = (T)std::pow(std::exp(-(nu * (c.g.ky[y] * c.g.ky[y]) * term)), ipr);
+    term = b33 * c.dt;
+    for (int z = 0; z < n; z++) zd[z] = (T)std::pow(std::exp(-(nu * (c.g.kz[z] * c.g.kz[z]) * term)), ipr);
+  }
 }
 
 static int upload_tables(Ctx& c) {
@@ -594,7 +626,8 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
   if (!p || !out) return set_error("null argument");
   *out = nullptr;
   if (p->nx != p->ny || p->nx != p->nz) return set_error("only cubic boxes are supported (nx=ny=nz)");
-  if (p->nc != 0) return set_error("nc=%d: passive scalars are not supported by this build", p->nc);
+  if (p->nc != 0 && p->nc != 1) return set_error("nc=%d: 0 or 1 passive scalars are supported", p->nc);
+  if (p->nc == 1 && !(p->pr > 0.)) return set_error("Schmidt number pr must be positive");
   if (p->precision != PSDNS_PREC_FP32 && p->precision != PSDNS_PREC_FP64)
     return set_error("precision must be PSDNS_PREC_FP32 or PSDNS_PREC_FP64");
   if (p->kshift < 1 || p->kshift > 4) return set_error("kshift must be 1..4");
@@ -603,11 +636,13 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
   if (p->seed_input <= 0) return set_error("seed iseed=%d must be positive (ranu.f:33)", p->seed_input);
   if (p->cfl <= 0. && !(p->dt > 0.)) return set_error("fixed dt must be positive when cfl <= 0");
   Ops o;
-  if (!get_ops(p->precision, p->nx, o)) return set_error("grid size %d not supported (16..1024, powers of 2)", p->nx);
+  if (!get_ops(p->precision, p->nx, p->nc, o)) return set_error("grid size %d not supported (16..1024, powers of 2)", p->nx);
   Ctx* c = new Ctx();
   c->p = *p;
   c->n = p->nx;
   c->prec = p->precision;
+  c->nc = p->nc;
+  c->nv = 3 + p->nc;
   build_geometry(c->n, c->g);
   const int n = c->n;
   const bool dbl = c->prec == PSDNS_PREC_FP64;
@@ -618,9 +653,11 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
   c->nzt = n / tz;
   c->nab_i = (c->g.xz_tot + tbi - 1) / tbi;
   c->nab_f = (c->g.xz_tot + tbf - 1) / tbf;
-  c->ub_elems = std::max((size_t)3 * c->nab_i * tbi, (size_t)4 * c->nab_f * tbf) * n;
-  c->uz_elems = (size_t)5 * n * n * c->g.kxn;
-  c->st_elems = (size_t)3 * c->g.xz_tot * n;
+  // ub: 3 + 2 nc backward variables (TB_I blocks) or 4 + nc forward terms
+  // (TB_F blocks); uz: 5 + nc slots (3 + 3 nc inputs, 5 + nc outputs)
+  c->ub_elems = std::max((size_t)(3 + 2 * c->nc) * c->nab_i * tbi, (size_t)(4 + c->nc) * c->nab_f * tbf) * n;
+  c->uz_elems = (size_t)(5 + c->nc) * n * n * c->g.kxn;
+  c->st_elems = (size_t)c->nv * c->g.xz_tot * n;
   c->rng.init(p->seed_input);
   c->dt0 = p->dt;
   c->dt = p->dt;
@@ -719,7 +756,7 @@ int psdns_gpu_set_state(void* ctx, const double* un, int32_t layout) {
   if (layout != PSDNS_LAYOUT_YCYL) return set_error("unsupported layout %d", layout);
   const size_t vs = (size_t)c->g.xz_tot * c->n;
   // stage one variable at a time: ub holds >= 2 variables of complex double
-  for (int v = 0; v < 3; v++) {
+  for (int v = 0; v < c->nv; v++) {
     CK(cudaMemcpyAsync(c->d_ub, un + 2 * v * vs, sizeof(double2) * vs, cudaMemcpyHostToDevice, c->stream));
     const int blocks = 148 * 8;
     if (c->prec == PSDNS_PREC_FP64)
@@ -741,7 +778,7 @@ int psdns_gpu_get_state(void* ctx, double* out, int32_t which, int32_t layout) {
   if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
   const size_t vs = (size_t)c->g.xz_tot * c->n;
   void* src = which == PSDNS_FIELD_U ? c->d_u : c->d_un;
-  for (int v = 0; v < 3; v++) {
+  for (int v = 0; v < c->nv; v++) {
     const int blocks = 148 * 8;
     if (c->prec == PSDNS_PREC_FP64)
       k_to_f64<double><<<blocks, 256, 0, c->stream>>>((const double2*)src + v * vs, (double2*)c->d_ub, vs);
@@ -758,7 +795,7 @@ int psdns_gpu_step(void* ctx, double* info) {
   Ctx* c = (Ctx*)ctx;
   if (!c) return set_error("null context");
   Ops o;
-  if (!get_ops(c->prec, c->n, o)) return set_error("bad context");
+  if (!get_ops(c->prec, c->n, c->nc, o)) return set_error("bad context");
   c->jstep += 1;
   draw_shifts(*c);
   if (c->prec == PSDNS_PREC_FP64) fill_shift_tables<double>(*c); else fill_shift_tables<float>(*c);
@@ -794,7 +831,7 @@ int psdns_gpu_rk_stage(void* ctx, int32_t kstep, const double* gsh, const double
   if (forcing != nullptr && !(c->p.kforce > 0))
     return set_error("a forcing table was passed but the context was created with kforce = 0");
   Ops o;
-  if (!get_ops(c->prec, c->n, o)) return set_error("bad context");
+  if (!get_ops(c->prec, c->n, c->nc, o)) return set_error("bad context");
   for (int i = 0; i < 3; i++) { c->gsh[i][0] = gsh[i]; c->gsh[i][1] = gsh[3 + i]; }
   if (c->prec == PSDNS_PREC_FP64) fill_shift_tables<double>(*c); else fill_shift_tables<float>(*c);
   if (kstep == 1) {
@@ -834,6 +871,12 @@ int psdns_gpu_field_init(void* ctx, int32_t seed) {
   if (seed <= 0) return set_error("seed %d must be positive (ranu.f:33)", seed);
   const Geometry& g = c->g;
   const int n = c->n;
+  if (c->nc > 0) {
+    // the scalar starts from zero fluctuations (incond.f:49, kinit = 0)
+    const size_t vs = (size_t)g.xz_tot * n;
+    CK(cudaMemsetAsync((char*)c->d_u + 3 * vs * c->csz, 0, vs * c->csz, c->stream));
+    CK(cudaMemsetAsync((char*)c->d_un + 3 * vs * c->csz, 0, vs * c->csz, c->stream));
+  }
   // offsets of each column's first draw (in modes) in the traversal order
   std::vector<long long> off(g.xz_tot);
   long long acc = 0;
@@ -850,6 +893,7 @@ int psdns_gpu_field_init(void* ctx, int32_t seed) {
   if (e != cudaSuccess) { cudaFree(d_off); return set_error("upload failed: %s", cudaGetErrorString(e)); }
   Geo geo = make_geo(*c);
   const double s1 = c->p.beta1, s2 = c->p.beta2, s3 = c->p.beta3;
+
   const int kc0 = n / 2 - 1 - g.cut[0];
   if (c->prec == PSDNS_PREC_FP64) {
     k_field_init<double><<<148 * 8, 256, 0, c->stream>>>(geo, d_off, (uint32_t)seed, s1, s2, s3, (double2*)c->d_un,

@@ -39,6 +39,9 @@ template <typename T> struct StageTables {
   const T* xfac;     // [n/2+1] integrating factors
   const T* yfac;     // [n]
   const T* zfac;     // [n]
+  const T* xdif;     // [n/2+1] scalar factors xfac^(1/Sc) (step.f:387-407)
+  const T* ydif;     // [n]
+  const T* zdif;     // [n]
   const C2<T>* forc; // for(kfor,k2fo,k2fo,3) or null
   int kfor, k2fo;
   double kforce2;    // kforce^2
@@ -82,10 +85,12 @@ template <int N> struct LS { static constexpr int value = N + N / 32 + 4; };
 // K1: phase shift + mask + y backward FFT, transposed store to ub (TB_I block)
 // grid (ceil(xz_tot/TB_I), 3); one block = one ub block of TB_I columns
 // ---------------------------------------------------------------------------
-template <typename T, int N, bool SPL = false>
+template <typename T, int N, bool SPL = false, int NC = 0>
 __global__ void __launch_bounds__(Launch<T, N, Tiles<T>::TB_I>::THREADS)
 k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict__ ub,
        const C2<T>* __restrict__ tw_g) {
+  // NC = 1 (one passive scalar, grid.y = 5): ub variable 3 is the shifted
+  // scalar and variable 4 its y gradient i b22 ky theta (phase1.f:52-64)
   // SPL: also divide by the cubic B-spline symbol, (4 + 2 cos(2 pi k/n))/6 per
   // axis, so that the backward transform yields the periodic spline
   // coefficients of the shifted-grid field (the circulant tridiagonal systems
@@ -99,6 +104,7 @@ k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict_
   C* buf = tw + FFTPlan<T, N>::TWSIZE;
   load_twiddles<T, N>(tw, tw_g);
   const int at = blockIdx.x, v = blockIdx.y;
+  const int src = v < 3 ? v : 3;
   const int a0 = at * TB;
   const size_t vs = (size_t)g.xz_tot * N;
   for (int e = threadIdx.x; e < TB * N; e += THREADS) {
@@ -107,7 +113,13 @@ k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict_
     if (a < g.xz_tot && mask_ok(g, a, y, N)) {
       C sxz = cmul(__ldg(st.sx + __ldg(g.ax + a)), __ldg(st.sz + __ldg(g.az + a)));
       C sh = cmul(__ldg(st.sy + y), sxz);
-      val = cmul(u[v * vs + (size_t)a * N + y], sh);
+      val = cmul(u[src * vs + (size_t)a * N + y], sh);
+      if constexpr (NC > 0) {
+        if (v == 4) {
+          const T bk = st.b22 * T(kwave<N>(y));
+          val = cmk<C>(-bk * val.y, bk * val.x);
+        }
+      }
       if constexpr (SPL) {
         const T f = __ldg(st.spf + __ldg(g.ax + a)) * __ldg(st.spf + (N / 2 + 1) + y) *
                     __ldg(st.spf + (N / 2 + 1) + N + __ldg(g.az + a));
@@ -129,9 +141,13 @@ k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict_
 // K2: cylinder unpack (zero fill) + z backward FFT, store to uz
 // grid (n, ceil(kxn/XT2), 3)
 // ---------------------------------------------------------------------------
-template <typename T, int N>
+template <typename T, int N, int NC = 0>
 __global__ void __launch_bounds__(Launch<T, N, Tiles<T>::XT2>::THREADS)
-k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g) {
+k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11 = T(1),
+       T b33 = T(1)) {
+  // NC = 1 (grid.z = 6): uz slot 3 = y gradient of the scalar (ub 4), slot
+  // 4 = i b11 kx theta and slot 5 = i b33 kz theta (both from ub 3),
+  // itransform.f:188-198
   using C = C2<T>;
   constexpr int XT = Tiles<T>::XT2, TB = Tiles<T>::TB_I, TZ = Tiles<T>::TZ;
   constexpr int THREADS = Launch<T, N, XT>::THREADS;
@@ -146,10 +162,17 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
   for (int e = threadIdx.x; e < XT * N; e += THREADS) buf[(e / N) * L + pad32(e % N)] = cmk<C>(0, 0);
   __syncthreads();
   const int abeg = __ldg(g.colstart + x0), aend = __ldg(g.colstart + x1);
-  const C* src = ub + (size_t)v * g.nab_i * N * TB;
+  const int sv = v < 3 ? v : (v == 3 ? 4 : 3);
+  const C* src = ub + (size_t)sv * g.nab_i * N * TB;
   for (int a = abeg + threadIdx.x; a < aend; a += THREADS) {
     const int l = __ldg(g.ax + a) - x0, z = __ldg(g.az + a);
     C val = src[((size_t)(a / TB) * N + y) * TB + (a % TB)];
+    if constexpr (NC > 0) {
+      if (v >= 4) {
+        const T bk = v == 4 ? b11 * T(x0 + l) : b33 * T(kwave<N>(z));
+        val = cmk<C>(-bk * val.y, bk * val.x);
+      }
+    }
     buf[l * L + pad32(z)] = cconj(val);
   }
   __syncthreads();
@@ -192,12 +215,16 @@ __device__ __forceinline__ void xchain_store(const Geo& g, const C2<T>* buf, int
   }
 }
 
-template <typename T, int N>
+template <typename T, int N, int NC = 0>
 __global__ void __launch_bounds__(Launch<T, N, 2 * Tiles<T>::TZ>::THREADS)
 k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T b22, T b33,
-         unsigned long long* velmax_bits, int want_velmax) {
+         unsigned long long* velmax_bits, int want_velmax, T cb1 = T(0), T cb2 = T(0), T cb3 = T(0)) {
+  // NC = 1: inputs also hold the scalar gradient (slots 3 = d/dy, 4 = d/dx,
+  // 5 = d/dz); the advection term u.(G + grad theta) (itransform.f:522-530,
+  // G = cb, init.f:42-45) is formed in physical space and goes to slot 5.
   using C = C2<T>;
   constexpr int TZ = Tiles<T>::TZ, NPAIR = TZ / 2;
+  constexpr int NVIN = 3 + 3 * NC;
   constexpr int THREADS = Launch<T, N, 2 * TZ>::THREADS;
   constexpr int L = LS<N>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -205,12 +232,12 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
   C* bufU = tw + FFTPlan<T, N>::TWSIZE;
   C* bufV = bufU + NPAIR * L;
   C* bufW = bufV + NPAIR * L;
-  C* bufE = bufW + NPAIR * L;
+  C* bufE = bufW + NPAIR * L;   // with NC = 1 this is the y-gradient buffer until the scalar term is done
   load_twiddles<T, N>(tw, tw_g);
   const int zt = blockIdx.x, y = blockIdx.y;
   const int kxn = g.kxn;
   // zero the band kx in [kxn, n-kxn] (includes the Nyquist column)
-  for (int e = threadIdx.x; e < 3 * NPAIR * N; e += THREADS) {
+  for (int e = threadIdx.x; e < NVIN * NPAIR * N; e += THREADS) {
     const int k = e % N;
     if (k >= kxn && k <= N - kxn) bufU[(e / N) * L + pad32(k)] = cmk<C>(0, 0);
   }
@@ -218,7 +245,7 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
   // Hermitian extension and the imaginary part of the kx=0 term dropped;
   // stored conjugated (backward transform by conjugation)
   const int pth = threadIdx.x % NPAIR, xth = threadIdx.x / NPAIR, xst = THREADS / NPAIR;
-  for (int v = 0; v < 3; v++)
+  for (int v = 0; v < NVIN; v++)
   for (int x = xth; x < kxn; x += xst) {
     const int p = pth;
     const C* src = uz + ((((size_t)v * N + y) * g.nzt + zt) * kxn + x) * TZ + 2 * p;
@@ -232,8 +259,25 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
     }
   }
   __syncthreads();
-  fft_lines<T, N, THREADS>(bufU, 3 * NPAIR, L, tw);
+  fft_lines<T, N, THREADS>(bufU, NVIN * NPAIR, L, tw);
   // buffers now hold conj(a + i b): a = re, b = -im
+  const T hf = T(0.5) / T(N);
+  if constexpr (NC > 0) {
+    C* bufGY = bufW + NPAIR * L;
+    C* bufGX = bufGY + NPAIR * L;
+    C* bufGZ = bufGX + NPAIR * L;
+    for (int e = threadIdx.x; e < NPAIR * N; e += THREADS) {
+      const int i = (e / N) * L + pad32(e % N);
+      const C U = bufU[i], V = bufV[i], W = bufW[i], GY = bufGY[i], GX = bufGX[i], GZ = bufGZ[i];
+      const T sa = U.x * (cb1 + GX.x) + V.x * (cb2 + GY.x) + W.x * (cb3 + GZ.x);
+      const T sb = (-U.y) * (cb1 - GX.y) + (-V.y) * (cb2 - GY.y) + (-W.y) * (cb3 - GZ.y);
+      bufGX[i] = cmk<C>(sa, sb);
+    }
+    __syncthreads();
+    fft_lines<T, N, THREADS>(bufGX, NPAIR, L, tw);
+    xchain_store<T, N>(g, bufGX, 1, L, uz, 5, y, zt, hf);   // scalar advection term
+    __syncthreads();
+  }
   double vm = 0.0;
   const double xn = (double)b11 * N, yn = (double)b22 * N, zn = (double)b33 * N;
   for (int e = threadIdx.x; e < NPAIR * N; e += THREADS) {
@@ -252,7 +296,6 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
     if ((threadIdx.x & 31) == 0) atomic_max_pos<T>(velmax_bits, vm);
   }
   __syncthreads();
-  const T hf = T(0.5) / T(N);
   fft_lines<T, N, THREADS>(bufE, NPAIR, L, tw);
   xchain_store<T, N>(g, bufE, 1, L, uz, 4, y, zt, hf);   // slot is2 = 5: u*w
   __syncthreads();
@@ -337,10 +380,12 @@ __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const 
   }
 }
 
-template <typename T, int N>
+template <typename T, int N, int NC = 0>
 __global__ void __launch_bounds__(Launch<T, N, 2 * Tiles<T>::XT4 * Tiles<T>::YT4>::THREADS)
 k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>* __restrict__ tw_g,
        T b11, T b33) {
+  // NC = 1: the scalar advection term (uz slot 5) goes to ub slot 4 without
+  // derivatives (transform.f: i2f = 4+nc)
   // grid (n / YT4, ceil(kxn / XT4)): YT4 adjacent y rows x XT4 x lines
   using C = C2<T>;
   constexpr int XT = Tiles<T>::XT4, YT = Tiles<T>::YT4, NLT = XT * YT;
@@ -385,6 +430,13 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
   }
   zfwd_store<T, N, 2>(g, s0, s1, L, ub, 1, y0, YT, x0, x1, b11, b33);
   zfwd_store<T, N, 3>(g, s0, s1, L, ub, 3, y0, YT, x0, x1, b11, b33);
+  if constexpr (NC > 0) {
+    __syncthreads();
+    zfwd_load<T, N>(g, uz, 5, y0, YT, x0, nl, s1, L);
+    __syncthreads();
+    fft_lines<T, N, THREADS>(s1, nt, L, tw);
+    zfwd_store<T, N, 3>(g, s0, s1, L, ub, 4, y0, YT, x0, x1, b11, b33);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -407,20 +459,24 @@ __device__ __forceinline__ void project3(C2<T>& u1, C2<T>& u2, C2<T>& u3, T kx, 
   u3 = cmk<C>(u3.x + kz * psi.x, u3.y + kz * psi.y);
 }
 
-template <typename T, int N, int KSTEP>
-__global__ void __launch_bounds__(Launch<T, N, 4 * Tiles<T>::TB_F>::THREADS)
+template <typename T, int N, int KSTEP, int NC = 0>
+__global__ void __launch_bounds__(Launch<T, N, (4 + NC) * Tiles<T>::TB_F>::THREADS)
 k_yfwd(Geo g, StageTables<T> st, const C2<T>* __restrict__ ub, C2<T>* __restrict__ u,
        C2<T>* __restrict__ un, const C2<T>* __restrict__ tw_g, double* __restrict__ efkz) {
+  // NC = 1: ub slot 4 is the scalar advection term; the scalar is un-shifted
+  // (wavespace_module.f:344-357) and advanced with the diffusivity factors
+  // xdif ydif zdif (proc4a.f:508-522, proc4b.f:69-75), without projection
   using C = C2<T>;
   constexpr int TB = Tiles<T>::TB_F;
-  constexpr int THREADS = Launch<T, N, 4 * TB>::THREADS;
+  constexpr int NVF = 4 + NC;
+  constexpr int THREADS = Launch<T, N, NVF * TB>::THREADS;
   constexpr int L = LS<N>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   C* buf = tw + FFTPlan<T, N>::TWSIZE;   // [4][TB] lines
   load_twiddles<T, N>(tw, tw_g);
   const int at = blockIdx.x, a0 = at * TB;
-  for (int v = 0; v < 4; v++) {
+  for (int v = 0; v < NVF; v++) {
     const C* src = ub + ((size_t)v * g.nab_f + at) * N * TB;
     for (int e = threadIdx.x; e < TB * N; e += THREADS) {
       const int y = e / TB, l = e % TB;
@@ -428,7 +484,7 @@ k_yfwd(Geo g, StageTables<T> st, const C2<T>* __restrict__ ub, C2<T>* __restrict
     }
   }
   __syncthreads();
-  fft_lines<T, N, THREADS>(buf, 4 * TB, L, tw);
+  fft_lines<T, N, THREADS>(buf, NVF * TB, L, tw);
   const size_t vs = (size_t)g.xz_tot * N;
   for (int e = threadIdx.x; e < TB * N; e += THREADS) {
     const int l = e / N, y = e % N, a = a0 + l;
@@ -438,6 +494,7 @@ k_yfwd(Geo g, StageTables<T> st, const C2<T>* __restrict__ ub, C2<T>* __restrict
       u[o] = cmk<C>(0, 0);
       u[vs + o] = cmk<C>(0, 0);
       u[2 * vs + o] = cmk<C>(0, 0);
+      if constexpr (NC > 0) u[3 * vs + o] = cmk<C>(0, 0);
       continue;
     }
     const int x = __ldg(g.ax + a), z = __ldg(g.az + a);
@@ -510,6 +567,22 @@ k_yfwd(Geo g, StageTables<T> st, const C2<T>* __restrict__ ub, C2<T>* __restrict
           u3 = cadd(u3, f3);
         }
       }
+    }
+    if constexpr (NC > 0) {
+      const C V5 = buf[(4 * TB + l) * L + i];
+      const C w4 = cmul(sxyz, V5);
+      C n4 = un[3 * vs + o], u4;
+      if constexpr (KSTEP == 1) {
+        const T fs = __ldg(st.xdif + x) * __ldg(st.ydif + y) * __ldg(st.zdif + z);
+        u4 = cscale(fs, cmk<C>(n4.x + T(2) * w4.x, n4.y + T(2) * w4.y));
+        n4 = cscale(fs, cadd(n4, w4));
+      } else {
+        u4 = cadd(n4, w4);
+        if (k0) u4 = cmk<C>(0, 0);
+        n4 = u4;
+      }
+      u[3 * vs + o] = u4;
+      un[3 * vs + o] = n4;
     }
     if constexpr (KSTEP == 2) {
       if (k0) {

@@ -171,6 +171,7 @@ static int run(const psdns_params* prm, int kstep, const double* gsh, double dt,
   stb.xfac = (const T*)(base + pl.tabs + 2 * (N / 2 + 1 + 2 * N) * cs);
   stb.yfac = stb.xfac + (N / 2 + 1);
   stb.zfac = stb.yfac + N;
+  stb.xdif = stb.ydif = stb.zdif = nullptr;   // no scalar on this path
   stb.forc = nullptr;
   stb.kfor = 0; stb.k2fo = 0; stb.kforce2 = 0;
   stb.b11 = (T)b11; stb.b22 = (T)b22; stb.b33 = (T)b33;

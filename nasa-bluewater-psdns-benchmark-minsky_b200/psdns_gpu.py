@@ -175,6 +175,7 @@ class Solver:
         self._ctx = ctypes.c_void_p()
         _check(L.psdns_gpu_init(ctypes.byref(self.params), ctypes.byref(self._ctx)), "psdns_gpu_init")
         self.n = self.params.nx
+        self.nc = self.params.nc
         g = geometry(self.n)
         self.kxn = g["kxn"]
         self.xz_tot = g["xz_tot"]
@@ -191,7 +192,8 @@ class Solver:
             pass
 
     def state_shape(self):
-        return (3, self.xz_tot, self.n)
+        """(3 + nc, xz_tot, n): velocity components, then the scalar."""
+        return (3 + self.nc, self.xz_tot, self.n)
 
     def set_state(self, un):
         a = np.ascontiguousarray(un, dtype=np.complex128)

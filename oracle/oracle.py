@@ -58,6 +58,8 @@ def lib():
         L.orc_spectra.argtypes = [vp, ctypes.c_int, dp, dp, dp, dp]
         L.orc_particles_set.argtypes = [vp, ctypes.c_long, dp]
         L.orc_particles_get.argtypes = [vp, dp, dp]
+        L.orc_set_scalar.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double]
         _LIB = L
     return _LIB
 
@@ -91,6 +93,7 @@ class Oracle:
     def __init__(self, n, viscos, cfl=-1.0, dt=0.005, kshift=1, seed_input=122929298, ksran=1,
                  beta=(1.0, 1.0, 1.0)):
         self.n = n
+        self.nc = 0
         self._c = lib().orc_create(n, viscos, cfl, dt, kshift, seed_input, ksran, *beta)
         self.kxn = lib().orc_kxn(self._c)
         self.xz_tot = lib().orc_xz_tot(self._c)
@@ -114,12 +117,19 @@ class Oracle:
         lib().orc_geometry(self._c, _ip(cut), _ip(col), _ip(kym), _ip(az))
         return {"cut": cut, "colstart": col, "kymax": kym, "az": az}
 
+    def set_scalar(self, pr=1.0, grad=(0.0, 1.0, 0.0)):
+        """One passive scalar (nc = 1): Schmidt number pr, mean gradient grad.
+        The state grows to 4 variables; the scalar starts at zero."""
+        lib().orc_set_scalar(self._c, 1, float(pr), *[float(g) for g in grad])
+        self.nc = 1
+
     def state_shape(self):
-        return (3, self.xz_tot, self.n)
+        return (3 + self.nc, self.xz_tot, self.n)
 
     def field_init(self, seed):
+        """Velocity of field.f (3 variables); a scalar is left at zero."""
         out = np.zeros(self.state_shape(), np.complex128)
-        lib().orc_field_init(self._c, int(seed), _dp(out.view(np.float64)))
+        lib().orc_field_init(self._c, int(seed), _dp(out[:3].view(np.float64)))
         return out
 
     def set_state(self, un):

@@ -168,14 +168,17 @@ typedef struct {
     double b11, b22, b33;  /* init.f:33-37 (beta^2) */
     double viscos, cfl, dt0, dt, dt2, time, velmax;
     int kshift, ksran;
-    int nc;
+    int nc;                /* passive scalars: 0 or 1 */
+    double beta[3];        /* init.f:33-37 */
+    double pr, cb[3];      /* Schmidt number; cb = beta * grad (init.f:42-45) */
+    double *xdif, *ydif, *zdif;  /* step.f:387-407 */
     orc_rng rng;
     double gsh[3][2];      /* shifts.f */
     double gsh4[3][2];     /* gsh(:,3:4) drawn by the RKFOUR-compiled build */
     int jstep;
     cx *sx, *sy, *sz;      /* [2][n]: shifts.f:146-178 */
     double *xfac, *yfac, *zfac;  /* step.f:366-385 */
-    cx *u, *un;            /* [3][xz_tot][n] */
+    cx *u, *un;            /* [3+nc][xz_tot][n] */
     fft_tw tw;
     int status;
     /* Eswaran-Pope forcing (force.f, vfuo.f, vfiuo.f, raniuo.f, rann2.f) */
@@ -269,6 +272,8 @@ orc_ctx *orc_create(int n, double viscos, double cfl, double dt, int kshift,
     c->viscos = viscos; c->cfl = cfl; c->dt0 = dt; c->dt = dt;
     c->kshift = kshift; c->ksran = ksran;
     c->b11 = beta1 * beta1; c->b22 = beta2 * beta2; c->b33 = beta3 * beta3;
+    c->beta[0] = beta1; c->beta[1] = beta2; c->beta[2] = beta3;
+    c->pr = 1.0;
     rng_init(&c->rng, seed_input);
     geom_build(c);
     size_t nst = (size_t)3 * c->xz_tot * n;
@@ -280,6 +285,9 @@ orc_ctx *orc_create(int n, double viscos, double cfl, double dt, int kshift,
     c->xfac = (double *)calloc((size_t)n, sizeof(double));
     c->yfac = (double *)calloc((size_t)n, sizeof(double));
     c->zfac = (double *)calloc((size_t)n, sizeof(double));
+    c->xdif = (double *)calloc((size_t)n, sizeof(double));
+    c->ydif = (double *)calloc((size_t)n, sizeof(double));
+    c->zdif = (double *)calloc((size_t)n, sizeof(double));
     tw_make(&c->tw, n);
     return c;
 }
@@ -290,6 +298,7 @@ void orc_destroy(orc_ctx *c)
     free(c->kx); free(c->ky); free(c->kz); free(c->cut); free(c->kc); free(c->colstart);
     free(c->ax); free(c->az); free(c->kymax); free(c->u); free(c->un);
     free(c->sx); free(c->sy); free(c->sz); free(c->xfac); free(c->yfac); free(c->zfac);
+    free(c->xdif); free(c->ydif); free(c->zdif);
     free(c->tw.w);
     free(c->pp);
     free(c->suo); free(c->svo); free(c->velinc); free(c->w1); free(c->w2); free(c->forc); free(c->efkz);
@@ -306,19 +315,36 @@ void orc_geometry(orc_ctx *c, int *cut, int *colstart, int *kymax, int *az)
     memcpy(az, c->az, sizeof(int) * (size_t)c->xz_tot);
 }
 
-/* state I/O: [3][xz_tot][n] complex (re,im interleaved), the reference's
- * uy(ny,num_al,3) layout.  set_state copies un into both un and u
+/* One passive scalar (nc = 1) with Schmidt number pr and mean gradient
+ * grad (input records of input.f; cb = beta * grad, init.f:42-45).  The
+ * state grows to 4 variables; the scalar starts at zero (incond.f:49). */
+void orc_set_scalar(orc_ctx *c, int nc, double pr, double g1, double g2, double g3)
+{
+    size_t vs = (size_t)c->xz_tot * c->n;
+    c->nc = nc ? 1 : 0;
+    c->pr = pr;
+    c->cb[0] = c->beta[0] * g1; c->cb[1] = c->beta[1] * g2; c->cb[2] = c->beta[2] * g3;
+    c->u = (cx *)realloc(c->u, sizeof(cx) * (3 + c->nc) * vs);
+    c->un = (cx *)realloc(c->un, sizeof(cx) * (3 + c->nc) * vs);
+    if (c->nc) {
+        memset(c->u + 3 * vs, 0, sizeof(cx) * vs);
+        memset(c->un + 3 * vs, 0, sizeof(cx) * vs);
+    }
+}
+
+/* state I/O: [3+nc][xz_tot][n] complex (re,im interleaved), the reference's
+ * uy(ny,num_al,3+nc) layout.  set_state copies un into both un and u
  * (incond.f:146). */
 void orc_set_state(orc_ctx *c, const double *un)
 {
-    size_t nst = (size_t)3 * c->xz_tot * c->n;
+    size_t nst = (size_t)(3 + c->nc) * c->xz_tot * c->n;
     memcpy(c->un, un, nst * sizeof(cx));
     memcpy(c->u, un, nst * sizeof(cx));
 }
 
 void orc_get_state(orc_ctx *c, double *u, double *un)
 {
-    size_t nst = (size_t)3 * c->xz_tot * c->n;
+    size_t nst = (size_t)(3 + c->nc) * c->xz_tot * c->n;
     if (u) memcpy(u, c->u, nst * sizeof(cx));
     if (un) memcpy(un, c->un, nst * sizeof(cx));
 }
@@ -429,6 +455,9 @@ static void phase_shift(orc_ctx *c, cx *u, int nv, int ks)
  * pencils with zero fill of the cut band, :205-255), the z backward FFT with
  * the Nyquist row zeroed (itransform_vel.f:80-94) and kxcomm2.f (x backward
  * complex-to-real, kx >= kxn zero padded, :308-321).
+ * nv = 6 carries one scalar: u[3] = its y gradient, u[4] and u[5] the
+ * shifted scalar, multiplied in the z pencils by i b11 kx and i b33 kz
+ * (itransform.f:188-198).
  * in: u[v][a][y] (overwritten: y transformed), out: p[v][y][z][x] real. */
 static void itransform(orc_ctx *c, cx *u, int nv, double *p)
 {
@@ -454,6 +483,13 @@ static void itransform(orc_ctx *c, cx *u, int nv, double *p)
                     for (int a = c->colstart[x]; a < c->colstart[x + 1]; a++)
                         line[c->az[a]] = u[((size_t)v * tot + a) * n + y];
                     line[n / 2] = CZERO;
+                    if (nv == 6 && v == 4) {
+                        cx bk1i = cmk(0.0, c->b11 * c->kx[x]);
+                        for (int z = 0; z < n; z++) if (z != n / 2) line[z] = cmul(bk1i, line[z]);
+                    } else if (nv == 6 && v == 5) {
+                        for (int z = 0; z < n; z++)
+                            if (z != n / 2) line[z] = cmul(cmk(0.0, c->b33 * c->kz[z]), line[z]);
+                    }
                     fft_line(line, tmp, n, +1, &c->tw);
                 }
         free(tmp);
@@ -484,7 +520,9 @@ static void itransform(orc_ctx *c, cx *u, int nv, double *p)
 }
 
 /* realspace_vel.f:61-118 (stage 1, with velmax) and :143-178 (stage 2).
- * in: p[0..2] = u,v,w ; out: p[0..4] = b11 u^2 - bv2, uv, b33 w^2 - bv2, vw, uw */
+ * in: p[0..2] = u,v,w ; out: p[0..4] = b11 u^2 - bv2, uv, b33 w^2 - bv2, vw, uw.
+ * With a scalar, in: p[3..5] = its y, x, z gradients; out: p[5] = the
+ * advection term u.(cb + grad theta) (itransform.f:522-530). */
 static double realspace(orc_ctx *c, double *p, int want_velmax)
 {
     int n = c->n;
@@ -494,6 +532,13 @@ static double realspace(orc_ctx *c, double *p, int want_velmax)
     #pragma omp parallel for reduction(max:vm) schedule(static)
     for (long i = 0; i < (long)np; i++) {
         double u = p[i], v = p[np + i], w = p[2 * np + i];
+        if (c->nc) {
+            double gy = p[3 * np + i], gx = p[4 * np + i], gz = p[5 * np + i];
+            double term1 = u * (c->cb[0] + gx);
+            double term2 = v * (c->cb[1] + gy);
+            double term3 = w * (c->cb[2] + gz);
+            p[5 * np + i] = term1 + term2 + term3;
+        }
         double bv2 = c->b22 * v * v;
         p[4 * np + i] = u * w;
         p[3 * np + i] = v * w;
@@ -512,19 +557,22 @@ static double realspace(orc_ctx *c, double *p, int want_velmax)
  * z forward FFT (transform.f:129-138), derivative combination
  * (transform.f:230-234, Nyquist z row skipped), cylinder gather keeping
  * |kz| <= kc(x) (xkcomm2.f:96-125) and y forward FFT (xkcomm2.f:229).
- * in: p[5][y][z][x] ; out: u[4][a][y] */
+ * A scalar's advection term (p[5]) is transformed without derivatives into
+ * u[4] (transform.f: i2f = 4 + nc).
+ * in: p[5+nc][y][z][x] ; out: u[4+nc][a][y] */
 static void transform(orc_ctx *c, const double *p, cx *u)
 {
     int n = c->n, kxn = c->kxn, tot = c->xz_tot;
+    int nvp = 5 + c->nc;
     double factor = 1. / (double)n;
-    cx *zl = (cx *)calloc((size_t)5 * n * kxn * n, sizeof(cx));
+    cx *zl = (cx *)calloc((size_t)nvp * n * kxn * n, sizeof(cx));
     /* x r2c, scale, transpose to z pencils zl[v][y][x][z] */
     #pragma omp parallel
     {
         cx *line = (cx *)malloc(sizeof(cx) * (size_t)n);
         cx *tmp = (cx *)malloc(sizeof(cx) * (size_t)n);
         #pragma omp for schedule(static) collapse(2)
-        for (int v = 0; v < 5; v++)
+        for (int v = 0; v < nvp; v++)
             for (int y = 0; y < n; y++)
                 for (int z = 0; z < n; z++) {
                     const double *in = p + (((size_t)v * n + y) * n + z) * n;
@@ -540,7 +588,7 @@ static void transform(orc_ctx *c, const double *p, cx *u)
     {
         cx *tmp = (cx *)malloc(sizeof(cx) * (size_t)n);
         #pragma omp for schedule(static)
-        for (long l = 0; l < (long)5 * n * kxn; l++) fft_line(zl + l * n, tmp, n, -1, &c->tw);
+        for (long l = 0; l < (long)nvp * n * kxn; l++) fft_line(zl + l * n, tmp, n, -1, &c->tw);
         free(tmp);
     }
     /* derivative combination, m = 2 mesh (b11(2) = b11 etc.) */
@@ -560,16 +608,18 @@ static void transform(orc_ctx *c, const double *p, cx *u)
                 zl[2 * vs + o] = cadd(cmul(bk1i2, u5), cmul(bk3i2, u3));
             }
         }
-    /* cylinder gather (4 variables: slots 1,2,3,4) and y forward */
+    /* cylinder gather (4 variables: slots 1,2,3,4; the scalar term as the
+     * fifth, taken from zl variable 5) and y forward */
     #pragma omp parallel
     {
         cx *tmp = (cx *)malloc(sizeof(cx) * (size_t)n);
         #pragma omp for schedule(static) collapse(2)
-        for (int v = 0; v < 4; v++)
+        for (int v = 0; v < 4 + c->nc; v++)
             for (int a = 0; a < tot; a++) {
                 cx *line = u + ((size_t)v * tot + a) * n;
                 int x = c->ax[a], z = c->az[a];
-                for (int y = 0; y < n; y++) line[y] = zl[(((size_t)v * n + y) * kxn + x) * n + z];
+                int vz = v < 4 ? v : 5;
+                for (int y = 0; y < n; y++) line[y] = zl[(((size_t)vz * n + y) * kxn + x) * n + z];
                 fft_line(line, tmp, n, -1, &c->tw);
             }
         free(tmp);
@@ -604,11 +654,19 @@ static int step_control(orc_ctx *c)
     for (int y = 0; y < n; y++) c->yfac[y] = exp(-(c->viscos * (c->ky[y] * c->ky[y]) * term));
     term = c->b33 * c->dt;
     for (int z = 0; z < n; z++) c->zfac[z] = exp(-(c->viscos * (c->kz[z] * c->kz[z]) * term));
+    if (c->nc) {
+        /* step.f:387-407 */
+        for (int z = 0; z < n; z++) c->zdif[z] = pow(c->zfac[z], 1. / c->pr);
+        for (int x = 0; x <= n / 2 && x < n; x++) c->xdif[x] = pow(c->xfac[x], 1. / c->pr);
+        for (int y = 0; y < n; y++) c->ydif[y] = pow(c->yfac[y], 1. / c->pr);
+    }
     return err;
 }
 
 /* wavespace_vel.f:80,163-174: un-shift and finish the y derivatives.
- * in: w[4][a][y]; out: w[0..2] = (dt/2) N(u) */
+ * in: w[4][a][y]; out: w[0..2] = (dt/2) N(u).  A scalar's term w[4] is
+ * un-shifted the same way (wavespace_module.f:344-357); every variable is
+ * zero outside the sphere (:289-291). */
 static void wavespace(orc_ctx *c, cx *w, int ks)
 {
     int n = c->n, tot = c->xz_tot;
@@ -632,8 +690,10 @@ static void wavespace(orc_ctx *c, cx *w, int ks)
                 cx si = cmul(sxyz, cmk(0.0, 1.0));
                 w[vs + o] = cmul(si, cadd(cscale(bk1, u2), cscale(bk3, u4)));
                 w[2 * vs + o] = cadd(cmul(sxyz, u3), cmul(utmp1, u4));
+                if (c->nc) w[4 * vs + o] = cmul(sxyz, w[4 * vs + o]);
             } else {
                 w[o] = CZERO; w[vs + o] = CZERO; w[2 * vs + o] = CZERO; w[3 * vs + o] = CZERO;
+                if (c->nc) w[4 * vs + o] = CZERO;
             }
         }
     }
@@ -678,6 +738,14 @@ static void proc4a(orc_ctx *c, cx *w, cx *un)
                 un[o] = cscale(f, cadd(untemp, w[o]));
                 w[o] = cscale(f, cadd(untemp, cscale(2., w[o])));
             }
+            if (c->nc) {
+                /* proc4a.f:507-522: scalar term in w[4], old scalar in un[3] */
+                double fs = c->xdif[x] * c->ydif[y] * c->zdif[z];
+                size_t o = (size_t)a * n + y;
+                cx untemp = un[3 * vs + o];
+                un[3 * vs + o] = cscale(fs, cadd(untemp, w[4 * vs + o]));
+                w[4 * vs + o] = cscale(fs, cadd(untemp, cscale(2., w[4 * vs + o])));
+            }
             if (a == 0 && y == 0) continue;
             project(c, w, a, y);
         }
@@ -699,6 +767,11 @@ static void proc4b(orc_ctx *c, cx *w, cx *un)
                 size_t o = i * vs + (size_t)a * n + y;
                 w[o] = cadd(un[o], w[o]);
             }
+            if (c->nc) {
+                /* proc4b.f:69-75 */
+                size_t o = (size_t)a * n + y;
+                w[4 * vs + o] = cadd(un[3 * vs + o], w[4 * vs + o]);
+            }
             if (a == 0 && y == 0) continue;
             project(c, w, a, y);
         }
@@ -712,9 +785,11 @@ static void proc4b(orc_ctx *c, cx *w, cx *un)
                 size_t o = i * vs + (size_t)a * n + y;
                 un[o] = w[o];
             }
+            if (c->nc) un[3 * vs + (size_t)a * n + y] = w[4 * vs + (size_t)a * n + y];
         }
     }
     for (int i = 0; i < 3; i++) { w[i * vs] = CZERO; un[i * vs] = CZERO; }
+    if (c->nc) { w[4 * vs] = CZERO; un[3 * vs] = CZERO; }
 }
 
 
@@ -1143,20 +1218,34 @@ static void particles_stage1(orc_ctx *c, const double *p)
     free(bs);
 }
 
-/* One RK stage (timestep_module.f:70-481, CLEAN velocity path, nc = 0).
- * The work array holds u (3 vars) on entry and the nonlinear slots (4 vars)
- * after the forward transform; u keeps the result. */
+/* One RK stage (timestep_module.f:70-481, CLEAN velocity path, nc = 0 or 1).
+ * The work array holds u (3 vars; with a scalar also its y gradient and two
+ * copies of it, wavespace_module.f:81-97) on entry and the nonlinear slots
+ * (4 vars, then the scalar term) after the forward transform; u keeps the
+ * result. */
 static int rk_stage(orc_ctx *c, int kstep)
 {
     int n = c->n, tot = c->xz_tot;
     int ks = kstep - 1;
     size_t vs = (size_t)tot * n;
     size_t np = (size_t)n * n * n;
-    phase_shift(c, c->u, 3, ks);
-    cx *w = (cx *)malloc(sizeof(cx) * 4 * vs);
+    int nc = c->nc;
+    phase_shift(c, c->u, 3 + nc, ks);
+    cx *w = (cx *)malloc(sizeof(cx) * (4 + 2 * nc) * vs);
     memcpy(w, c->u, sizeof(cx) * 3 * vs);
-    double *p = (double *)malloc(sizeof(double) * 5 * np);
-    itransform(c, w, 3, p);
+    if (nc) {
+        #pragma omp parallel for schedule(static)
+        for (int a = 0; a < tot; a++)
+            for (int y = 0; y < n; y++) {
+                size_t o = (size_t)a * n + y;
+                cx th = c->u[3 * vs + o];
+                w[3 * vs + o] = cmul(cmk(0.0, c->b22 * c->ky[y]), th);
+                w[4 * vs + o] = th;
+                w[5 * vs + o] = th;
+            }
+    }
+    double *p = (double *)malloc(sizeof(double) * (5 + nc) * np);
+    itransform(c, w, 3 + 3 * nc, p);
     if (kstep == 1 && c->np > 0) particles_stage1(c, p);   /* realspace -> lagpart */
     double vm = realspace(c, p, kstep == 1);
     if (kstep == 1) c->velmax = vm;
@@ -1168,6 +1257,7 @@ static int rk_stage(orc_ctx *c, int kstep)
     if (kstep == 1) proc4a(c, w, c->un);
     else proc4b(c, w, c->un);
     memcpy(c->u, w, sizeof(cx) * 3 * vs);
+    if (nc) memcpy(c->u + 3 * vs, w + 4 * vs, sizeof(cx) * vs);
     free(w);
     return err;
 }

@@ -50,7 +50,8 @@ def test_default_params_match_reference_input(gpu_mod):
 
 def test_init_rejects_bad_parameters_without_touching_a_device(gpu_mod):
     import pytest
-    for kw in ({"n": 20}, {"kshift": 7}, {"seed_input": -1}, {"nx": 64, "ny": 32, "nz": 64}):
+    for kw in ({"n": 20}, {"kshift": 7}, {"seed_input": -1}, {"nx": 64, "ny": 32, "nz": 64},
+               {"nc": 2}, {"nc": 1, "pr": 0.0}):
         p = gpu_mod.default_params(n=64)
         for k, v in kw.items():
             if k == "n":
