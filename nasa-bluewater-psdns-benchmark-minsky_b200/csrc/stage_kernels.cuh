@@ -65,10 +65,27 @@ __device__ __forceinline__ bool mask_ok(const Geo& g, int a, int y, int n) {
   return ky <= __ldg(g.kymax + a);
 }
 
+// Asynchronous global -> shared copies of one complex element (cp.async,
+// 8 or 16 bytes).  A thread issues all of its copies before waiting, so a
+// block keeps its whole tile in flight; after cp_async_wait_all() the
+// thread's own copies have landed (other threads' copies need a barrier).
+template <typename C>
+__device__ __forceinline__ void cp_async_elem(C* smem_dst, const C* gmem_src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  if constexpr (sizeof(C) == 16) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+  }
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// twiddles are copied asynchronously: every kernel calls cp_async_wait_all()
+// and __syncthreads() before its first FFT
 template <typename T, int N>
 __device__ __forceinline__ void load_twiddles(C2<T>* tw_s, const C2<T>* __restrict__ tw_g) {
   constexpr int TS = FFTPlan<T, N>::TWSIZE;
-  for (int i = threadIdx.x; i < TS; i += blockDim.x) tw_s[i] = tw_g[i];
+  for (int i = threadIdx.x; i < TS; i += blockDim.x) cp_async_elem(tw_s + i, tw_g + i);
 }
 
 template <typename T, int N, int LINES>
@@ -107,13 +124,18 @@ k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict_
   const int src = v < 3 ? v : 3;
   const int a0 = at * TB;
   const size_t vs = (size_t)g.xz_tot * N;
+  // the TB columns are contiguous in u: copy them raw, then shift in place
+  const C* col = u + src * vs + (size_t)a0 * N;
+  const int lim = min(TB, g.xz_tot - a0) * N;
+  for (int e = threadIdx.x; e < lim; e += THREADS) cp_async_elem(buf + (e / N) * L + pad32(e % N), col + e);
+  cp_async_wait_all();
   for (int e = threadIdx.x; e < TB * N; e += THREADS) {
     const int l = e / N, y = e % N, a = a0 + l;
     C val = cmk<C>(0, 0);
-    if (a < g.xz_tot && mask_ok(g, a, y, N)) {
+    if (e < lim && mask_ok(g, a, y, N)) {
       C sxz = cmul(__ldg(st.sx + __ldg(g.ax + a)), __ldg(st.sz + __ldg(g.az + a)));
       C sh = cmul(__ldg(st.sy + y), sxz);
-      val = cmul(u[src * vs + (size_t)a * N + y], sh);
+      val = cmul(buf[l * L + pad32(y)], sh);
       if constexpr (NC > 0) {
         if (v == 4) {
           const T bk = st.b22 * T(kwave<N>(y));
@@ -159,21 +181,33 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
   const int y = blockIdx.x, x0 = blockIdx.y * XT, v = blockIdx.z;
   const int x1 = min(x0 + XT, g.kxn);
   const int nl = x1 - x0;
-  for (int e = threadIdx.x; e < XT * N; e += THREADS) buf[(e / N) * L + pad32(e % N)] = cmk<C>(0, 0);
-  __syncthreads();
   const int abeg = __ldg(g.colstart + x0), aend = __ldg(g.colstart + x1);
   const int sv = v < 3 ? v : (v == 3 ? 4 : 3);
   const C* src = ub + (size_t)sv * g.nab_i * N * TB;
+  // the cylinder entries of the XT lines, copied raw (column a of line
+  // x - x0 holds kz = az[a]); then the cut band is zeroed, and each thread
+  // conjugates the entries it copied
+  for (int a = abeg + threadIdx.x; a < aend; a += THREADS)
+    cp_async_elem(buf + (__ldg(g.ax + a) - x0) * L + pad32(__ldg(g.az + a)),
+                  src + ((size_t)(a / TB) * N + y) * TB + (a % TB));
+  for (int e = threadIdx.x; e < XT * N; e += THREADS) {
+    const int l = e / N, z = e % N;
+    // column x0 + l keeps |kz| <= kc = (count - 1) / 2
+    const int kc = l < nl ? (__ldg(g.colstart + x0 + l + 1) - __ldg(g.colstart + x0 + l) - 1) / 2 : -1;
+    if (z > kc && z < N - kc) buf[l * L + pad32(z)] = cmk<C>(0, 0);
+  }
+  cp_async_wait_all();
   for (int a = abeg + threadIdx.x; a < aend; a += THREADS) {
     const int l = __ldg(g.ax + a) - x0, z = __ldg(g.az + a);
-    C val = src[((size_t)(a / TB) * N + y) * TB + (a % TB)];
+    C* p = buf + l * L + pad32(z);
+    C val = *p;
     if constexpr (NC > 0) {
       if (v >= 4) {
         const T bk = v == 4 ? b11 * T(x0 + l) : b33 * T(kwave<N>(z));
         val = cmk<C>(-bk * val.y, bk * val.x);
       }
     }
-    buf[l * L + pad32(z)] = cconj(val);
+    *p = cconj(val);
   }
   __syncthreads();
   fft_lines<T, N, THREADS>(buf, nl, L, tw);
@@ -215,6 +249,56 @@ __device__ __forceinline__ void xchain_store(const Geo& g, const C2<T>* buf, int
   }
 }
 
+// Load NV x-line tiles (uz slots v0..v0+NV-1, TZ lines each) and pack two
+// real lines per complex line: Z(k) = A(k) + i B(k), with the Hermitian
+// extension and the imaginary part of the kx=0 term dropped; stored
+// conjugated (backward transform by conjugation).  All loads of a thread are
+// issued before the first shared-memory store.
+template <typename T, int N, int NV, int THREADS>
+__device__ __forceinline__ void xchain_pack(const Geo& g, const C2<T>* __restrict__ uz, int v0, int y, int zt,
+                                            C2<T>* bufU, int L) {
+  using C = C2<T>;
+  constexpr int TZ = Tiles<T>::TZ, NPAIR = TZ / 2;
+  constexpr int XST = THREADS / NPAIR;
+  constexpr int XI = (N / 2 + XST - 1) / XST;
+  const int kxn = g.kxn;
+  const int p = threadIdx.x % NPAIR, xth = threadIdx.x / NPAIR;
+  C A[NV][XI], B[NV][XI];
+#pragma unroll
+  for (int v = 0; v < NV; v++)
+#pragma unroll
+    for (int i = 0; i < XI; i++) {
+      const int x = xth + i * XST;
+      if (x < kxn) {
+        const C* src = uz + ((((size_t)(v0 + v) * N + y) * g.nzt + zt) * kxn + x) * TZ + 2 * p;
+        if constexpr (sizeof(C) == 8) {
+          const float4 q = *reinterpret_cast<const float4*>(src);
+          A[v][i] = cmk<C>(q.x, q.y);
+          B[v][i] = cmk<C>(q.z, q.w);
+        } else {
+          A[v][i] = src[0];
+          B[v][i] = src[1];
+        }
+      }
+    }
+#pragma unroll
+  for (int v = 0; v < NV; v++)
+#pragma unroll
+    for (int i = 0; i < XI; i++) {
+      const int x = xth + i * XST;
+      if (x < kxn) {
+        const C a = A[v][i], b = B[v][i];
+        C* line = bufU + (v * NPAIR + p) * L;
+        if (x == 0) {
+          line[pad32(0)] = cmk<C>(a.x, -b.x);
+        } else {
+          line[pad32(x)] = cmk<C>(a.x - b.y, -(a.y + b.x));
+          line[pad32(N - x)] = cmk<C>(a.x + b.y, -(b.x - a.y));
+        }
+      }
+    }
+}
+
 template <typename T, int N, int NC = 0>
 __global__ void __launch_bounds__(Launch<T, N, 2 * Tiles<T>::TZ>::THREADS)
 k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T b22, T b33,
@@ -241,23 +325,9 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
     const int k = e % N;
     if (k >= kxn && k <= N - kxn) bufU[(e / N) * L + pad32(k)] = cmk<C>(0, 0);
   }
-  // pack two real lines per complex line: Z(k) = A(k) + i B(k), with the
-  // Hermitian extension and the imaginary part of the kx=0 term dropped;
-  // stored conjugated (backward transform by conjugation)
-  const int pth = threadIdx.x % NPAIR, xth = threadIdx.x / NPAIR, xst = THREADS / NPAIR;
-  for (int v = 0; v < NVIN; v++)
-  for (int x = xth; x < kxn; x += xst) {
-    const int p = pth;
-    const C* src = uz + ((((size_t)v * N + y) * g.nzt + zt) * kxn + x) * TZ + 2 * p;
-    const C A = src[0], B = src[1];
-    C* line = bufU + (v * NPAIR + p) * L;
-    if (x == 0) {
-      line[pad32(0)] = cmk<C>(A.x, -B.x);
-    } else {
-      line[pad32(x)] = cmk<C>(A.x - B.y, -(A.y + B.x));
-      line[pad32(N - x)] = cmk<C>(A.x + B.y, -(B.x - A.y));
-    }
-  }
+  xchain_pack<T, N, 3, THREADS>(g, uz, 0, y, zt, bufU, L);
+  if constexpr (NC > 0) xchain_pack<T, N, 3, THREADS>(g, uz, 3, y, zt, bufU + 3 * NPAIR * L, L);
+  cp_async_wait_all();
   __syncthreads();
   fft_lines<T, N, THREADS>(bufU, NVIN * NPAIR, L, tw);
   // buffers now hold conj(a + i b): a = re, b = -im
@@ -336,7 +406,7 @@ __device__ __forceinline__ void zfwd_load(const Geo& g, const C2<T>* __restrict_
     C2<T>* b = buf + yy * nl * L;
     for (int e = threadIdx.x; e < nl * N; e += blockDim.x) {
       const int zt = e / (nl * TZ), rem = e % (nl * TZ), l = rem / TZ, zz = rem % TZ;
-      b[l * L + pad32(zt * TZ + zz)] = uz[((vbase + zt) * g.kxn + x0 + l) * TZ + zz];
+      cp_async_elem(b + l * L + pad32(zt * TZ + zz), uz + ((vbase + zt) * g.kxn + x0 + l) * TZ + zz);
     }
   }
 }
@@ -403,6 +473,7 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
   // round 1: P5 -> s0, P1 -> s1
   zfwd_load<T, N>(g, uz, 4, y0, YT, x0, nl, s0, L);
   zfwd_load<T, N>(g, uz, 0, y0, YT, x0, nl, s1, L);
+  cp_async_wait_all();
   __syncthreads();
   if (nl == XT) {
     fft_lines<T, N, THREADS>(s0, 2 * NLT, L, tw);
@@ -414,6 +485,7 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
   __syncthreads();
   // round 2: P3 -> s1
   zfwd_load<T, N>(g, uz, 2, y0, YT, x0, nl, s1, L);
+  cp_async_wait_all();
   __syncthreads();
   fft_lines<T, N, THREADS>(s1, nt, L, tw);
   zfwd_store<T, N, 1>(g, s0, s1, L, ub, 2, y0, YT, x0, x1, b11, b33);
@@ -421,6 +493,7 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
   // round 3: P2 -> s0, P4 -> s1
   zfwd_load<T, N>(g, uz, 1, y0, YT, x0, nl, s0, L);
   zfwd_load<T, N>(g, uz, 3, y0, YT, x0, nl, s1, L);
+  cp_async_wait_all();
   __syncthreads();
   if (nl == XT) {
     fft_lines<T, N, THREADS>(s0, 2 * NLT, L, tw);
@@ -433,6 +506,7 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
   if constexpr (NC > 0) {
     __syncthreads();
     zfwd_load<T, N>(g, uz, 5, y0, YT, x0, nl, s1, L);
+    cp_async_wait_all();
     __syncthreads();
     fft_lines<T, N, THREADS>(s1, nt, L, tw);
     zfwd_store<T, N, 3>(g, s0, s1, L, ub, 4, y0, YT, x0, x1, b11, b33);
@@ -480,9 +554,10 @@ k_yfwd(Geo g, StageTables<T> st, const C2<T>* __restrict__ ub, C2<T>* __restrict
     const C* src = ub + ((size_t)v * g.nab_f + at) * N * TB;
     for (int e = threadIdx.x; e < TB * N; e += THREADS) {
       const int y = e / TB, l = e % TB;
-      buf[(v * TB + l) * L + pad32(y)] = src[e];
+      cp_async_elem(buf + (v * TB + l) * L + pad32(y), src + e);
     }
   }
+  cp_async_wait_all();
   __syncthreads();
   fft_lines<T, N, THREADS>(buf, NVF * TB, L, tw);
   const size_t vs = (size_t)g.xz_tot * N;
@@ -623,20 +698,8 @@ k_xspline(Geo g, const C2<T>* __restrict__ uz, typename V4T<T>::type* __restrict
     const int k = e % N;
     if (k >= kxn && k <= N - kxn) bufU[(e / N) * L + pad32(k)] = cmk<C>(0, 0);
   }
-  const int pth = threadIdx.x % NPAIR, xth = threadIdx.x / NPAIR, xst = THREADS / NPAIR;
-  for (int v = 0; v < 3; v++)
-  for (int x = xth; x < kxn; x += xst) {
-    const int p = pth;
-    const C* src = uz + ((((size_t)v * N + y) * g.nzt + zt) * kxn + x) * TZ + 2 * p;
-    const C A = src[0], B = src[1];
-    C* line = bufU + (v * NPAIR + p) * L;
-    if (x == 0) {
-      line[pad32(0)] = cmk<C>(A.x, -B.x);
-    } else {
-      line[pad32(x)] = cmk<C>(A.x - B.y, -(A.y + B.x));
-      line[pad32(N - x)] = cmk<C>(A.x + B.y, -(B.x - A.y));
-    }
-  }
+  xchain_pack<T, N, 3, THREADS>(g, uz, 0, y, zt, bufU, L);
+  cp_async_wait_all();
   __syncthreads();
   fft_lines<T, N, THREADS>(bufU, 3 * NPAIR, L, tw);
   // buffer = conj(a + i b): line z = 2p is re, line 2p+1 is -im
