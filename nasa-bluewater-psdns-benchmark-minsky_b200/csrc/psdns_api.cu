@@ -356,7 +356,7 @@ template <typename T, int N, int NC> struct Impl {
   static int stage_b(Ctx& c, int kstep) {
     Geo g = make_geo(c);
     StageTables<T> st = make_tables<T>(c, kstep - 1);
-    constexpr int TH = Launch<T, N, (4 + NC) * TL::TB_F>::THREADS;
+    constexpr int TH = K5Launch<T, N, NC>::THREADS;
     prof_mark(c, kstep - 1, 4, 0);
     if (kstep == 1)
       k_yfwd<T, N, 1, NC><<<c.nab_f, TH, sm5(), c.stream>>>(g, st, (const C*)c.d_ub, (C*)c.d_u, (C*)c.d_un,

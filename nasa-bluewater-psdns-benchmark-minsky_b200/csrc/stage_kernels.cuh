@@ -88,13 +88,19 @@ __device__ __forceinline__ void load_twiddles(C2<T>* tw_s, const C2<T>* __restri
   for (int i = threadIdx.x; i < TS; i += blockDim.x) cp_async_elem(tw_s + i, tw_g + i);
 }
 
-template <typename T, int N, int LINES>
+// threads of a block that transforms LINES lines at once (capped at CAP)
+template <typename T, int N, int LINES, int CAP = 256>
 struct Launch {
   static constexpr int P = FFTPlan<T, N>::P;
   static constexpr int want = LINES * P;
-  static constexpr int THREADS = want >= 256 ? 256 : (want < 32 ? 32 : want);
+  static constexpr int THREADS = want >= CAP ? CAP : (want < 32 ? 32 : want);
   static_assert(THREADS % P == 0, "threads per line must divide the block");
 };
+
+// K5 holds one CTA per SM (its (4 + nc) * TB_F lines fill shared memory), so
+// it runs every line of a block at once
+template <typename T, int N, int NC>
+struct K5Launch : Launch<T, N, (4 + NC) * Tiles<T>::TB_F, 1024> {};
 
 template <int N> struct LS { static constexpr int value = N + N / 32 + 4; };
 
@@ -534,7 +540,7 @@ __device__ __forceinline__ void project3(C2<T>& u1, C2<T>& u2, C2<T>& u3, T kx, 
 }
 
 template <typename T, int N, int KSTEP, int NC = 0>
-__global__ void __launch_bounds__(Launch<T, N, (4 + NC) * Tiles<T>::TB_F>::THREADS)
+__global__ void __launch_bounds__(K5Launch<T, N, NC>::THREADS)
 k_yfwd(Geo g, StageTables<T> st, const C2<T>* __restrict__ ub, C2<T>* __restrict__ u,
        C2<T>* __restrict__ un, const C2<T>* __restrict__ tw_g, double* __restrict__ efkz) {
   // NC = 1: ub slot 4 is the scalar advection term; the scalar is un-shifted
@@ -543,7 +549,7 @@ k_yfwd(Geo g, StageTables<T> st, const C2<T>* __restrict__ ub, C2<T>* __restrict
   using C = C2<T>;
   constexpr int TB = Tiles<T>::TB_F;
   constexpr int NVF = 4 + NC;
-  constexpr int THREADS = Launch<T, N, NVF * TB>::THREADS;
+  constexpr int THREADS = K5Launch<T, N, NC>::THREADS;
   constexpr int L = LS<N>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
@@ -557,11 +563,32 @@ k_yfwd(Geo g, StageTables<T> st, const C2<T>* __restrict__ ub, C2<T>* __restrict
       cp_async_elem(buf + (v * TB + l) * L + pad32(y), src + e);
     }
   }
+  const size_t vs = (size_t)g.xz_tot * N;
+  // the old state un of this thread's points
+  constexpr int PER = (TB * N + THREADS - 1) / THREADS;
+  C nb[PER][3 + NC];
+  auto load_un = [&]() {
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+      const int e = threadIdx.x + q * THREADS;
+      const int l = e / N, y = e % N, a = a0 + l;
+      if (e < TB * N && a < g.xz_tot && mask_ok(g, a, y, N)) {
+        const size_t o = (size_t)a * N + y;
+#pragma unroll
+        for (int v = 0; v < 3 + NC; v++) nb[q][v] = un[v * vs + o];
+      }
+    }
+  };
   cp_async_wait_all();
   __syncthreads();
   fft_lines<T, N, THREADS>(buf, NVF * TB, L, tw);
-  const size_t vs = (size_t)g.xz_tot * N;
-  for (int e = threadIdx.x; e < TB * N; e += THREADS) {
+  // issued together after the transform (registers are free again), so each
+  // thread waits once for all of its points
+  load_un();
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    const int e = threadIdx.x + q * THREADS;
+    if (e >= TB * N) break;
     const int l = e / N, y = e % N, a = a0 + l;
     if (a >= g.xz_tot) continue;
     const size_t o = (size_t)a * N + y;
@@ -590,7 +617,7 @@ k_yfwd(Geo g, StageTables<T> st, const C2<T>* __restrict__ ub, C2<T>* __restrict
     C w2 = cmul(si, cmk<C>(bk1 * V2.x + bk3 * V4.x, bk1 * V2.y + bk3 * V4.y));
     C w3 = cadd(cmul(sxyz, V3), cmul(ut1, V4));
     const bool k0 = (a == 0 && y == 0);
-    C n1 = un[o], n2 = un[vs + o], n3 = un[2 * vs + o];
+    C n1 = nb[q][0], n2 = nb[q][1], n3 = nb[q][2];
     C u1, u2, u3;
     if constexpr (KSTEP == 1) {
       // proc4a.f:427, 479-486
@@ -646,7 +673,7 @@ k_yfwd(Geo g, StageTables<T> st, const C2<T>* __restrict__ ub, C2<T>* __restrict
     if constexpr (NC > 0) {
       const C V5 = buf[(4 * TB + l) * L + i];
       const C w4 = cmul(sxyz, V5);
-      C n4 = un[3 * vs + o], u4;
+      C n4 = nb[q][3], u4;
       if constexpr (KSTEP == 1) {
         const T fs = __ldg(st.xdif + x) * __ldg(st.ydif + y) * __ldg(st.zdif + z);
         u4 = cscale(fs, cmk<C>(n4.x + T(2) * w4.x, n4.y + T(2) * w4.y));

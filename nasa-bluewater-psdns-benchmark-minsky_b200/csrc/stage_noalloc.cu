@@ -203,7 +203,7 @@ static int run(const psdns_params* prm, int kstep, const double* gsh, double dt,
         geo, uz, ub, twd, stb.b11, stb.b33);
   }
   {
-    constexpr int TH = Launch<T, N, 4 * TL::TB_F>::THREADS;
+    constexpr int TH = K5Launch<T, N, 0>::THREADS;
     if (kstep == 1)
       k_yfwd<T, N, 1><<<geo.nab_f, TH, TWB + sizeof(C) * 4 * TL::TB_F * L, st>>>(geo, stb, ub, u, un, twd, nullptr);
     else
