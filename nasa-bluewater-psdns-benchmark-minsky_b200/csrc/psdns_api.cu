@@ -250,7 +250,7 @@ template <typename T, int N, int NC> struct Impl {
   static constexpr size_t TWB = sizeof(C) * FFTPlan<T, N>::TWSIZE;
   static size_t sm1() { return TWB + sizeof(C) * TL::TB_I * L; }
   static size_t sm2() { return TWB + sizeof(C) * TL::XT2 * L; }
-  static size_t sm3() { return TWB + sizeof(C) * (NC ? 6 : 4) * (TL::TZ / 2) * L; }
+  static size_t sm3() { return K3Launch<T, N, NC>::SMEM; }
   static size_t sm4() { return TWB + sizeof(C) * 2 * TL::XT4 * TL::YT4 * L; }
   static size_t sm5() { return TWB + sizeof(C) * (4 + NC) * TL::TB_F * L; }
 
@@ -281,7 +281,7 @@ template <typename T, int N, int NC> struct Impl {
     C* uz = (C*)c.d_uz;
     const int kxn = c.g.kxn;
     prof_mark(c, 0, 5, 0);
-    k_yinv<T, N, true><<<dim3(c.nab_i, 3), Launch<T, N, TL::TB_I>::THREADS, sm1(), c.stream>>>(g, st, (const C*)c.d_u,
+    k_yinv<T, N, true><<<dim3(c.nab_i, 3), K1Launch<T, N>::THREADS, sm1(), c.stream>>>(g, st, (const C*)c.d_u,
                                                                                                ub, tw);
     k_zinv<T, N><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3), Launch<T, N, TL::XT2>::THREADS, sm2(), c.stream>>>(
         g, ub, uz, tw);
@@ -319,7 +319,7 @@ template <typename T, int N, int NC> struct Impl {
     const int kxn = c.g.kxn;
     const int s = kstep - 1;
     {
-      constexpr int TH = Launch<T, N, TL::TB_I>::THREADS;
+      constexpr int TH = K1Launch<T, N>::THREADS;
       prof_mark(c, s, 0, 0);
       k_yinv<T, N, false, NC><<<dim3(c.nab_i, 3 + 2 * NC), TH, sm1(), c.stream>>>(g, st, u, ub, tw);
       prof_mark(c, s, 0, 1);
@@ -332,7 +332,7 @@ template <typename T, int N, int NC> struct Impl {
       prof_mark(c, s, 1, 1);
     }
     {
-      constexpr int TH = Launch<T, N, 2 * TL::TZ>::THREADS;
+      constexpr int TH = K3Launch<T, N, NC>::THREADS;
       prof_mark(c, s, 2, 0);
       // mean-gradient coefficients cb = beta * grad (init.f:42-45)
       const T cb1 = (T)(c.p.beta1 * c.p.grad[0]), cb2 = (T)(c.p.beta2 * c.p.grad[1]),
@@ -342,7 +342,7 @@ template <typename T, int N, int NC> struct Impl {
       prof_mark(c, s, 2, 1);
     }
     {
-      constexpr int TH = Launch<T, N, 2 * TL::XT4 * TL::YT4>::THREADS;
+      constexpr int TH = K4Launch<T, N>::THREADS;
       prof_mark(c, s, 3, 0);
       k_zfwd<T, N, NC><<<dim3(N / TL::YT4, (kxn + TL::XT4 - 1) / TL::XT4), TH, sm4(), c.stream>>>(g, uz, ub, tw,
                                                                                                    st.b11, st.b33);

@@ -50,9 +50,12 @@ template <typename T> struct StageTables {
   const T* spf;      // spline prefilter 6/(4+2cos(2 pi k/n)): [n/2+1] x, [n] y, [n] z
 };
 
-// per-precision tile sizes: TB_I = columns per K1 block (64 B segments),
-// TB_F = columns per K5 block, TZ = z lines per K3 tile (32 B runs),
-// XT2/XT4 = x lines per K2/K4 block.
+// per-precision tile sizes: TB_I = columns per K1 block (64 B runs in ub
+// for K2), TB_F = columns per K5 block, TZ = z lines per K3 tile (32 B
+// runs), XT2/XT4 = x lines per K2/K4 block, YT4 = y rows per K4 block.
+// Eight lines per block keep two to three blocks resident per SM, so that
+// one block's copies overlap another's transforms; sixteen-line blocks (one
+// per SM) measured slower for K1 and K4.
 template <typename T> struct Tiles;
 template <> struct Tiles<float> { static constexpr int TB_I = 8, TB_F = 4, TZ = 4, XT2 = 8, XT4 = 4, YT4 = 1; };
 template <> struct Tiles<double> { static constexpr int TB_I = 4, TB_F = 2, TZ = 2, XT2 = 4, XT4 = 2, YT4 = 1; };
@@ -97,6 +100,12 @@ struct Launch {
   static_assert(THREADS % P == 0, "threads per line must divide the block");
 };
 
+// K1 and K4: one warp per line at n = 1024 FP32
+template <typename T, int N>
+struct K1Launch : Launch<T, N, Tiles<T>::TB_I, 1024> {};
+template <typename T, int N>
+struct K4Launch : Launch<T, N, 2 * Tiles<T>::XT4 * Tiles<T>::YT4, 1024> {};
+
 // K5 holds one CTA per SM (its (4 + nc) * TB_F lines fill shared memory), so
 // it runs every line of a block at once
 template <typename T, int N, int NC>
@@ -109,7 +118,7 @@ template <int N> struct LS { static constexpr int value = N + N / 32 + 4; };
 // grid (ceil(xz_tot/TB_I), 3); one block = one ub block of TB_I columns
 // ---------------------------------------------------------------------------
 template <typename T, int N, bool SPL = false, int NC = 0>
-__global__ void __launch_bounds__(Launch<T, N, Tiles<T>::TB_I>::THREADS)
+__global__ void __launch_bounds__(K1Launch<T, N>::THREADS)
 k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict__ ub,
        const C2<T>* __restrict__ tw_g) {
   // NC = 1 (one passive scalar, grid.y = 5): ub variable 3 is the shifted
@@ -120,7 +129,7 @@ k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict_
   // that splx.f/splz_m.f/sply.f solve in physical space)
   using C = C2<T>;
   constexpr int TB = Tiles<T>::TB_I;
-  constexpr int THREADS = Launch<T, N, TB>::THREADS;
+  constexpr int THREADS = K1Launch<T, N>::THREADS;
   constexpr int L = LS<N>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
@@ -187,33 +196,42 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
   const int y = blockIdx.x, x0 = blockIdx.y * XT, v = blockIdx.z;
   const int x1 = min(x0 + XT, g.kxn);
   const int nl = x1 - x0;
-  const int abeg = __ldg(g.colstart + x0), aend = __ldg(g.colstart + x1);
   const int sv = v < 3 ? v : (v == 3 ? 4 : 3);
   const C* src = ub + (size_t)sv * g.nab_i * N * TB;
-  // the cylinder entries of the XT lines, copied raw (column a of line
-  // x - x0 holds kz = az[a]); then the cut band is zeroed, and each thread
-  // conjugates the entries it copied
-  for (int a = abeg + threadIdx.x; a < aend; a += THREADS)
-    cp_async_elem(buf + (__ldg(g.ax + a) - x0) * L + pad32(__ldg(g.az + a)),
-                  src + ((size_t)(a / TB) * N + y) * TB + (a % TB));
+  // slot (l, z): column x0 + l holds kz = 0..kc then -kc..-1 (count 2 kc + 1,
+  // mpisetup.f:322-357), so its cylinder index follows from colstart alone.
+  // Cylinder entries are copied raw, the cut band is zeroed, then each
+  // thread conjugates the entries it copied.
   for (int e = threadIdx.x; e < XT * N; e += THREADS) {
     const int l = e / N, z = e % N;
-    // column x0 + l keeps |kz| <= kc = (count - 1) / 2
-    const int kc = l < nl ? (__ldg(g.colstart + x0 + l + 1) - __ldg(g.colstart + x0 + l) - 1) / 2 : -1;
-    if (z > kc && z < N - kc) buf[l * L + pad32(z)] = cmk<C>(0, 0);
+    int kc = -1, ac = 0;
+    if (l < nl) {
+      ac = __ldg(g.colstart + x0 + l);
+      kc = (__ldg(g.colstart + x0 + l + 1) - ac - 1) / 2;
+    }
+    C* p = buf + l * L + pad32(z);
+    if (z <= kc || z >= N - kc) {
+      const int a = ac + (z <= kc ? z : z - N + 2 * kc + 1);
+      cp_async_elem(p, src + ((size_t)(a / TB) * N + y) * TB + (a % TB));
+    } else {
+      *p = cmk<C>(0, 0);
+    }
   }
   cp_async_wait_all();
-  for (int a = abeg + threadIdx.x; a < aend; a += THREADS) {
-    const int l = __ldg(g.ax + a) - x0, z = __ldg(g.az + a);
-    C* p = buf + l * L + pad32(z);
-    C val = *p;
-    if constexpr (NC > 0) {
-      if (v >= 4) {
-        const T bk = v == 4 ? b11 * T(x0 + l) : b33 * T(kwave<N>(z));
-        val = cmk<C>(-bk * val.y, bk * val.x);
+  for (int e = threadIdx.x; e < nl * N; e += THREADS) {
+    const int l = e / N, z = e % N;
+    const int kc = (__ldg(g.colstart + x0 + l + 1) - __ldg(g.colstart + x0 + l) - 1) / 2;
+    if (z <= kc || z >= N - kc) {
+      C* p = buf + l * L + pad32(z);
+      C val = *p;
+      if constexpr (NC > 0) {
+        if (v >= 4) {
+          const T bk = v == 4 ? b11 * T(x0 + l) : b33 * T(kwave<N>(z));
+          val = cmk<C>(-bk * val.y, bk * val.x);
+        }
       }
+      *p = cconj(val);
     }
-    *p = cconj(val);
   }
   __syncthreads();
   fft_lines<T, N, THREADS>(buf, nl, L, tw);
@@ -305,8 +323,24 @@ __device__ __forceinline__ void xchain_pack(const Geo& g, const C2<T>* __restric
     }
 }
 
+// K3 runs the five output products of a tile as one batch of 5 * TZ/2
+// lines: one warp per line at n = 1024 (a multiple of 32 threads, so that
+// the velmax warp reduction sees whole warps)
+template <typename T, int N, int NC>
+struct K3Launch {
+  static constexpr int P = FFTPlan<T, N>::P;
+  static constexpr int NPAIR = Tiles<T>::TZ / 2;
+  static constexpr int want = 5 * NPAIR * P;
+  static constexpr int r32 = (want + 31) / 32 * 32;
+  static constexpr int THREADS = r32 > 1024 ? 1024 : r32;
+  static_assert(THREADS % P == 0, "threads per line must divide the block");
+  // twiddles + 5 product buffers (6 input buffers with a scalar) of TZ/2 lines
+  static constexpr size_t SMEM =
+      sizeof(C2<T>) * (FFTPlan<T, N>::TWSIZE + (size_t)(NC ? 6 : 5) * NPAIR * LS<N>::value);
+};
+
 template <typename T, int N, int NC = 0>
-__global__ void __launch_bounds__(Launch<T, N, 2 * Tiles<T>::TZ>::THREADS)
+__global__ void __launch_bounds__(K3Launch<T, N, NC>::THREADS)
 k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T b22, T b33,
          unsigned long long* velmax_bits, int want_velmax, T cb1 = T(0), T cb2 = T(0), T cb3 = T(0)) {
   // NC = 1: inputs also hold the scalar gradient (slots 3 = d/dy, 4 = d/dx,
@@ -315,14 +349,16 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
   using C = C2<T>;
   constexpr int TZ = Tiles<T>::TZ, NPAIR = TZ / 2;
   constexpr int NVIN = 3 + 3 * NC;
-  constexpr int THREADS = Launch<T, N, 2 * TZ>::THREADS;
+  constexpr int THREADS = K3Launch<T, N, NC>::THREADS;
   constexpr int L = LS<N>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   C* bufU = tw + FFTPlan<T, N>::TWSIZE;
   C* bufV = bufU + NPAIR * L;
   C* bufW = bufV + NPAIR * L;
-  C* bufE = bufW + NPAIR * L;   // with NC = 1 this is the y-gradient buffer until the scalar term is done
+  // with NC = 1, E and F hold the y and x gradients until the scalar term is done
+  C* bufE = bufW + NPAIR * L;
+  C* bufF = bufE + NPAIR * L;
   load_twiddles<T, N>(tw, tw_g);
   const int zt = blockIdx.x, y = blockIdx.y;
   const int kxn = g.kxn;
@@ -338,33 +374,34 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
   fft_lines<T, N, THREADS>(bufU, NVIN * NPAIR, L, tw);
   // buffers now hold conj(a + i b): a = re, b = -im
   const T hf = T(0.5) / T(N);
-  if constexpr (NC > 0) {
-    C* bufGY = bufW + NPAIR * L;
-    C* bufGX = bufGY + NPAIR * L;
-    C* bufGZ = bufGX + NPAIR * L;
-    for (int e = threadIdx.x; e < NPAIR * N; e += THREADS) {
-      const int i = (e / N) * L + pad32(e % N);
-      const C U = bufU[i], V = bufV[i], W = bufW[i], GY = bufGY[i], GX = bufGX[i], GZ = bufGZ[i];
-      const T sa = U.x * (cb1 + GX.x) + V.x * (cb2 + GY.x) + W.x * (cb3 + GZ.x);
-      const T sb = (-U.y) * (cb1 - GX.y) + (-V.y) * (cb2 - GY.y) + (-W.y) * (cb3 - GZ.y);
-      bufGX[i] = cmk<C>(sa, sb);
-    }
-    __syncthreads();
-    fft_lines<T, N, THREADS>(bufGX, NPAIR, L, tw);
-    xchain_store<T, N>(g, bufGX, 1, L, uz, 5, y, zt, hf);   // scalar advection term
-    __syncthreads();
-  }
+  // realspace_vel.f:105-114, in place: slot 0 = b11 u^2 - bv2, 1 = uv,
+  // 2 = b33 w^2 - bv2, 3 = vw (is1), 4 = uw (is2); velmax at stage 1.  With
+  // a scalar, slot 5 = its advection term (buffer 5 held d/dz theta).
   double vm = 0.0;
   const double xn = (double)b11 * N, yn = (double)b22 * N, zn = (double)b33 * N;
   for (int e = threadIdx.x; e < NPAIR * N; e += THREADS) {
     const int i = (e / N) * L + pad32(e % N);
     const C U = bufU[i], V = bufV[i], W = bufW[i];
+    if constexpr (NC > 0) {
+      C* bufGZ = bufF + NPAIR * L;
+      const C GY = bufE[i], GX = bufF[i], GZ = bufGZ[i];
+      const T sa = U.x * (cb1 + GX.x) + V.x * (cb2 + GY.x) + W.x * (cb3 + GZ.x);
+      const T sb = (-U.y) * (cb1 - GX.y) + (-V.y) * (cb2 - GY.y) + (-W.y) * (cb3 - GZ.y);
+      bufGZ[i] = cmk<C>(sa, sb);
+    }
     if (want_velmax) {
       double va = xn * fabs((double)U.x) + yn * fabs((double)V.x) + zn * fabs((double)W.x);
       double vb = xn * fabs((double)U.y) + yn * fabs((double)V.y) + zn * fabs((double)W.y);
       vm = fmax(vm, fmax(va, vb));
     }
-    bufE[i] = cmk<C>(U.x * W.x, U.y * W.y);   // uw (sign of b cancels in the product)
+    // the sign of b cancels in the mixed products
+    bufF[i] = cmk<C>(U.x * W.x, U.y * W.y);
+    bufE[i] = cmk<C>(V.x * W.x, V.y * W.y);
+    const T ua = U.x, ub = -U.y, va = V.x, vb = -V.y, wa = W.x, wb = -W.y;
+    const T bva = b22 * va * va, bvb = b22 * vb * vb;
+    bufW[i] = cmk<C>(b33 * wa * wa - bva, b33 * wb * wb - bvb);
+    bufV[i] = cmk<C>(ua * va, ub * vb);
+    bufU[i] = cmk<C>(b11 * ua * ua - bva, b11 * ub * ub - bvb);
   }
   if (want_velmax) {
     // block max through warp shuffles then one atomic per warp
@@ -372,29 +409,8 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
     if ((threadIdx.x & 31) == 0) atomic_max_pos<T>(velmax_bits, vm);
   }
   __syncthreads();
-  fft_lines<T, N, THREADS>(bufE, NPAIR, L, tw);
-  xchain_store<T, N>(g, bufE, 1, L, uz, 4, y, zt, hf);   // slot is2 = 5: u*w
-  __syncthreads();
-  for (int e = threadIdx.x; e < NPAIR * N; e += THREADS) {
-    const int i = (e / N) * L + pad32(e % N);
-    const C V = bufV[i], W = bufW[i];
-    bufE[i] = cmk<C>(V.x * W.x, V.y * W.y);   // vw
-  }
-  __syncthreads();
-  fft_lines<T, N, THREADS>(bufE, NPAIR, L, tw);
-  xchain_store<T, N>(g, bufE, 1, L, uz, 3, y, zt, hf);   // slot is1 = 4: v*w
-  for (int e = threadIdx.x; e < NPAIR * N; e += THREADS) {
-    const int i = (e / N) * L + pad32(e % N);
-    const C U = bufU[i], V = bufV[i], W = bufW[i];
-    const T ua = U.x, ub = -U.y, va = V.x, vb = -V.y, wa = W.x, wb = -W.y;
-    const T bva = b22 * va * va, bvb = b22 * vb * vb;
-    bufW[i] = cmk<C>(b33 * wa * wa - bva, b33 * wb * wb - bvb);
-    bufV[i] = cmk<C>(ua * va, ub * vb);
-    bufU[i] = cmk<C>(b11 * ua * ua - bva, b11 * ub * ub - bvb);
-  }
-  __syncthreads();
-  fft_lines<T, N, THREADS>(bufU, 3 * NPAIR, L, tw);
-  xchain_store<T, N>(g, bufU, 3, L, uz, 0, y, zt, hf);
+  fft_lines<T, N, THREADS>(bufU, (5 + NC) * NPAIR, L, tw);
+  xchain_store<T, N>(g, bufU, 5 + NC, L, uz, 0, y, zt, hf);
 }
 
 // ---------------------------------------------------------------------------
@@ -430,13 +446,24 @@ __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const 
   const int as = abeg - (abeg % TB);                      // first block boundary
   const int cnt = ((aend - as + TB - 1) / TB) * TB * ny;  // whole blocks x rows
   C* dst = ub + (size_t)slot * g.nab_f * N * TB;
+  // column starts of the XT lines: x and z of a cylinder index follow from
+  // them (column x0 + j holds kz = 0..kc then -kc..-1)
+  constexpr int XT = Tiles<T>::XT4;
+  int csr[XT + 1];
+#pragma unroll
+  for (int j = 0; j <= XT; j++) csr[j] = __ldg(g.colstart + min(x0 + j, g.kxn));
   for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
     // e -> (block q, row yy, column a): the ny rows of a block are adjacent
     // in memory, so consecutive threads write consecutive addresses
     const int q = e / (TB * ny), r = e % (TB * ny);
     const int yy = r / TB, a = as + q * TB + r % TB;
     if (a < abeg || a >= aend) continue;
-    const int x = __ldg(g.ax + a), z = __ldg(g.az + a), l = yy * nl + (x - x0);
+    int lx = 0, c0 = csr[0], c1 = csr[1];
+#pragma unroll
+    for (int j = 1; j < XT; j++)
+      if (a >= csr[j]) { lx = j; c0 = csr[j]; c1 = csr[j + 1]; }
+    const int kc = (c1 - c0 - 1) / 2, ia = a - c0;
+    const int x = x0 + lx, z = ia <= kc ? ia : ia + N - (2 * kc + 1), l = yy * nl + lx;
     const int i = l * L + pad32(z);
     C out;
     if constexpr (MODE == 0) {          // i kx P1 + i b33 kz P5   (s1 = P1, s0 = P5)
@@ -457,7 +484,7 @@ __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const 
 }
 
 template <typename T, int N, int NC = 0>
-__global__ void __launch_bounds__(Launch<T, N, 2 * Tiles<T>::XT4 * Tiles<T>::YT4>::THREADS)
+__global__ void __launch_bounds__(K4Launch<T, N>::THREADS)
 k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>* __restrict__ tw_g,
        T b11, T b33) {
   // NC = 1: the scalar advection term (uz slot 5) goes to ub slot 4 without
@@ -465,7 +492,7 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
   // grid (n / YT4, ceil(kxn / XT4)): YT4 adjacent y rows x XT4 x lines
   using C = C2<T>;
   constexpr int XT = Tiles<T>::XT4, YT = Tiles<T>::YT4, NLT = XT * YT;
-  constexpr int THREADS = Launch<T, N, 2 * NLT>::THREADS;
+  constexpr int THREADS = K4Launch<T, N>::THREADS;
   constexpr int L = LS<N>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);

@@ -184,7 +184,7 @@ static int run(const psdns_params* prm, int kstep, const double* gsh, double dt,
   constexpr size_t TWB = sizeof(C) * FFTPlan<T, N>::TWSIZE;
   const int kxn = g.kxn;
   {
-    constexpr int TH = Launch<T, N, TL::TB_I>::THREADS;
+    constexpr int TH = K1Launch<T, N>::THREADS;
     k_yinv<T, N><<<dim3(geo.nab_i, 3), TH, TWB + sizeof(C) * TL::TB_I * L, st>>>(geo, stb, u, ub, twd);
   }
   {
@@ -193,12 +193,12 @@ static int run(const psdns_params* prm, int kstep, const double* gsh, double dt,
                                                                                                        twd);
   }
   {
-    constexpr int TH = Launch<T, N, 2 * TL::TZ>::THREADS;
-    k_xchain<T, N><<<dim3(geo.nzt, N), TH, TWB + sizeof(C) * 4 * (TL::TZ / 2) * L, st>>>(
+    constexpr int TH = K3Launch<T, N, 0>::THREADS;
+    k_xchain<T, N><<<dim3(geo.nzt, N), TH, K3Launch<T, N, 0>::SMEM, st>>>(
         geo, uz, twd, stb.b11, stb.b22, stb.b33, vmx, kstep == 1 ? 1 : 0);
   }
   {
-    constexpr int TH = Launch<T, N, 2 * TL::XT4 * TL::YT4>::THREADS;
+    constexpr int TH = K4Launch<T, N>::THREADS;
     k_zfwd<T, N><<<dim3(N / TL::YT4, (kxn + TL::XT4 - 1) / TL::XT4), TH, TWB + sizeof(C) * 2 * TL::XT4 * TL::YT4 * L, st>>>(
         geo, uz, ub, twd, stb.b11, stb.b33);
   }
