@@ -144,12 +144,12 @@ k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict_
   const int lim = min(TB, g.xz_tot - a0) * N;
   for (int e = threadIdx.x; e < lim; e += THREADS) cp_async_elem(buf + (e / N) * L + pad32(e % N), col + e);
   cp_async_wait_all();
-  for (int e = threadIdx.x; e < TB * N; e += THREADS) {
-    const int l = e / N, y = e % N, a = a0 + l;
+  // shift (and mask, gradient, prefilter) the entries this thread copied;
+  // sxz, fx, fz are constants of column a0 + l
+  auto finish = [&](int l, int y, bool ok, C sxz, T fx, T fz) {
     C val = cmk<C>(0, 0);
-    if (e < lim && mask_ok(g, a, y, N)) {
-      C sxz = cmul(__ldg(st.sx + __ldg(g.ax + a)), __ldg(st.sz + __ldg(g.az + a)));
-      C sh = cmul(__ldg(st.sy + y), sxz);
+    if (ok) {
+      const C sh = cmul(__ldg(st.sy + y), sxz);
       val = cmul(buf[l * L + pad32(y)], sh);
       if constexpr (NC > 0) {
         if (v == 4) {
@@ -157,13 +157,43 @@ k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict_
           val = cmk<C>(-bk * val.y, bk * val.x);
         }
       }
-      if constexpr (SPL) {
-        const T f = __ldg(st.spf + __ldg(g.ax + a)) * __ldg(st.spf + (N / 2 + 1) + y) *
-                    __ldg(st.spf + (N / 2 + 1) + N + __ldg(g.az + a));
-        val = cscale(f, val);
-      }
+      if constexpr (SPL) val = cscale(fx * __ldg(st.spf + (N / 2 + 1) + y) * fz, val);
     }
     buf[l * L + pad32(y)] = cconj(val);
+  };
+  if constexpr (N % THREADS == 0) {
+#pragma unroll
+    for (int l = 0; l < TB; l++) {
+      const int a = a0 + l;
+      C sxz = cmk<C>(0, 0);
+      T fx = T(0), fz = T(0);
+      int kym = -1;
+      if (a < g.xz_tot) {
+        const int x = __ldg(g.ax + a), z = __ldg(g.az + a);
+        sxz = cmul(__ldg(st.sx + x), __ldg(st.sz + z));
+        kym = __ldg(g.kymax + a);
+        if constexpr (SPL) { fx = __ldg(st.spf + x); fz = __ldg(st.spf + (N / 2 + 1) + N + z); }
+      }
+#pragma unroll
+      for (int k = 0; k < N / THREADS; k++) {
+        const int y = threadIdx.x + k * THREADS;
+        const int ky = y > N / 2 ? N - y : y;
+        finish(l, y, y != N / 2 && ky <= kym, sxz, fx, fz);
+      }
+    }
+  } else {
+    for (int e = threadIdx.x; e < TB * N; e += THREADS) {
+      const int l = e / N, y = e % N, a = a0 + l;
+      const bool ok = e < lim && mask_ok(g, a, y, N);
+      C sxz = cmk<C>(0, 0);
+      T fx = T(0), fz = T(0);
+      if (ok) {
+        const int x = __ldg(g.ax + a), z = __ldg(g.az + a);
+        sxz = cmul(__ldg(st.sx + x), __ldg(st.sz + z));
+        if constexpr (SPL) { fx = __ldg(st.spf + x); fz = __ldg(st.spf + (N / 2 + 1) + N + z); }
+      }
+      finish(l, y, ok, sxz, fx, fz);
+    }
   }
   __syncthreads();
   fft_lines<T, N, THREADS>(buf, TB, L, tw);
@@ -179,7 +209,7 @@ k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict_
 // grid (n, ceil(kxn/XT2), 3)
 // ---------------------------------------------------------------------------
 template <typename T, int N, int NC = 0>
-__global__ void __launch_bounds__(Launch<T, N, Tiles<T>::XT2>::THREADS)
+__global__ void __launch_bounds__(Launch<T, N, Tiles<T>::XT2>::THREADS, 3)
 k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11 = T(1),
        T b33 = T(1)) {
   // NC = 1 (grid.z = 6): uz slot 3 = y gradient of the scalar (ub 4), slot
