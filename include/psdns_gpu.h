@@ -39,6 +39,13 @@ extern "C" {
  *   ((v*xz_tot + a)*ny + y); a enumerates the (kx,kz) columns inside the
  *   truncation cylinder in the order of next_xz (PSDNS/mpisetup.f:710-732). */
 #define PSDNS_LAYOUT_YCYL 0
+/* PSDNS_LAYOUT_FULL: the whole half-complex spectrum u(nxh,ny,nz,nv),
+ *   nxh = nx/2+1, column-major: element (x, y, z, v) at
+ *   (((v*nz + z)*ny + y)*nxh + x) -- the shape FFTW's real-to-complex
+ *   transform gives a real (nx,ny,nz) array (PSDNS/epfftw.f).  set_state
+ *   keeps the modes inside the truncation cylinder (kx < kxn, |kz| <= kc(kx),
+ *   PSDNS/mpisetup.f:307-357); get_state writes zeros outside it. */
+#define PSDNS_LAYOUT_FULL 1
 
 /* Which field get_state returns. */
 #define PSDNS_FIELD_U  0   /* u  (module comp, PSDNS/module.f:324-385) */

@@ -198,14 +198,17 @@ __host__ __device__ constexpr int plan_rad(int N, bool dbl, int p) {
   }
   if (N == 6) return p == 0 ? 6 : 1;
   if (N == 12) return p == 0 ? 3 : (p == 1 ? 4 : 1);
-  if (N == 24) return p == 0 ? 3 : (p == 1 ? 8 : 1);
-  if (N == 48) return p == 0 ? 6 : (p == 1 ? 8 : 1);
+  if (N == 24) return p == 0 ? 6 : (p == 1 ? 4 : 1);
+  if (N == 48) return p == 0 ? 12 : (p == 1 ? 4 : 1);
   if (N == 96) return p == 0 ? 12 : (p == 1 ? 8 : 1);
   return 1;
 }
+__host__ __device__ constexpr int gcd_i(int a, int b) { return b == 0 ? a : gcd_i(b, a % b); }
+// operands per thread: a multiple of every radix (their lcm), so that each
+// pass gives every thread whole butterflies
 __host__ __device__ constexpr int plan_e(int N, bool dbl) {
   int e = 1;
-  for (int p = 0; p < 3; p++) { int r = plan_rad(N, dbl, p); if (r > e) e = r; }
+  for (int p = 0; p < 3; p++) { int r = plan_rad(N, dbl, p); e = e / gcd_i(e, r) * r; }
   return e;
 }
 __host__ __device__ constexpr int plan_ns(int N, bool dbl, int p) {
@@ -223,6 +226,7 @@ template <typename T, int N> struct FFTPlan {
   static constexpr int rad(int p) { return plan_rad(N, DBL, p); }
   static constexpr int E = plan_e(N, DBL);
   static constexpr int P = N / E;   // threads per line
+  static_assert(P * E == N, "operands per thread must divide the line");
   static constexpr int ns(int p) { return plan_ns(N, DBL, p); }
   static constexpr int twoff(int p) { return plan_twoff(N, DBL, p); }
   static constexpr int TWSIZE = plan_twoff(N, DBL, plan_npass(N, DBL)) > 0 ? plan_twoff(N, DBL, plan_npass(N, DBL)) : 1;
@@ -248,6 +252,7 @@ template <typename C, int N, int R, int NS, int E, int P, int THREADS>
 __device__ __forceinline__ void fft_pass(C* buf, int nlines, int ls, const C* __restrict__ twp) {
   constexpr int LPR = THREADS / P;
   constexpr int NB = E / R;   // butterflies per thread
+  static_assert(NB * R == E && NB * P * R == N, "a pass must give every thread whole butterflies");
   const int tid = threadIdx.x;
   const int lr = tid / P, t = tid % P;
   for (int l0 = 0; l0 < nlines; l0 += LPR) {

@@ -207,6 +207,9 @@ template <typename T> struct TabLayout {
   }
 };
 
+// complex elements of one variable in the full half-complex layout
+static size_t full_elems(const Ctx& c) { return (size_t)(c.n / 2 + 1) * c.n * c.n; }
+
 static Geo make_geo(const Ctx& c) {
   Geo g;
   g.n = c.n; g.kxn = c.g.kxn; g.xz_tot = c.g.xz_tot; g.nzt = c.nzt;
@@ -396,7 +399,9 @@ static bool get_ops(int prec, int n, int nc, Ops& o) {
   switch (n) {
     PSDNS_CASE(16)
     PSDNS_CASE(32)
+    PSDNS_CASE(48)
     PSDNS_CASE(64)
+    PSDNS_CASE(96)
     PSDNS_CASE(128)
     PSDNS_CASE(256)
     PSDNS_CASE(512)
@@ -636,7 +641,8 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
   if (p->seed_input <= 0) return set_error("seed iseed=%d must be positive (ranu.f:33)", p->seed_input);
   if (p->cfl <= 0. && !(p->dt > 0.)) return set_error("fixed dt must be positive when cfl <= 0");
   Ops o;
-  if (!get_ops(p->precision, p->nx, p->nc, o)) return set_error("grid size %d not supported (16..1024, powers of 2)", p->nx);
+  if (!get_ops(p->precision, p->nx, p->nc, o))
+    return set_error("grid size %d not supported (16..1024 powers of 2, 48, 96)", p->nx);
   Ctx* c = new Ctx();
   c->p = *p;
   c->n = p->nx;
@@ -753,8 +759,26 @@ int psdns_gpu_finalize(void* ctx) {
 int psdns_gpu_set_state(void* ctx, const double* un, int32_t layout) {
   Ctx* c = (Ctx*)ctx;
   if (!c || !un) return set_error("null argument");
-  if (layout != PSDNS_LAYOUT_YCYL) return set_error("unsupported layout %d", layout);
+  if (layout != PSDNS_LAYOUT_YCYL && layout != PSDNS_LAYOUT_FULL) return set_error("unsupported layout %d", layout);
   const size_t vs = (size_t)c->g.xz_tot * c->n;
+  if (layout == PSDNS_LAYOUT_FULL) {
+    // one variable of the full half-complex array at a time, staged in uz
+    const size_t fs = full_elems(*c);
+    if (fs * sizeof(double2) > c->uz_elems * c->csz) return set_error("full-layout staging does not fit");
+    const Geo g = make_geo(*c);
+    for (int v = 0; v < c->nv; v++) {
+      CK(cudaMemcpyAsync(c->d_uz, un + 2 * v * fs, sizeof(double2) * fs, cudaMemcpyHostToDevice, c->stream));
+      if (c->prec == PSDNS_PREC_FP64)
+        k_full_to_cyl<double><<<148 * 8, 256, 0, c->stream>>>(g, (const double2*)c->d_uz,
+                                                               (double2*)c->d_un + v * vs, (double2*)c->d_u + v * vs);
+      else
+        k_full_to_cyl<float><<<148 * 8, 256, 0, c->stream>>>(g, (const double2*)c->d_uz, (float2*)c->d_un + v * vs,
+                                                              (float2*)c->d_u + v * vs);
+      CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+  }
   // stage one variable at a time: ub holds >= 2 variables of complex double
   for (int v = 0; v < c->nv; v++) {
     CK(cudaMemcpyAsync(c->d_ub, un + 2 * v * vs, sizeof(double2) * vs, cudaMemcpyHostToDevice, c->stream));
@@ -774,10 +798,26 @@ int psdns_gpu_set_state(void* ctx, const double* un, int32_t layout) {
 int psdns_gpu_get_state(void* ctx, double* out, int32_t which, int32_t layout) {
   Ctx* c = (Ctx*)ctx;
   if (!c || !out) return set_error("null argument");
-  if (layout != PSDNS_LAYOUT_YCYL) return set_error("unsupported layout %d", layout);
+  if (layout != PSDNS_LAYOUT_YCYL && layout != PSDNS_LAYOUT_FULL) return set_error("unsupported layout %d", layout);
   if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
   const size_t vs = (size_t)c->g.xz_tot * c->n;
   void* src = which == PSDNS_FIELD_U ? c->d_u : c->d_un;
+  if (layout == PSDNS_LAYOUT_FULL) {
+    const size_t fs = full_elems(*c);
+    if (fs * sizeof(double2) > c->uz_elems * c->csz) return set_error("full-layout staging does not fit");
+    const Geo g = make_geo(*c);
+    for (int v = 0; v < c->nv; v++) {
+      CK(cudaMemsetAsync(c->d_uz, 0, sizeof(double2) * fs, c->stream));
+      if (c->prec == PSDNS_PREC_FP64)
+        k_cyl_to_full<double><<<148 * 8, 256, 0, c->stream>>>(g, (const double2*)src + v * vs, (double2*)c->d_uz);
+      else
+        k_cyl_to_full<float><<<148 * 8, 256, 0, c->stream>>>(g, (const float2*)src + v * vs, (double2*)c->d_uz);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(out + 2 * v * fs, c->d_uz, sizeof(double2) * fs, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+  }
   for (int v = 0; v < c->nv; v++) {
     const int blocks = 148 * 8;
     if (c->prec == PSDNS_PREC_FP64)

@@ -91,12 +91,16 @@ __device__ __forceinline__ void load_twiddles(C2<T>* tw_s, const C2<T>* __restri
   for (int i = threadIdx.x; i < TS; i += blockDim.x) cp_async_elem(tw_s + i, tw_g + i);
 }
 
-// threads of a block that transforms LINES lines at once (capped at CAP)
+// threads of a block that transforms LINES lines at once (capped at CAP, at
+// least one warp, and a multiple of the P threads of a line: P = 6 at
+// n = 48)
+__host__ __device__ constexpr int round_up(int a, int m) { return (a + m - 1) / m * m; }
+__host__ __device__ constexpr int gcd_c(int a, int b) { return b == 0 ? a : gcd_c(b, a % b); }
 template <typename T, int N, int LINES, int CAP = 256>
 struct Launch {
   static constexpr int P = FFTPlan<T, N>::P;
   static constexpr int want = LINES * P;
-  static constexpr int THREADS = want >= CAP ? CAP : (want < 32 ? 32 : want);
+  static constexpr int THREADS = round_up((want >= CAP ? CAP : (want < 32 ? 32 : want)), P);
   static_assert(THREADS % P == 0, "threads per line must divide the block");
 };
 
@@ -361,8 +365,8 @@ struct K3Launch {
   static constexpr int P = FFTPlan<T, N>::P;
   static constexpr int NPAIR = Tiles<T>::TZ / 2;
   static constexpr int want = 5 * NPAIR * P;
-  static constexpr int r32 = (want + 31) / 32 * 32;
-  static constexpr int THREADS = r32 > 1024 ? 1024 : r32;
+  static constexpr int WP = 32 / gcd_c(32, P) * P;   // lcm(32, P): whole warps and whole lines
+  static constexpr int THREADS = round_up(want, WP) > 1024 ? 1024 : round_up(want, WP);
   static_assert(THREADS % P == 0, "threads per line must divide the block");
   // twiddles + 5 product buffers (6 input buffers with a scalar) of TZ/2 lines
   static constexpr size_t SMEM =
@@ -909,6 +913,34 @@ __global__ void k_to_f64(const C2<T>* __restrict__ src, double2* __restrict__ ds
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const C2<T> s = src[i];
     dst[i] = make_double2((double)s.x, (double)s.y);
+  }
+}
+
+// Full half-complex layout u(nxh, ny, nz) (column-major, nxh = n/2 + 1, the
+// FFTW real-to-complex shape of a real (nx, ny, nz) array) <-> cylinder
+// columns: column a = (x, z) holds every y of (x, ., z).
+template <typename T>
+__global__ void k_full_to_cyl(Geo g, const double2* __restrict__ full, C2<T>* __restrict__ dst,
+                              C2<T>* __restrict__ dst2) {
+  const int n = g.n, nxh = n / 2 + 1;
+  const size_t tot = (size_t)g.xz_tot * n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
+    const int a = (int)(i / n), y = (int)(i % n);
+    const double2 s = full[((size_t)__ldg(g.az + a) * n + y) * nxh + __ldg(g.ax + a)];
+    const C2<T> d = cmk<C2<T>>((T)s.x, (T)s.y);
+    dst[i] = d;
+    if (dst2) dst2[i] = d;
+  }
+}
+
+template <typename T>
+__global__ void k_cyl_to_full(Geo g, const C2<T>* __restrict__ src, double2* __restrict__ full) {
+  const int n = g.n, nxh = n / 2 + 1;
+  const size_t tot = (size_t)g.xz_tot * n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
+    const int a = (int)(i / n), y = (int)(i % n);
+    const C2<T> s = src[i];
+    full[((size_t)__ldg(g.az + a) * n + y) * nxh + __ldg(g.ax + a)] = make_double2((double)s.x, (double)s.y);
   }
 }
 

@@ -9,6 +9,7 @@ module psdns_gpu_mod
 
   integer(c_int32_t), parameter :: PSDNS_PREC_FP32 = 0, PSDNS_PREC_FP64 = 1
   integer(c_int32_t), parameter :: PSDNS_LAYOUT_YCYL = 0
+  integer(c_int32_t), parameter :: PSDNS_LAYOUT_FULL = 1
   integer(c_int32_t), parameter :: PSDNS_FIELD_U = 0, PSDNS_FIELD_UN = 1
 
   type, bind(c) :: psdns_params

@@ -21,6 +21,7 @@ _LIB = None
 PREC_FP32 = 0
 PREC_FP64 = 1
 LAYOUT_YCYL = 0
+LAYOUT_FULL = 1
 FIELD_U = 0
 FIELD_UN = 1
 
@@ -195,21 +196,26 @@ class Solver:
         """(3 + nc, xz_tot, n): velocity components, then the scalar."""
         return (3 + self.nc, self.xz_tot, self.n)
 
-    def set_state(self, un):
+    def full_shape(self):
+        """(3 + nc, nz, ny, nx/2+1): the Fortran array u(nxh,ny,nz,nv) in C order."""
+        return (3 + self.nc, self.n, self.n, self.n // 2 + 1)
+
+    def set_state(self, un, layout=LAYOUT_YCYL):
         a = np.ascontiguousarray(un, dtype=np.complex128)
-        if a.shape != self.state_shape():
-            raise ValueError(f"state shape {a.shape} != {self.state_shape()}")
-        _check(load().psdns_gpu_set_state(self._ctx, _dp(a.view(np.float64)), LAYOUT_YCYL), "set_state")
+        want = self.state_shape() if layout == LAYOUT_YCYL else self.full_shape()
+        if a.shape != want:
+            raise ValueError(f"state shape {a.shape} != {want}")
+        _check(load().psdns_gpu_set_state(self._ctx, _dp(a.view(np.float64)), layout), "set_state")
 
     def set_state_ptr(self, ptr):
         """set_state from a raw host pointer (complex(8) YCYL, e.g. pinned memory)."""
         _check(load().psdns_gpu_set_state(self._ctx, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)),
                                           LAYOUT_YCYL), "set_state")
 
-    def get_state(self, which=FIELD_UN, out=None):
+    def get_state(self, which=FIELD_UN, out=None, layout=LAYOUT_YCYL):
         if out is None:
-            out = np.zeros(self.state_shape(), np.complex128)
-        _check(load().psdns_gpu_get_state(self._ctx, _dp(out.view(np.float64)), which, LAYOUT_YCYL),
+            out = np.zeros(self.state_shape() if layout == LAYOUT_YCYL else self.full_shape(), np.complex128)
+        _check(load().psdns_gpu_get_state(self._ctx, _dp(out.view(np.float64)), which, layout),
                "get_state")
         return out
 

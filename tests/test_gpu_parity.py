@@ -59,7 +59,7 @@ def o_seed_default():
     return 122929298
 
 
-@pytest.mark.parametrize("n", [16, 32, 64])
+@pytest.mark.parametrize("n", [16, 32, 48, 64, 96])
 def test_fp64_one_step(oracle_mod, gpu_mod, n):
     u_o, un_o, u_g, un_g, infos, geo = run_pair(oracle_mod, gpu_mod, n, gpu_mod.PREC_FP64, 1)
     so, sg = infos[0]
@@ -80,7 +80,7 @@ def test_fp64_five_steps_adaptive_dt(oracle_mod, gpu_mod):
     assert np.max(np.abs(Eg[m] - Eo[m]) / Eo[m]) < 1e-10
 
 
-@pytest.mark.parametrize("n", [32, 64])
+@pytest.mark.parametrize("n", [32, 48, 64])
 def test_fp32_five_steps(oracle_mod, gpu_mod, n):
     u_o, un_o, u_g, un_g, infos, geo = run_pair(oracle_mod, gpu_mod, n, gpu_mod.PREC_FP32, 5)
     err = rel_l2(un_g, un_o)
@@ -218,3 +218,28 @@ def test_particles_match_oracle(oracle_mod, gpu_mod, prec, tol_p, tol_v):
     assert np.abs(vg - vo).max() < tol_v * np.abs(vo).max()
     assert np.abs(pg - pos).max() > 0.05     # they did move
     o.close(); s.close()
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_full_layout_round_trip(oracle_mod, gpu_mod, prec):
+    """PSDNS_LAYOUT_FULL: u(nxh,ny,nz,nv) <-> cylinder columns (x, ., z)."""
+    n = 32
+    o = oracle_mod.Oracle(n, 0.01)
+    un = o.field_init(55)
+    geo = o.geometry()
+    o.close()
+    s = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=-1.0, dt=0.005)
+    s.set_state(un)
+    full = s.get_state(gpu_mod.FIELD_UN, layout=gpu_mod.LAYOUT_FULL)
+    assert full.shape == (3, n, n, n // 2 + 1)
+    kx = np.repeat(np.arange(len(geo["colstart"]) - 1), np.diff(geo["colstart"]))
+    expect = np.zeros_like(full)
+    expect[:, geo["az"], :, kx] = un.transpose(1, 0, 2)
+    tol = 0 if prec == 1 else 1e-6
+    np.testing.assert_allclose(full, expect, rtol=0, atol=tol * np.abs(un).max())
+    # back through the full layout: the cylinder is reproduced
+    s2 = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=-1.0, dt=0.005)
+    s2.set_state(full, layout=gpu_mod.LAYOUT_FULL)
+    np.testing.assert_allclose(s2.get_state(gpu_mod.FIELD_UN), s.get_state(gpu_mod.FIELD_UN), rtol=0, atol=0)
+    s.close()
+    s2.close()
