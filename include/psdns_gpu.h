@@ -188,6 +188,31 @@ int psdns_gpu_kernel_times(void *ctx, double *ms, int64_t *launches);
 int psdns_gpu_rk_stage_noalloc(const psdns_params *p, int32_t kstep, const double *gsh, const double *dt,
                                void *u_dev, void *un_dev, double *velmax_out, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Ensembles: independent boxes advanced together (no reference routine: the
+ * reference runs one box per job).  p[0..count-1] describe the boxes; each
+ * has its own grid size (16..1024 powers of two, 48, 96), viscosity, dt or
+ * cfl, kshift and seed, and follows exactly the run of a single context made
+ * with the same parameters.  All boxes share precision and beta; nc = 0,
+ * kforce = 0.  Boxes of the same n share every kernel launch (the box is a
+ * grid dimension); boxes with a fixed dt (cfl <= 0) replay each step from a
+ * captured CUDA graph.
+ * ------------------------------------------------------------------------ */
+int psdns_gpu_ensemble_create(const psdns_params *p, int32_t count, void **ens);
+int psdns_gpu_ensemble_destroy(void *ens);
+/* Random solenoidal initial field of box i from seeds[i] (as psdns_gpu_field_init). */
+int psdns_gpu_ensemble_field_init(void *ens, const int32_t *seeds);
+/* State of one box (PSDNS_LAYOUT_YCYL, 3 variables). */
+int psdns_gpu_ensemble_set_state(void *ens, int32_t box, const double *un, int32_t layout);
+int psdns_gpu_ensemble_get_state(void *ens, int32_t box, double *out, int32_t which, int32_t layout);
+/* nsteps RK2 steps of every box; info[8*i .. 8*i+7] = the last step's
+ * psdns_gpu_step info of box i.  Returns 2 if a box met an abort condition
+ * of step.f (the steps are completed). */
+int psdns_gpu_ensemble_step(void *ens, int32_t nsteps, double *info);
+/* Shell spectra of one box (as psdns_gpu_spectra). */
+int psdns_gpu_ensemble_spectra(void *ens, int32_t box, int32_t which, double *ek, double *dk, double *eijk,
+                               double *stats);
+
 /* Message of the last error on this thread ("" if none). */
 int psdns_gpu_last_error(char *buf, int32_t len);
 

@@ -581,6 +581,60 @@ static int run_stage(Ctx& c, const Ops& o, int kstep, int* ctl_err) {
   return 0;
 }
 
+// sptr.f:139-193 shell sums on the device (FP64), :235-237 and :350-400 on
+// the host, for the state at src (one box, geometry g); scratch holds
+// n * kSpecVals doubles
+static int spectra_of(const Geo& g, const void* src, int prec, const psdns_params& p, cudaStream_t stream,
+                      void* scratch, double* ek, double* dk, double* eijk, double* stats) {
+  const int n = g.n, ns = n;   // mxyz = max(nx,ny,nz)/beta_min shells (comsp_set.f:14)
+  const size_t nv = (size_t)ns * kSpecVals;
+  double* d_out = (double*)scratch;
+  CK(cudaMemsetAsync(d_out, 0, nv * sizeof(double), stream));
+  const double b11 = p.beta1 * p.beta1, b22 = p.beta2 * p.beta2, b33 = p.beta3 * p.beta3;
+  const size_t smem = nv * sizeof(double);
+  if (prec == PSDNS_PREC_FP64) {
+    CK(cudaFuncSetAttribute(k_spectra<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_spectra<double><<<148 * 2, 512, smem, stream>>>(g, (const double2*)src, b11, b22, b33, ns, d_out);
+  } else {
+    CK(cudaFuncSetAttribute(k_spectra<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_spectra<float><<<148 * 2, 512, smem, stream>>>(g, (const float2*)src, b11, b22, b33, ns, d_out);
+  }
+  CK(cudaGetLastError());
+  std::vector<double> h(nv);
+  CK(cudaMemcpyAsync(h.data(), d_out, nv * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  const double nu = p.viscos;
+  double tke = 0, eps = 0, skew = 0, ekl = 0;
+  for (int k = 0; k < ns; k++) {
+    const double* v = &h[(size_t)k * kSpecVals];
+    double e = 0.5 * (v[0] + v[3] + v[5]);
+    double d = 0.5 * (2 * nu * v[6]);
+    const double sk = 0.5 * (2 * nu * v[7]);
+    if (k == 0) { e = 0; d = 0; }
+    if (ek) ek[k] = e;
+    if (dk) dk[k] = d;
+    if (eijk) for (int j = 0; j < 6; j++) eijk[(size_t)k * 6 + j] = v[j];
+    tke += e;
+    eps += d;
+    skew += sk;
+    if (k < n / 2) ekl += v[8] / 2.;
+  }
+  const double pi = 4. * std::atan(1.);
+  double klen = 0, kvel = 0, ktime = 0;
+  if (eps > 0) {
+    skew = 2. / 35. * std::pow(15. * nu / eps, 1.5) * skew;
+    klen = std::pow(nu * nu * nu / eps, .25);
+    kvel = std::pow(nu * eps, .25);
+    ktime = std::pow(nu / eps, .5);
+  }
+  ekl = 1.5 * pi / (2 * tke) * ekl;
+  if (stats) {
+    stats[0] = tke; stats[1] = eps; stats[2] = skew; stats[3] = klen; stats[4] = kvel; stats[5] = ktime;
+    stats[6] = ekl;
+  }
+  return 0;
+}
+
 }  // namespace psdns
 
 using namespace psdns;
@@ -991,57 +1045,9 @@ int psdns_gpu_spectra(void* ctx, int32_t which, double* ek, double* dk, double* 
   Ctx* c = (Ctx*)ctx;
   if (!c) return set_error("null context");
   if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
-  const int n = c->n, ns = n;   // mxyz = max(nx,ny,nz)/beta_min shells (comsp_set.f:14)
-  const size_t nv = (size_t)ns * kSpecVals;
   // the ub work array is free between steps: use it for the sums
-  double* d_out = (double*)c->d_ub;
-  CK(cudaMemsetAsync(d_out, 0, nv * sizeof(double), c->stream));
-  Geo g = make_geo(*c);
-  const double b11 = c->p.beta1 * c->p.beta1, b22 = c->p.beta2 * c->p.beta2, b33 = c->p.beta3 * c->p.beta3;
-  const size_t smem = nv * sizeof(double);
-  const void* src = which == PSDNS_FIELD_U ? c->d_u : c->d_un;
-  if (c->prec == PSDNS_PREC_FP64) {
-    CK(cudaFuncSetAttribute(k_spectra<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_spectra<double><<<148 * 2, 512, smem, c->stream>>>(g, (const double2*)src, b11, b22, b33, ns, d_out);
-  } else {
-    CK(cudaFuncSetAttribute(k_spectra<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_spectra<float><<<148 * 2, 512, smem, c->stream>>>(g, (const float2*)src, b11, b22, b33, ns, d_out);
-  }
-  CK(cudaGetLastError());
-  std::vector<double> h(nv);
-  CK(cudaMemcpyAsync(h.data(), d_out, nv * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  // sptr.f:235-237 (2 nu), :350-400
-  const double nu = c->p.viscos;
-  double tke = 0, eps = 0, skew = 0, ekl = 0;
-  for (int k = 0; k < ns; k++) {
-    const double* v = &h[(size_t)k * kSpecVals];
-    double e = 0.5 * (v[0] + v[3] + v[5]);
-    double d = 0.5 * (2 * nu * v[6]);
-    const double sk = 0.5 * (2 * nu * v[7]);
-    if (k == 0) { e = 0; d = 0; }
-    if (ek) ek[k] = e;
-    if (dk) dk[k] = d;
-    if (eijk) for (int j = 0; j < 6; j++) eijk[(size_t)k * 6 + j] = v[j];
-    tke += e;
-    eps += d;
-    skew += sk;
-    if (k < n / 2) ekl += v[8] / 2.;
-  }
-  const double pi = 4. * std::atan(1.);
-  double klen = 0, kvel = 0, ktime = 0;
-  if (eps > 0) {
-    skew = 2. / 35. * std::pow(15. * nu / eps, 1.5) * skew;
-    klen = std::pow(nu * nu * nu / eps, .25);
-    kvel = std::pow(nu * eps, .25);
-    ktime = std::pow(nu / eps, .5);
-  }
-  ekl = 1.5 * pi / (2 * tke) * ekl;
-  if (stats) {
-    stats[0] = tke; stats[1] = eps; stats[2] = skew; stats[3] = klen; stats[4] = kvel; stats[5] = ktime;
-    stats[6] = ekl;
-  }
-  return 0;
+  return spectra_of(make_geo(*c), which == PSDNS_FIELD_U ? c->d_u : c->d_un, c->prec, c->p, c->stream, c->d_ub, ek,
+                    dk, eijk, stats);
 }
 
 int psdns_gpu_forcing_stats(void* ctx, double* efk, double* eirate, double* erate) {
@@ -1104,3 +1110,6 @@ int psdns_gpu_get_time(void* ctx, double* out4) {
 }
 
 }  // extern "C"
+
+// ensembles of boxes (batched stage kernels, CUDA graphs)
+#include "ensemble.cuh"

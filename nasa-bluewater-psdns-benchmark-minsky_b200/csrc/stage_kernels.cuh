@@ -30,6 +30,9 @@ struct Geo {
   const int* ax;         // [xz_tot] x index of column a
   const int* az;         // [xz_tot] z index (0..n-1) of column a
   const int* kymax;      // [xz_tot] largest |ky| inside the sphere
+  // a batch of boxes of the same n (ensembles): box b's u/un, ub and uz start
+  // b * sbox, b * bbox, b * zbox elements after box 0's (0 for one box)
+  size_t sbox = 0, bbox = 0, zbox = 0;
 };
 
 template <typename T> struct StageTables {
@@ -48,6 +51,23 @@ template <typename T> struct StageTables {
   T b11, b22, b33;
   T norm;            // dt2/ny/nz
   const T* spf;      // spline prefilter 6/(4+2cos(2 pi k/n)): [n/2+1] x, [n] y, [n] z
+  // batches: box b's tables start tbox bytes after box (b-1)'s, and its
+  // norm is normv[b] (normv null: one box, norm above)
+  size_t tbox = 0;
+  const T* normv = nullptr;
+
+  __device__ __forceinline__ StageTables at_box(int b) const {
+    StageTables t = *this;
+    if (tbox != 0) {
+      const size_t o = (size_t)b * tbox;
+      auto sh = [o](auto* p) { return p ? (decltype(p))((const char*)p + o) : p; };
+      t.sx = sh(sx); t.sy = sh(sy); t.sz = sh(sz);
+      t.xfac = sh(xfac); t.yfac = sh(yfac); t.zfac = sh(zfac);
+      t.xdif = sh(xdif); t.ydif = sh(ydif); t.zdif = sh(zdif);
+    }
+    if (normv) t.norm = normv[b];
+    return t;
+  }
 };
 
 // per-precision tile sizes: TB_I = columns per K1 block (64 B runs in ub
@@ -123,8 +143,13 @@ template <int N> struct LS { static constexpr int value = N + N / 32 + 4; };
 // ---------------------------------------------------------------------------
 template <typename T, int N, bool SPL = false, int NC = 0>
 __global__ void __launch_bounds__(K1Launch<T, N>::THREADS)
-k_yinv(Geo g, StageTables<T> st, const C2<T>* __restrict__ u, C2<T>* __restrict__ ub,
+k_yinv(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ u, C2<T>* __restrict__ ub,
        const C2<T>* __restrict__ tw_g) {
+  // grid (nab_i, 3 + 2 nc, boxes)
+  const int box = blockIdx.z;
+  const StageTables<T> st = st_all.at_box(box);
+  u += box * g.sbox;
+  ub += box * g.bbox;
   // NC = 1 (one passive scalar, grid.y = 5): ub variable 3 is the shifted
   // scalar and variable 4 its y gradient i b22 ky theta (phase1.f:52-64)
   // SPL: also divide by the cubic B-spline symbol, (4 + 2 cos(2 pi k/n))/6 per
@@ -227,7 +252,11 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
   C* tw = reinterpret_cast<C*>(smem_raw);
   C* buf = tw + FFTPlan<T, N>::TWSIZE;
   load_twiddles<T, N>(tw, tw_g);
-  const int y = blockIdx.x, x0 = blockIdx.y * XT, v = blockIdx.z;
+  // grid (n, ceil(kxn / XT2), (3 + 3 nc) * boxes)
+  constexpr int NVZ = 3 + 3 * NC;
+  const int y = blockIdx.x, x0 = blockIdx.y * XT, v = blockIdx.z % NVZ, box = blockIdx.z / NVZ;
+  ub += box * g.bbox;
+  uz += box * g.zbox;
   const int x1 = min(x0 + XT, g.kxn);
   const int nl = x1 - x0;
   const int sv = v < 3 ? v : (v == 3 ? 4 : 3);
@@ -394,7 +423,10 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
   C* bufE = bufW + NPAIR * L;
   C* bufF = bufE + NPAIR * L;
   load_twiddles<T, N>(tw, tw_g);
-  const int zt = blockIdx.x, y = blockIdx.y;
+  // grid (nzt, n, boxes)
+  const int zt = blockIdx.x, y = blockIdx.y, box = blockIdx.z;
+  uz += box * g.zbox;
+  velmax_bits += box;
   const int kxn = g.kxn;
   // zero the band kx in [kxn, n-kxn] (includes the Nyquist column)
   for (int e = threadIdx.x; e < NVIN * NPAIR * N; e += THREADS) {
@@ -533,7 +565,10 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
   C* s0 = tw + FFTPlan<T, N>::TWSIZE;
   C* s1 = s0 + NLT * L;
   load_twiddles<T, N>(tw, tw_g);
-  const int y0 = blockIdx.x * YT, x0 = blockIdx.y * XT;
+  // grid (n / YT4, ceil(kxn / XT4), boxes)
+  const int y0 = blockIdx.x * YT, x0 = blockIdx.y * XT, box = blockIdx.z;
+  uz += box * g.zbox;
+  ub += box * g.bbox;
   const int x1 = min(x0 + XT, g.kxn);
   const int nl = x1 - x0;
   const int nt = nl * YT;
@@ -602,8 +637,14 @@ __device__ __forceinline__ void project3(C2<T>& u1, C2<T>& u2, C2<T>& u3, T kx, 
 
 template <typename T, int N, int KSTEP, int NC = 0>
 __global__ void __launch_bounds__(K5Launch<T, N, NC>::THREADS)
-k_yfwd(Geo g, StageTables<T> st, const C2<T>* __restrict__ ub, C2<T>* __restrict__ u,
+k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __restrict__ u,
        C2<T>* __restrict__ un, const C2<T>* __restrict__ tw_g, double* __restrict__ efkz) {
+  // grid (nab_f, boxes); forcing (efkz) is for single boxes only
+  const int box = blockIdx.y;
+  const StageTables<T> st = st_all.at_box(box);
+  ub += box * g.bbox;
+  u += box * g.sbox;
+  un += box * g.sbox;
   // NC = 1: ub slot 4 is the scalar advection term; the scalar is un-shifted
   // (wavespace_module.f:344-357) and advanced with the diffusivity factors
   // xdif ydif zdif (proc4a.f:508-522, proc4b.f:69-75), without projection

@@ -27,6 +27,13 @@ FIELD_UN = 1
 
 # every entry point declared in include/psdns_gpu.h
 EXPORTS = (
+    "psdns_gpu_ensemble_create",
+    "psdns_gpu_ensemble_destroy",
+    "psdns_gpu_ensemble_field_init",
+    "psdns_gpu_ensemble_set_state",
+    "psdns_gpu_ensemble_get_state",
+    "psdns_gpu_ensemble_step",
+    "psdns_gpu_ensemble_spectra",
     "psdns_gpu_default_params",
     "psdns_gpu_geometry",
     "psdns_gpu_init",
@@ -103,6 +110,13 @@ def load():
     L.psdns_gpu_spectra.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
+    L.psdns_gpu_ensemble_create.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]
+    L.psdns_gpu_ensemble_destroy.argtypes = [vp]
+    L.psdns_gpu_ensemble_field_init.argtypes = [vp, ip]
+    L.psdns_gpu_ensemble_set_state.argtypes = [vp, ctypes.c_int32, dp, ctypes.c_int32]
+    L.psdns_gpu_ensemble_get_state.argtypes = [vp, ctypes.c_int32, dp, ctypes.c_int32, ctypes.c_int32]
+    L.psdns_gpu_ensemble_step.argtypes = [vp, ctypes.c_int32, dp]
+    L.psdns_gpu_ensemble_spectra.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, dp, dp, dp, dp]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     _LIB = L
@@ -301,3 +315,65 @@ class Solver:
         out = np.zeros(4, np.float64)
         _check(load().psdns_gpu_get_time(self._ctx, _dp(out)), "get_time")
         return {"time": out[0], "dt": out[1], "velmax": out[2], "jstep": int(out[3])}
+
+
+class Ensemble:
+    """Independent boxes advanced together (psdns_gpu_ensemble_*): boxes of
+    the same n share every kernel launch; fixed-dt boxes replay CUDA graphs."""
+
+    def __init__(self, params_list):
+        L = load()
+        self.params = list(params_list)
+        arr = (Params * len(self.params))(*self.params)
+        self._ens = ctypes.c_void_p()
+        _check(L.psdns_gpu_ensemble_create(arr, len(self.params), ctypes.byref(self._ens)),
+               "psdns_gpu_ensemble_create")
+        self.count = len(self.params)
+        self.shapes = []
+        for p in self.params:
+            g = geometry(p.nx)
+            self.shapes.append((3, g["xz_tot"], p.nx))
+
+    def close(self):
+        if self._ens:
+            load().psdns_gpu_ensemble_destroy(self._ens)
+            self._ens = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def field_init(self, seeds):
+        s = np.ascontiguousarray(seeds, dtype=np.int32)
+        _check(load().psdns_gpu_ensemble_field_init(self._ens, s.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))),
+               "ensemble_field_init")
+
+    def set_state(self, box, un):
+        a = np.ascontiguousarray(un, dtype=np.complex128)
+        if a.shape != self.shapes[box]:
+            raise ValueError(f"state shape {a.shape} != {self.shapes[box]}")
+        _check(load().psdns_gpu_ensemble_set_state(self._ens, int(box), _dp(a.view(np.float64)), LAYOUT_YCYL),
+               "ensemble_set_state")
+
+    def get_state(self, box, which=FIELD_UN):
+        out = np.zeros(self.shapes[box], np.complex128)
+        _check(load().psdns_gpu_ensemble_get_state(self._ens, int(box), _dp(out.view(np.float64)), int(which),
+                                                   LAYOUT_YCYL), "ensemble_get_state")
+        return out
+
+    def step(self, nsteps=1):
+        """Advance every box nsteps steps; returns (status, info[count, 8])."""
+        info = np.zeros((self.count, 8), np.float64)
+        rc = load().psdns_gpu_ensemble_step(self._ens, int(nsteps), _dp(info))
+        if rc not in (0, 2):
+            _check(rc, "psdns_gpu_ensemble_step")
+        return rc, info
+
+    def spectra(self, box, which=FIELD_UN):
+        n = self.params[box].nx
+        ek = np.zeros(n); dk = np.zeros(n); e6 = np.zeros(n * 6); st = np.zeros(7)
+        _check(load().psdns_gpu_ensemble_spectra(self._ens, int(box), int(which), _dp(ek), _dp(dk), _dp(e6),
+                                                 _dp(st)), "ensemble_spectra")
+        return ek, dk, e6.reshape(n, 6), dict(zip(["tke", "eps", "skew", "klen", "kvel", "ktime", "ekl"], st))
