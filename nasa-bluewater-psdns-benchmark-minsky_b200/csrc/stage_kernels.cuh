@@ -20,6 +20,8 @@
 //                 (wavespace_vel.f:163-174), proc4a/proc4b update, projection and
 //                 Eswaran-Pope forcing (proc4a.f:418-651, proc4b.f:38-205)
 #pragma once
+#include <type_traits>
+
 #include "fft_core.cuh"
 
 namespace psdns {
@@ -142,7 +144,7 @@ template <int N> struct LS { static constexpr int value = N + N / 32 + 4; };
 // grid (ceil(xz_tot/TB_I), 3); one block = one ub block of TB_I columns
 // ---------------------------------------------------------------------------
 template <typename T, int N, bool SPL = false, int NC = 0>
-__global__ void __launch_bounds__(K1Launch<T, N>::THREADS)
+__global__ void __launch_bounds__(K1Launch<T, N>::THREADS, 3)
 k_yinv(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ u, C2<T>* __restrict__ ub,
        const C2<T>* __restrict__ tw_g) {
   // grid (nab_i, 3 + 2 nc, boxes)
@@ -275,7 +277,7 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
     C* p = buf + l * L + pad32(z);
     if (z <= kc || z >= N - kc) {
       const int a = ac + (z <= kc ? z : z - N + 2 * kc + 1);
-      cp_async_elem(p, src + ((size_t)(a / TB) * N + y) * TB + (a % TB));
+      cp_async_elem(p, src + ((size_t)((unsigned)a / TB) * N + y) * TB + ((unsigned)a % TB));
     } else {
       *p = cmk<C>(0, 0);
     }
@@ -487,15 +489,26 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
 template <typename T, int N>
 __device__ __forceinline__ void zfwd_load(const Geo& g, const C2<T>* __restrict__ uz, int slot, int y0, int ny,
                                           int x0, int nl, C2<T>* buf, int L) {
-  // lines l = yy*nl + xl, rows y0+yy, columns x0+xl
-  constexpr int TZ = Tiles<T>::TZ;
+  // lines l = yy*nl + xl, rows y0+yy, columns x0+xl; full tiles (nl = XT4)
+  // take the loop with compile-time divisors
+  constexpr int TZ = Tiles<T>::TZ, XT = Tiles<T>::XT4;
+  auto copy = [&](auto nlc, const C2<T>* src, C2<T>* b) {
+    constexpr int NLC = decltype(nlc)::value;
+    const unsigned w = (NLC > 0 ? NLC : nl) * TZ;
+    const unsigned cnt = (NLC > 0 ? NLC : nl) * N;
+    for (unsigned e = threadIdx.x; e < cnt; e += blockDim.x) {
+      const unsigned zt = e / w, rem = e % w, l = rem / TZ, zz = rem % TZ;
+      cp_async_elem(b + l * L + pad32(zt * TZ + zz), src + ((size_t)zt * g.kxn + l) * TZ + zz);
+    }
+  };
   for (int yy = 0; yy < ny; yy++) {
     const size_t vbase = ((size_t)slot * N + y0 + yy) * g.nzt;
+    const C2<T>* src = uz + (vbase * g.kxn + x0) * TZ;
     C2<T>* b = buf + yy * nl * L;
-    for (int e = threadIdx.x; e < nl * N; e += blockDim.x) {
-      const int zt = e / (nl * TZ), rem = e % (nl * TZ), l = rem / TZ, zz = rem % TZ;
-      cp_async_elem(b + l * L + pad32(zt * TZ + zz), uz + ((vbase + zt) * g.kxn + x0 + l) * TZ + zz);
-    }
+    if (nl == XT)
+      copy(std::integral_constant<int, XT>(), src, b);
+    else
+      copy(std::integral_constant<int, 0>(), src, b);
   }
 }
 
@@ -545,12 +558,12 @@ __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const 
     } else {
       out = s1[i];
     }
-    dst[((size_t)(a / TB) * N + y0 + yy) * TB + (a % TB)] = out;
+    dst[((size_t)((unsigned)a / TB) * N + y0 + yy) * TB + ((unsigned)a % TB)] = out;
   }
 }
 
 template <typename T, int N, int NC = 0>
-__global__ void __launch_bounds__(K4Launch<T, N>::THREADS)
+__global__ void __launch_bounds__(K4Launch<T, N>::THREADS, 3)
 k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>* __restrict__ tw_g,
        T b11, T b33) {
   // NC = 1: the scalar advection term (uz slot 5) goes to ub slot 4 without
