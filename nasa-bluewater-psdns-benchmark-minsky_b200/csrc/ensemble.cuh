@@ -90,7 +90,7 @@ template <typename T, int N> struct EnsImpl {
     C* ub = (C*)e.d_ub;
     C* uz = (C*)e.d_uz;
     const int kxn = e.g.kxn, nb = e.nb;
-    k_yinv<T, N><<<dim3(e.nab_i, 3, nb), K1Launch<T, N>::THREADS, I::sm1(), e.stream>>>(g, st, u, ub, tw);
+    k_yinv<T, N><<<dim3(k1_blocks<T>(e.nab_i), 3, nb), K1Launch<T, N>::THREADS, I::sm1(), e.stream>>>(g, st, u, ub, tw);
     k_zinv<T, N><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3 * nb), Launch<T, N, TL::XT2>::THREADS, I::sm2(),
                    e.stream>>>(g, ub, uz, tw, st.b11, st.b33);
     k_xchain<T, N><<<dim3(e.nzt, N, nb), K3Launch<T, N, 0>::THREADS, I::sm3(), e.stream>>>(
@@ -177,7 +177,8 @@ static int ens_alloc_class(EnsClass& e) {
   // per-box strides rounded to 256 bytes so that every box's arrays stay aligned
   auto up = [csz](size_t el) { return ((el * csz + 255) / 256 * 256) / csz; };
   e.st_elems = up((size_t)3 * e.g.xz_tot * n);
-  e.ub_elems = up(std::max((size_t)3 * e.nab_i * tbi, (size_t)4 * e.nab_f * tbf) * n);
+  const size_t ubi = dbl ? ubi_var_elems<double>(e.nab_i, n) : ubi_var_elems<float>(e.nab_i, n);
+  e.ub_elems = up(std::max((size_t)3 * ubi, (size_t)4 * e.nab_f * tbf * n));
   e.uz_elems = up((size_t)5 * n * n * e.g.kxn);
   e.tab_bytes = dbl ? TabLayout<double>(n).total : TabLayout<float>(n).total;
   const size_t nb = e.nb;

@@ -284,7 +284,7 @@ template <typename T, int N, int NC> struct Impl {
     C* uz = (C*)c.d_uz;
     const int kxn = c.g.kxn;
     prof_mark(c, 0, 5, 0);
-    k_yinv<T, N, true><<<dim3(c.nab_i, 3), K1Launch<T, N>::THREADS, sm1(), c.stream>>>(g, st, (const C*)c.d_u,
+    k_yinv<T, N, true><<<dim3(k1_blocks<T>(c.nab_i), 3), K1Launch<T, N>::THREADS, sm1(), c.stream>>>(g, st, (const C*)c.d_u,
                                                                                                ub, tw);
     k_zinv<T, N><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3), Launch<T, N, TL::XT2>::THREADS, sm2(), c.stream>>>(
         g, ub, uz, tw);
@@ -324,7 +324,7 @@ template <typename T, int N, int NC> struct Impl {
     {
       constexpr int TH = K1Launch<T, N>::THREADS;
       prof_mark(c, s, 0, 0);
-      k_yinv<T, N, false, NC><<<dim3(c.nab_i, 3 + 2 * NC), TH, sm1(), c.stream>>>(g, st, u, ub, tw);
+      k_yinv<T, N, false, NC><<<dim3(k1_blocks<T>(c.nab_i), 3 + 2 * NC), TH, sm1(), c.stream>>>(g, st, u, ub, tw);
       prof_mark(c, s, 0, 1);
     }
     {
@@ -715,7 +715,8 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
   c->nab_f = (c->g.xz_tot + tbf - 1) / tbf;
   // ub: 3 + 2 nc backward variables (TB_I blocks) or 4 + nc forward terms
   // (TB_F blocks); uz: 5 + nc slots (3 + 3 nc inputs, 5 + nc outputs)
-  c->ub_elems = std::max((size_t)(3 + 2 * c->nc) * c->nab_i * tbi, (size_t)(4 + c->nc) * c->nab_f * tbf) * n;
+  const size_t ubi = dbl ? ubi_var_elems<double>(c->nab_i, n) : ubi_var_elems<float>(c->nab_i, n);
+  c->ub_elems = std::max((size_t)(3 + 2 * c->nc) * ubi, (size_t)(4 + c->nc) * c->nab_f * tbf * n);
   c->uz_elems = (size_t)(5 + c->nc) * n * n * c->g.kxn;
   c->st_elems = (size_t)c->nv * c->g.xz_tot * n;
   c->rng.init(p->seed_input);

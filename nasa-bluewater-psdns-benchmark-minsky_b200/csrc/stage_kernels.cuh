@@ -78,9 +78,22 @@ template <typename T> struct StageTables {
 // Eight lines per block keep two to three blocks resident per SM, so that
 // one block's copies overlap another's transforms; sixteen-line blocks (one
 // per SM) measured slower for K1 and K4.
+// The inverse ub layout is blocked by TBL_I = 2 TB_I columns (128 B runs for
+// K2's reads), filled by pairs of K1 blocks.
 template <typename T> struct Tiles;
-template <> struct Tiles<float> { static constexpr int TB_I = 8, TB_F = 4, TZ = 4, XT2 = 8, XT4 = 4, YT4 = 1; };
-template <> struct Tiles<double> { static constexpr int TB_I = 4, TB_F = 2, TZ = 2, XT2 = 4, XT4 = 2, YT4 = 1; };
+template <> struct Tiles<float> {
+  static constexpr int TB_I = 8, TBL_I = 16, TB_F = 4, TZ = 4, XT2 = 8, XT4 = 4, YT4 = 1;
+};
+template <> struct Tiles<double> {
+  static constexpr int TB_I = 4, TBL_I = 8, TB_F = 2, TZ = 2, XT2 = 4, XT4 = 2, YT4 = 1;
+};
+
+// elements of one variable of the inverse ub layout [a/TBL_I][y][a%TBL_I]
+template <typename T>
+__host__ __device__ __forceinline__ size_t ubi_var_elems(int nab_i, int n) {
+  constexpr int R = Tiles<T>::TBL_I / Tiles<T>::TB_I;
+  return (size_t)((nab_i + R - 1) / R * R) * Tiles<T>::TB_I * n;
+}
 
 template <int N> __device__ __forceinline__ int kwave(int i) { return i > N / 2 ? i - N : i; }
 
@@ -228,12 +241,20 @@ k_yinv(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ u, C2<T>* __restr
   }
   __syncthreads();
   fft_lines<T, N, THREADS>(buf, TB, L, tw);
-  C* out = ub + ((size_t)v * g.nab_i + at) * N * TB;
+  // columns a0 + l sit at ((a / TBL) n + y) TBL + a % TBL of variable v: a
+  // block writes 64-byte halves of the 128-byte runs (a sequential pair of
+  // groups per block measured slower than independent blocks)
+  constexpr int TBL = Tiles<T>::TBL_I, R = TBL / TB;
+  C* out = ub + (size_t)v * ubi_var_elems<T>(g.nab_i, N) + (size_t)(at / R) * N * TBL + (at % R) * TB;
   for (int e = threadIdx.x; e < TB * N; e += THREADS) {
     const int y = e / TB, l = e % TB;
-    out[e] = cconj(buf[l * L + pad32(y)]);
+    out[y * TBL + l] = cconj(buf[l * L + pad32(y)]);
   }
 }
+
+// K1 grid.x: one block per TB_I columns
+template <typename T>
+__host__ __device__ __forceinline__ int k1_blocks(int nab_i) { return nab_i; }
 
 // ---------------------------------------------------------------------------
 // K2: cylinder unpack (zero fill) + z backward FFT, store to uz
@@ -262,7 +283,8 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
   const int x1 = min(x0 + XT, g.kxn);
   const int nl = x1 - x0;
   const int sv = v < 3 ? v : (v == 3 ? 4 : 3);
-  const C* src = ub + (size_t)sv * g.nab_i * N * TB;
+  constexpr int TBL = Tiles<T>::TBL_I;
+  const C* src = ub + (size_t)sv * ubi_var_elems<T>(g.nab_i, N);
   // slot (l, z): column x0 + l holds kz = 0..kc then -kc..-1 (count 2 kc + 1,
   // mpisetup.f:322-357), so its cylinder index follows from colstart alone.
   // Cylinder entries are copied raw, the cut band is zeroed, then each
@@ -277,7 +299,7 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
     C* p = buf + l * L + pad32(z);
     if (z <= kc || z >= N - kc) {
       const int a = ac + (z <= kc ? z : z - N + 2 * kc + 1);
-      cp_async_elem(p, src + ((size_t)((unsigned)a / TB) * N + y) * TB + ((unsigned)a % TB));
+      cp_async_elem(p, src + ((size_t)((unsigned)a / TBL) * N + y) * TBL + ((unsigned)a % TBL));
     } else {
       *p = cmk<C>(0, 0);
     }

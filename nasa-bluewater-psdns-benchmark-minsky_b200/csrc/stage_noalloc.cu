@@ -73,7 +73,7 @@ static Plan plan_for(const Geometry& g) {
   using TL = Tiles<T>;
   const size_t cs = sizeof(C2<T>);
   const size_t nab_i = (g.xz_tot + TL::TB_I - 1) / TL::TB_I, nab_f = (g.xz_tot + TL::TB_F - 1) / TL::TB_F;
-  const size_t ub_el = std::max(3 * nab_i * TL::TB_I, 4 * nab_f * TL::TB_F) * N;
+  const size_t ub_el = std::max(3 * ubi_var_elems<T>((int)nab_i, N), 4 * nab_f * TL::TB_F * N);
   const size_t uz_el = (size_t)5 * N * N * g.kxn;
   const size_t tab = 2 * (N / 2 + 1 + 2 * N) * cs + (N / 2 + 1 + 2 * N) * sizeof(T);
   Plan p;
@@ -185,7 +185,7 @@ static int run(const psdns_params* prm, int kstep, const double* gsh, double dt,
   const int kxn = g.kxn;
   {
     constexpr int TH = K1Launch<T, N>::THREADS;
-    k_yinv<T, N><<<dim3(geo.nab_i, 3), TH, TWB + sizeof(C) * TL::TB_I * L, st>>>(geo, stb, u, ub, twd);
+    k_yinv<T, N><<<dim3(k1_blocks<T>(geo.nab_i), 3), TH, TWB + sizeof(C) * TL::TB_I * L, st>>>(geo, stb, u, ub, twd);
   }
   {
     constexpr int TH = Launch<T, N, TL::XT2>::THREADS;
