@@ -178,7 +178,7 @@ static int ens_alloc_class(EnsClass& e) {
   auto up = [csz](size_t el) { return ((el * csz + 255) / 256 * 256) / csz; };
   e.st_elems = up((size_t)3 * e.g.xz_tot * n);
   const size_t ubi = dbl ? ubi_var_elems<double>(e.nab_i, n) : ubi_var_elems<float>(e.nab_i, n);
-  e.ub_elems = up(std::max((size_t)3 * ubi, (size_t)4 * e.nab_f * tbf * n));
+  e.ub_elems = up(std::max((size_t)3 * ubi, (size_t)4 * (dbl ? ubf_var_elems<double>(e.nab_f, n) : ubf_var_elems<float>(e.nab_f, n))));
   e.uz_elems = up((size_t)5 * n * n * e.g.kxn);
   e.tab_bytes = dbl ? TabLayout<double>(n).total : TabLayout<float>(n).total;
   const size_t nb = e.nb;

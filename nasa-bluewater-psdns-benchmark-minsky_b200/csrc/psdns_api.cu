@@ -716,7 +716,7 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
   // ub: 3 + 2 nc backward variables (TB_I blocks) or 4 + nc forward terms
   // (TB_F blocks); uz: 5 + nc slots (3 + 3 nc inputs, 5 + nc outputs)
   const size_t ubi = dbl ? ubi_var_elems<double>(c->nab_i, n) : ubi_var_elems<float>(c->nab_i, n);
-  c->ub_elems = std::max((size_t)(3 + 2 * c->nc) * ubi, (size_t)(4 + c->nc) * c->nab_f * tbf * n);
+  c->ub_elems = std::max((size_t)(3 + 2 * c->nc) * ubi, (size_t)(4 + c->nc) * (dbl ? ubf_var_elems<double>(c->nab_f, n) : ubf_var_elems<float>(c->nab_f, n)));
   c->uz_elems = (size_t)(5 + c->nc) * n * n * c->g.kxn;
   c->st_elems = (size_t)c->nv * c->g.xz_tot * n;
   c->rng.init(p->seed_input);

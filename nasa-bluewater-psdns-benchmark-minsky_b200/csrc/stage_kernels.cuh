@@ -82,11 +82,19 @@ template <typename T> struct StageTables {
 // K2's reads), filled by pairs of K1 blocks.
 template <typename T> struct Tiles;
 template <> struct Tiles<float> {
-  static constexpr int TB_I = 8, TBL_I = 16, TB_F = 4, TZ = 4, XT2 = 8, XT4 = 4, YT4 = 1;
+  static constexpr int TB_I = 8, TBL_I = 16, TB_F = 4, TBL_F = 8, TZ = 4, XT2 = 8, XT4 = 4, YT4 = 1;
 };
 template <> struct Tiles<double> {
-  static constexpr int TB_I = 4, TBL_I = 8, TB_F = 2, TZ = 2, XT2 = 4, XT4 = 2, YT4 = 1;
+  static constexpr int TB_I = 4, TBL_I = 8, TB_F = 2, TBL_F = 4, TZ = 2, XT2 = 4, XT4 = 2, YT4 = 1;
 };
+
+// elements of one variable of the forward ub layout [a/TBL_F][y][a%TBL_F]
+// (K4 writes 64-byte runs; K5 blocks of TB_F columns read halves)
+template <typename T>
+__host__ __device__ __forceinline__ size_t ubf_var_elems(int nab_f, int n) {
+  constexpr int R = Tiles<T>::TBL_F / Tiles<T>::TB_F;
+  return (size_t)((nab_f + R - 1) / R * R) * Tiles<T>::TB_F * n;
+}
 
 // elements of one variable of the inverse ub layout [a/TBL_I][y][a%TBL_I]
 template <typename T>
@@ -541,12 +549,12 @@ __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const 
   constexpr int ny = Tiles<T>::YT4;
   // the ny rows of one block column are adjacent in ub: write them together
   using C = C2<T>;
-  constexpr int TB = Tiles<T>::TB_F;
+  constexpr int TB = Tiles<T>::TBL_F;   // runs of the forward ub layout
   const int nl = x1 - x0;
   const int abeg = __ldg(g.colstart + x0), aend = __ldg(g.colstart + x1);
   const int as = abeg - (abeg % TB);                      // first block boundary
   const int cnt = ((aend - as + TB - 1) / TB) * TB * ny;  // whole blocks x rows
-  C* dst = ub + (size_t)slot * g.nab_f * N * TB;
+  C* dst = ub + (size_t)slot * ubf_var_elems<T>(g.nab_f, N);
   // column starts of the XT lines: x and z of a cylinder index follow from
   // them (column x0 + j holds kz = 0..kc then -kc..-1)
   constexpr int XT = Tiles<T>::XT4;
@@ -694,10 +702,11 @@ k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __rest
   load_twiddles<T, N>(tw, tw_g);
   const int at = blockIdx.x, a0 = at * TB;
   for (int v = 0; v < NVF; v++) {
-    const C* src = ub + ((size_t)v * g.nab_f + at) * N * TB;
+    constexpr int TBL = Tiles<T>::TBL_F, R = TBL / TB;
+    const C* src = ub + (size_t)v * ubf_var_elems<T>(g.nab_f, N) + (size_t)(at / R) * N * TBL + (at % R) * TB;
     for (int e = threadIdx.x; e < TB * N; e += THREADS) {
       const int y = e / TB, l = e % TB;
-      cp_async_elem(buf + (v * TB + l) * L + pad32(y), src + e);
+      cp_async_elem(buf + (v * TB + l) * L + pad32(y), src + y * TBL + l);
     }
   }
   const size_t vs = (size_t)g.xz_tot * N;

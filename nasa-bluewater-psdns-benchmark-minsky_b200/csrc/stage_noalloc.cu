@@ -73,7 +73,7 @@ static Plan plan_for(const Geometry& g) {
   using TL = Tiles<T>;
   const size_t cs = sizeof(C2<T>);
   const size_t nab_i = (g.xz_tot + TL::TB_I - 1) / TL::TB_I, nab_f = (g.xz_tot + TL::TB_F - 1) / TL::TB_F;
-  const size_t ub_el = std::max(3 * ubi_var_elems<T>((int)nab_i, N), 4 * nab_f * TL::TB_F * N);
+  const size_t ub_el = std::max(3 * ubi_var_elems<T>((int)nab_i, N), 4 * ubf_var_elems<T>((int)nab_f, N));
   const size_t uz_el = (size_t)5 * N * N * g.kxn;
   const size_t tab = 2 * (N / 2 + 1 + 2 * N) * cs + (N / 2 + 1 + 2 * N) * sizeof(T);
   Plan p;
