@@ -79,6 +79,49 @@ module psdns_gpu_mod
       type(c_ptr), value :: ctx
       real(c_double), intent(out) :: pos(*), vel(*)
     end function
+    ! ensembles of independent boxes (params(count): one psdns_params per box)
+    integer(c_int) function psdns_gpu_ensemble_create(params, count, ens) bind(c, name='psdns_gpu_ensemble_create')
+      import :: c_int, c_ptr, c_int32_t, psdns_params
+      type(psdns_params), intent(in) :: params(*)
+      integer(c_int32_t), value :: count
+      type(c_ptr), intent(out) :: ens
+    end function
+    integer(c_int) function psdns_gpu_ensemble_destroy(ens) bind(c, name='psdns_gpu_ensemble_destroy')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ens
+    end function
+    integer(c_int) function psdns_gpu_ensemble_field_init(ens, seeds) bind(c, name='psdns_gpu_ensemble_field_init')
+      import :: c_int, c_ptr, c_int32_t
+      type(c_ptr), value :: ens
+      integer(c_int32_t), intent(in) :: seeds(*)
+    end function
+    integer(c_int) function psdns_gpu_ensemble_set_state(ens, box, un, layout) &
+        bind(c, name='psdns_gpu_ensemble_set_state')
+      import :: c_int, c_ptr, c_int32_t, c_double
+      type(c_ptr), value :: ens
+      integer(c_int32_t), value :: box, layout
+      real(c_double), intent(in) :: un(*)
+    end function
+    integer(c_int) function psdns_gpu_ensemble_get_state(ens, box, out, which, layout) &
+        bind(c, name='psdns_gpu_ensemble_get_state')
+      import :: c_int, c_ptr, c_int32_t, c_double
+      type(c_ptr), value :: ens
+      integer(c_int32_t), value :: box, which, layout
+      real(c_double), intent(out) :: out(*)
+    end function
+    integer(c_int) function psdns_gpu_ensemble_step(ens, nsteps, info) bind(c, name='psdns_gpu_ensemble_step')
+      import :: c_int, c_ptr, c_int32_t, c_double
+      type(c_ptr), value :: ens
+      integer(c_int32_t), value :: nsteps
+      real(c_double), intent(out) :: info(*)
+    end function
+    integer(c_int) function psdns_gpu_ensemble_spectra(ens, box, which, ek, dk, eijk, stats) &
+        bind(c, name='psdns_gpu_ensemble_spectra')
+      import :: c_int, c_ptr, c_int32_t, c_double
+      type(c_ptr), value :: ens
+      integer(c_int32_t), value :: box, which
+      real(c_double), intent(out) :: ek(*), dk(*), eijk(*), stats(7)
+    end function
     integer(c_int) function psdns_gpu_last_error(buf, len) bind(c, name='psdns_gpu_last_error')
       import :: c_int, c_char, c_int32_t
       character(kind=c_char), intent(out) :: buf(*)
