@@ -13,7 +13,9 @@ uniformly at random (seeded); all data is synthetic.
 
 `value` is points per second (Gpts/s = n^3 / step time) with the state
 resident in HBM; `e2e` is the same metric through the C-ABI with the state in
-pinned host memory, copied in and out every step.
+pinned host memory, copied in and out every step (psdns_gpu_set_state_async /
+psdns_gpu_get_state_async: chunked copies on their own streams, so that the
+upload of a step overlaps the download of the one before).
 
 Multi-GPU: one independent box per GPU (replicas only; the single-box path
 has no data-path collective), timed as the max over ranks.
@@ -341,10 +343,14 @@ def main():
             f0 = torch.cuda.Event(enable_timing=True)
             f1 = torch.cuda.Event(enable_timing=True)
             f0.record(stream)
+            # each step: upload the state from pinned memory, step, download
+            # the new state to the same buffer; the asynchronous calls let an
+            # upload overlap the previous download chunk by chunk
             for _ in range(args.e2e_steps):
-                s.set_state_ptr(ptr)
+                s.set_state_async_ptr(ptr)
                 s.step()
-                s.get_state_ptr(ptr)
+                s.get_state_async_ptr(ptr)
+            s.sync()
             f1.record(stream)
             f1.synchronize()
             ems = f0.elapsed_time(f1) / args.e2e_steps

@@ -102,6 +102,19 @@ int psdns_gpu_field_init(void *ctx, int32_t seed);
 /* Copy u or un back to a host array (complex(8), 3+nc variables). */
 int psdns_gpu_get_state(void *ctx, double *out, int32_t which, int32_t layout);
 
+/* Asynchronous versions of set_state/get_state (PSDNS_LAYOUT_YCYL only):
+ * the copies run on the context's own copy streams through device staging
+ * (2 x 16 bytes per state element, allocated on first use), in chunks that
+ * overlap the conversions, and an upload overlaps the download issued before
+ * it (PCIe is full duplex).  Work on the state issued afterwards (step,
+ * rk_stage, spectra, ...) is ordered after the upload.  The host buffers
+ * must stay untouched until psdns_gpu_sync returns; an upload from the host
+ * range of a pending download reads each chunk after it has landed. */
+int psdns_gpu_set_state_async(void *ctx, const double *un, int32_t layout);
+int psdns_gpu_get_state_async(void *ctx, double *out, int32_t which, int32_t layout);
+/* Wait for every copy and kernel of the context. */
+int psdns_gpu_sync(void *ctx);
+
 /* One full RK2 time step: shifts (PSDNS/shifts.f), then rksubstep(1) and
  * rksubstep(2) (PSDNS/timestep_module.f:25-55) with step/force at stage 1.
  * On return info[0..7] = dt, time, velmax, courant number, gsh(1..3,1)

@@ -167,6 +167,15 @@ struct Ctx {
   // per-kernel CUDA-event timing: [stage][kernel][begin/end]
   bool prof = false;
   cudaEvent_t ev[2][6][2] = {};
+  // asynchronous state copies: copy streams, complex(8) staging of the whole
+  // state in each direction, per-chunk events (allocated on first use)
+  static constexpr int kChunks = 12;
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  void *d_in_stage = nullptr, *d_out_stage = nullptr;
+  cudaEvent_t ev_h2d[kChunks] = {}, ev_conv_in[kChunks] = {}, ev_conv_out[kChunks] = {}, ev_d2h[kChunks] = {};
+  const char* pend_out = nullptr;    // host range of the last get_state_async
+  size_t pend_out_bytes = 0;
+  bool in_pending = false;
   double prof_ms[6] = {0, 0, 0, 0, 0, 0};
   long long prof_n[6] = {0, 0, 0, 0, 0, 0};
   bool prof_pending[2] = {false, false};
@@ -635,6 +644,41 @@ static int spectra_of(const Geo& g, const void* src, int prec, const psdns_param
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Asynchronous state copies (YCYL): the state is cut into kChunks contiguous
+// pieces; H2D and D2H run on their own streams through complex(8) staging,
+// so that the copies of one call overlap the conversions, and the upload of
+// a state overlaps the download of the previous one (PCIe is full duplex).
+// A chunk of set_state_async whose host range is that of a pending
+// get_state_async waits only for that chunk's download.
+// ---------------------------------------------------------------------------
+static int async_setup(Ctx& c) {
+  if (c.s_in) return 0;
+  const size_t bytes = sizeof(double2) * c.st_elems;
+  size_t freeb = 0, totb = 0;
+  CK(cudaMemGetInfo(&freeb, &totb));
+  if (2 * bytes + (size_t)256 * 1024 * 1024 > freeb)
+    return set_error("asynchronous state copies need %.2f GB of staging, %.2f GB free", 2 * bytes / 1e9,
+                     freeb / 1e9);
+  CK(cudaMalloc(&c.d_in_stage, bytes));
+  CK(cudaMalloc(&c.d_out_stage, bytes));
+  CK(cudaStreamCreateWithFlags(&c.s_in, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&c.s_out, cudaStreamNonBlocking));
+  for (int k = 0; k < Ctx::kChunks; k++) {
+    CK(cudaEventCreateWithFlags(&c.ev_h2d[k], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c.ev_conv_in[k], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c.ev_conv_out[k], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c.ev_d2h[k], cudaEventDisableTiming));
+  }
+  return 0;
+}
+
+static void chunk_range(const Ctx& c, int k, size_t& off, size_t& cnt) {
+  const size_t tot = c.st_elems, per = (tot + Ctx::kChunks - 1) / Ctx::kChunks;
+  off = std::min(tot, per * k);
+  cnt = std::min(tot, off + per) - off;
+}
+
 }  // namespace psdns
 
 using namespace psdns;
@@ -802,11 +846,105 @@ int psdns_gpu_finalize(void* ctx) {
     for (int k = 0; k < 6; k++)
       for (int e = 0; e < 2; e++)
         if (c->ev[s][k][e]) cudaEventDestroy(c->ev[s][k][e]);
+  if (c->s_in) cudaStreamSynchronize(c->s_in);
+  if (c->s_out) cudaStreamSynchronize(c->s_out);
+  for (int k = 0; k < Ctx::kChunks; k++) {
+    cudaEvent_t* evs[] = {&c->ev_h2d[k], &c->ev_conv_in[k], &c->ev_conv_out[k], &c->ev_d2h[k]};
+    for (cudaEvent_t* e : evs)
+      if (*e) cudaEventDestroy(*e);
+  }
+  if (c->d_in_stage) cudaFree(c->d_in_stage);
+  if (c->d_out_stage) cudaFree(c->d_out_stage);
+  if (c->s_in) cudaStreamDestroy(c->s_in);
+  if (c->s_out) cudaStreamDestroy(c->s_out);
   if (c->h_tabs) cudaFreeHost(c->h_tabs);
   if (c->h_velmax) cudaFreeHost(c->h_velmax);
   if (c->h_forc) cudaFreeHost(c->h_forc);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
+  return 0;
+}
+
+int psdns_gpu_set_state_async(void* ctx, const double* un, int32_t layout) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !un) return set_error("null argument");
+  if (layout != PSDNS_LAYOUT_YCYL) return set_error("asynchronous state copies use PSDNS_LAYOUT_YCYL");
+  if (async_setup(*c)) return 1;
+  const char* h = (const char*)un;
+  const size_t bytes = sizeof(double2) * c->st_elems;
+  const bool same = c->pend_out == h && c->pend_out_bytes == bytes;
+  const bool overlap = c->pend_out && h < c->pend_out + c->pend_out_bytes && c->pend_out < h + bytes;
+  double2* stage = (double2*)c->d_in_stage;
+  for (int k = 0; k < Ctx::kChunks; k++) {
+    size_t off, cnt;
+    chunk_range(*c, k, off, cnt);
+    if (!cnt) continue;
+    // the staging chunk is free once the previous upload's conversion read it
+    if (c->in_pending) CK(cudaStreamWaitEvent(c->s_in, c->ev_conv_in[k], 0));
+    if (same) {
+      CK(cudaStreamWaitEvent(c->s_in, c->ev_d2h[k], 0));
+    } else if (overlap) {
+      for (int j = 0; j < Ctx::kChunks; j++) CK(cudaStreamWaitEvent(c->s_in, c->ev_d2h[j], 0));
+    }
+    CK(cudaMemcpyAsync(stage + off, h + off * sizeof(double2), cnt * sizeof(double2), cudaMemcpyHostToDevice,
+                       c->s_in));
+    CK(cudaEventRecord(c->ev_h2d[k], c->s_in));
+    CK(cudaStreamWaitEvent(c->stream, c->ev_h2d[k], 0));
+    if (c->prec == PSDNS_PREC_FP64)
+      k_from_f64<double><<<148 * 4, 256, 0, c->stream>>>(stage + off, (double2*)c->d_un + off,
+                                                          (double2*)c->d_u + off, cnt);
+    else
+      k_from_f64<float><<<148 * 4, 256, 0, c->stream>>>(stage + off, (float2*)c->d_un + off, (float2*)c->d_u + off,
+                                                         cnt);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev_conv_in[k], c->stream));
+  }
+  c->in_pending = true;
+  return 0;
+}
+
+int psdns_gpu_get_state_async(void* ctx, double* out, int32_t which, int32_t layout) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !out) return set_error("null argument");
+  if (layout != PSDNS_LAYOUT_YCYL) return set_error("asynchronous state copies use PSDNS_LAYOUT_YCYL");
+  if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
+  if (async_setup(*c)) return 1;
+  const void* src = which == PSDNS_FIELD_U ? c->d_u : c->d_un;
+  double2* stage = (double2*)c->d_out_stage;
+  const bool had = c->pend_out != nullptr;
+  for (int k = 0; k < Ctx::kChunks; k++) {
+    size_t off, cnt;
+    chunk_range(*c, k, off, cnt);
+    if (!cnt) continue;
+    // the staging chunk is free once the previous download of it finished
+    if (had) CK(cudaStreamWaitEvent(c->stream, c->ev_d2h[k], 0));
+    if (c->prec == PSDNS_PREC_FP64)
+      k_to_f64<double><<<148 * 4, 256, 0, c->stream>>>((const double2*)src + off, stage + off, cnt);
+    else
+      k_to_f64<float><<<148 * 4, 256, 0, c->stream>>>((const float2*)src + off, stage + off, cnt);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev_conv_out[k], c->stream));
+    CK(cudaStreamWaitEvent(c->s_out, c->ev_conv_out[k], 0));
+    CK(cudaMemcpyAsync((char*)out + off * sizeof(double2), stage + off, cnt * sizeof(double2),
+                       cudaMemcpyDeviceToHost, c->s_out));
+    CK(cudaEventRecord(c->ev_d2h[k], c->s_out));
+  }
+  c->pend_out = (const char*)out;
+  c->pend_out_bytes = sizeof(double2) * c->st_elems;
+  return 0;
+}
+
+int psdns_gpu_sync(void* ctx) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return set_error("null context");
+  if (c->s_in) {
+    CK(cudaStreamSynchronize(c->s_in));
+    CK(cudaStreamSynchronize(c->s_out));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  c->pend_out = nullptr;
+  c->pend_out_bytes = 0;
+  c->in_pending = false;
   return 0;
 }
 

@@ -79,6 +79,23 @@ module psdns_gpu_mod
       type(c_ptr), value :: ctx
       real(c_double), intent(out) :: pos(*), vel(*)
     end function
+    integer(c_int) function psdns_gpu_set_state_async(ctx, un, layout) bind(c, name='psdns_gpu_set_state_async')
+      import :: c_int, c_ptr, c_int32_t
+      type(c_ptr), value :: ctx
+      type(c_ptr), value :: un        ! c_loc of a pinned (page-locked) array
+      integer(c_int32_t), value :: layout
+    end function
+    integer(c_int) function psdns_gpu_get_state_async(ctx, out, which, layout) &
+        bind(c, name='psdns_gpu_get_state_async')
+      import :: c_int, c_ptr, c_int32_t
+      type(c_ptr), value :: ctx
+      type(c_ptr), value :: out
+      integer(c_int32_t), value :: which, layout
+    end function
+    integer(c_int) function psdns_gpu_sync(ctx) bind(c, name='psdns_gpu_sync')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
     ! ensembles of independent boxes (params(count): one psdns_params per box)
     integer(c_int) function psdns_gpu_ensemble_create(params, count, ens) bind(c, name='psdns_gpu_ensemble_create')
       import :: c_int, c_ptr, c_int32_t, psdns_params

@@ -27,6 +27,9 @@ FIELD_UN = 1
 
 # every entry point declared in include/psdns_gpu.h
 EXPORTS = (
+    "psdns_gpu_set_state_async",
+    "psdns_gpu_get_state_async",
+    "psdns_gpu_sync",
     "psdns_gpu_ensemble_create",
     "psdns_gpu_ensemble_destroy",
     "psdns_gpu_ensemble_field_init",
@@ -110,6 +113,9 @@ def load():
     L.psdns_gpu_spectra.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
+    L.psdns_gpu_set_state_async.argtypes = [vp, dp, ctypes.c_int32]
+    L.psdns_gpu_get_state_async.argtypes = [vp, dp, ctypes.c_int32, ctypes.c_int32]
+    L.psdns_gpu_sync.argtypes = [vp]
     L.psdns_gpu_ensemble_create.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]
     L.psdns_gpu_ensemble_destroy.argtypes = [vp]
     L.psdns_gpu_ensemble_field_init.argtypes = [vp, ip]
@@ -232,6 +238,19 @@ class Solver:
         _check(load().psdns_gpu_get_state(self._ctx, _dp(out.view(np.float64)), which, layout),
                "get_state")
         return out
+
+    def set_state_async_ptr(self, ptr):
+        """Upload from a pinned host pointer on the copy stream (returns at once)."""
+        _check(load().psdns_gpu_set_state_async(self._ctx, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)),
+                                                LAYOUT_YCYL), "set_state_async")
+
+    def get_state_async_ptr(self, ptr, which=FIELD_UN):
+        """Download into a pinned host pointer on the copy stream (returns at once)."""
+        _check(load().psdns_gpu_get_state_async(self._ctx, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)),
+                                                which, LAYOUT_YCYL), "get_state_async")
+
+    def sync(self):
+        _check(load().psdns_gpu_sync(self._ctx), "sync")
 
     def get_state_ptr(self, ptr, which=FIELD_UN):
         _check(load().psdns_gpu_get_state(self._ctx, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)),

@@ -243,3 +243,34 @@ def test_full_layout_round_trip(oracle_mod, gpu_mod, prec):
     np.testing.assert_allclose(s2.get_state(gpu_mod.FIELD_UN), s.get_state(gpu_mod.FIELD_UN), rtol=0, atol=0)
     s.close()
     s2.close()
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_async_state_copies_match_sync(oracle_mod, gpu_mod, prec):
+    """set_state_async / step / get_state_async into the same pinned host
+    buffer, three times, then sync: equal to the synchronous calls."""
+    import torch
+    n = 32
+    o = oracle_mod.Oracle(n, 0.01)
+    un0 = o.field_init(21)
+    o.close()
+    a = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=1.0)
+    b = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=1.0)
+    nbytes = un0.size * 16
+    host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    view = host.numpy().view(np.complex128).reshape(un0.shape)
+    view[...] = un0
+    for _ in range(3):
+        a.set_state_async_ptr(host.data_ptr())
+        a.step()
+        a.get_state_async_ptr(host.data_ptr())
+    a.sync()
+    b.set_state(un0)
+    cur = un0
+    for _ in range(3):
+        b.set_state(cur)
+        b.step()
+        cur = b.get_state()
+    np.testing.assert_array_equal(view, cur)
+    a.close()
+    b.close()
