@@ -226,6 +226,13 @@ int psdns_gpu_ensemble_step(void *ens, int32_t nsteps, double *info);
 int psdns_gpu_ensemble_spectra(void *ens, int32_t box, int32_t which, double *ek, double *dk, double *eijk,
                                double *stats);
 
+/* Moments of the velocity gradients (replaces PSDNS/vgmomt.f, called from
+ * itransform.f:385 on I/O steps): out[0..7] = <(du/dx)^m>, m = 1..8, and
+ * out[8..15] = <(dw/dz)^m> of u or un, averaged over the n^3 points of the
+ * grid shifted by gsh[3] in grid units (the stage-1 shifts gsh(:,1) of the
+ * step, as in the reference; null = unshifted).  FP64 sums. */
+int psdns_gpu_gradient_moments(void *ctx, int32_t which, const double *gsh, double *out);
+
 /* Message of the last error on this thread ("" if none). */
 int psdns_gpu_last_error(char *buf, int32_t len);
 

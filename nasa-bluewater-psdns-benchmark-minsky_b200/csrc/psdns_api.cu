@@ -252,6 +252,10 @@ static StageTables<T> make_tables(const Ctx& c, int ks) {
   return st;
 }
 
+template <typename T>
+static void fill_shift_tables(Ctx& c);
+static int upload_tables(Ctx& c);
+
 // ---------------------------------------------------------------------------
 // per-(precision, n, nc) kernel launch sequence
 // ---------------------------------------------------------------------------
@@ -273,6 +277,9 @@ template <typename T, int N, int NC> struct Impl {
     CK(cudaFuncSetAttribute(k_zfwd<T, N, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm4()));
     CK(cudaFuncSetAttribute(k_yfwd<T, N, 1, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
     CK(cudaFuncSetAttribute(k_yfwd<T, N, 2, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
+    CK(cudaFuncSetAttribute(k_zinv<T, N, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2()));
+    CK(cudaFuncSetAttribute(k_xmoments<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)KMomLaunch<T, N>::SMEM));
     // the particle path transforms the velocity only (NC = 0 instances)
     CK(cudaFuncSetAttribute(k_zinv<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2()));
     CK(cudaFuncSetAttribute(k_yinv<T, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1()));
@@ -310,6 +317,40 @@ template <typename T, int N, int NC> struct Impl {
     CK(cudaGetLastError());
     c.part_first = false;
     return 0;
+  }
+
+  // vgmomt.f: moments 1..8 of du/dx and dw/dz of u or un on the grid
+  // shifted by gsh (written as the stage-1 shifts for the duration)
+  static int moments(Ctx& c, int which, const double* gsh, double* out) {
+    double save[3][2];
+    std::memcpy(save, c.gsh, sizeof save);
+    for (int i = 0; i < 3; i++) c.gsh[i][0] = gsh ? gsh[i] : 0.0;
+    fill_shift_tables<T>(c);
+    int rc = upload_tables(c);
+    std::memcpy(c.gsh, save, sizeof save);
+    if (rc) return 1;
+    Geo g = make_geo(c);
+    StageTables<T> st = make_tables<T>(c, 0);
+    const C* tw = (const C*)c.d_tw;
+    C* ub = (C*)c.d_ub;
+    C* uz = (C*)c.d_uz;
+    const int kxn = c.g.kxn;
+    k_yinv<T, N><<<dim3(c.nab_i, 3), K1Launch<T, N>::THREADS, sm1(), c.stream>>>(
+        g, st, (const C*)(which == PSDNS_FIELD_U ? c.d_u : c.d_un), ub, tw);
+    k_zinv<T, N, 0, true><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 2), Launch<T, N, TL::XT2>::THREADS, sm2(),
+                           c.stream>>>(g, ub, uz, tw, st.b11, st.b33);
+    // the transposed copy in ub is consumed: its space holds the partial sums
+    double* partial = (double*)c.d_ub;
+    double* d_out = partial + (size_t)c.nzt * N * 16;
+    k_xmoments<T, N><<<dim3(c.nzt, N), KMomLaunch<T, N>::THREADS, KMomLaunch<T, N>::SMEM, c.stream>>>(g, uz, tw,
+                                                                                                    partial);
+    k_moments_reduce<<<16, 256, 0, c.stream>>>(partial, (long long)c.nzt * N, 1.0 / ((double)N * N * N), d_out);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, d_out, 16 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    // the next step refills its tables from c.gsh; restore the uploaded ones too
+    fill_shift_tables<T>(c);
+    return upload_tables(c);
   }
 
   static int twiddles(Ctx& c) {
@@ -388,11 +429,12 @@ struct Ops {
   int (*stage_a)(Ctx&, int);
   int (*stage_b)(Ctx&, int);
   int (*particles)(Ctx&);
+  int (*moments)(Ctx&, int, const double*, double*);
 };
 
 template <typename T, int N, int NC> static Ops ops_for() {
   using I = Impl<T, N, NC>;
-  return Ops{&I::setup, &I::twiddles, &I::stage_a, &I::stage_b, &I::particles};
+  return Ops{&I::setup, &I::twiddles, &I::stage_a, &I::stage_b, &I::particles, &I::moments};
 }
 
 template <int N> static Ops ops_n(int prec, int nc) {
@@ -1187,6 +1229,15 @@ int psdns_gpu_spectra(void* ctx, int32_t which, double* ek, double* dk, double* 
   // the ub work array is free between steps: use it for the sums
   return spectra_of(make_geo(*c), which == PSDNS_FIELD_U ? c->d_u : c->d_un, c->prec, c->p, c->stream, c->d_ub, ek,
                     dk, eijk, stats);
+}
+
+int psdns_gpu_gradient_moments(void* ctx, int32_t which, const double* gsh, double* out) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !out) return set_error("null argument");
+  if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
+  Ops o;
+  if (!get_ops(c->prec, c->n, c->nc, o)) return set_error("bad context");
+  return o.moments(*c, which, gsh, out);
 }
 
 int psdns_gpu_forcing_stats(void* ctx, double* efk, double* eirate, double* erate) {

@@ -268,10 +268,12 @@ __host__ __device__ __forceinline__ int k1_blocks(int nab_i) { return nab_i; }
 // K2: cylinder unpack (zero fill) + z backward FFT, store to uz
 // grid (n, ceil(kxn/XT2), 3)
 // ---------------------------------------------------------------------------
-template <typename T, int N, int NC = 0>
+template <typename T, int N, int NC = 0, bool GRAD = false>
 __global__ void __launch_bounds__(Launch<T, N, Tiles<T>::XT2>::THREADS, 3)
 k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11 = T(1),
        T b33 = T(1)) {
+  // GRAD (grid.z = 2): uz slot 0 = i b11 kx u, slot 1 = i b33 kz w, the
+  // gradients whose moments vgmomt.f takes (itransform.f:222-230)
   // NC = 1 (grid.z = 6): uz slot 3 = y gradient of the scalar (ub 4), slot
   // 4 = i b11 kx theta and slot 5 = i b33 kz theta (both from ub 3),
   // itransform.f:188-198
@@ -284,13 +286,13 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
   C* buf = tw + FFTPlan<T, N>::TWSIZE;
   load_twiddles<T, N>(tw, tw_g);
   // grid (n, ceil(kxn / XT2), (3 + 3 nc) * boxes)
-  constexpr int NVZ = 3 + 3 * NC;
+  constexpr int NVZ = GRAD ? 2 : 3 + 3 * NC;
   const int y = blockIdx.x, x0 = blockIdx.y * XT, v = blockIdx.z % NVZ, box = blockIdx.z / NVZ;
   ub += box * g.bbox;
   uz += box * g.zbox;
   const int x1 = min(x0 + XT, g.kxn);
   const int nl = x1 - x0;
-  const int sv = v < 3 ? v : (v == 3 ? 4 : 3);
+  const int sv = GRAD ? (v == 0 ? 0 : 2) : (v < 3 ? v : (v == 3 ? 4 : 3));
   constexpr int TBL = Tiles<T>::TBL_I;
   const C* src = ub + (size_t)sv * ubi_var_elems<T>(g.nab_i, N);
   // slot (l, z): column x0 + l holds kz = 0..kc then -kc..-1 (count 2 kc + 1,
@@ -319,7 +321,10 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
     if (z <= kc || z >= N - kc) {
       C* p = buf + l * L + pad32(z);
       C val = *p;
-      if constexpr (NC > 0) {
+      if constexpr (GRAD) {
+        const T bk = v == 0 ? b11 * T(x0 + l) : b33 * T(kwave<N>(z));
+        val = cmk<C>(-bk * val.y, bk * val.x);
+      } else if constexpr (NC > 0) {
         if (v >= 4) {
           const T bk = v == 4 ? b11 * T(x0 + l) : b33 * T(kwave<N>(z));
           val = cmk<C>(-bk * val.y, bk * val.x);
@@ -885,6 +890,92 @@ k_xspline(Geo g, const C2<T>* __restrict__ uz, typename V4T<T>::type* __restrict
     c.w = 0;
     bs[((size_t)y * N + zt * TZ + zz) * N + x] = c;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Velocity-gradient moments (vgmomt.f:50-143): x inverse of the two gradient
+// fields of uz slots 0 and 1, then the sums of g^m, m = 1..8, in FP64; each
+// block writes its 16 partial sums, k_moments_reduce adds them in a fixed
+// order.  grid (nzt, n).
+// ---------------------------------------------------------------------------
+template <typename T, int N>
+struct KMomLaunch : Launch<T, N, 2 * (Tiles<T>::TZ / 2)> {
+  static constexpr size_t SMEM =
+      sizeof(C2<T>) * (FFTPlan<T, N>::TWSIZE + (size_t)2 * (Tiles<T>::TZ / 2) * LS<N>::value);
+};
+
+template <typename T, int N>
+__global__ void __launch_bounds__(KMomLaunch<T, N>::THREADS)
+k_xmoments(Geo g, const C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, double* __restrict__ partial) {
+  using C = C2<T>;
+  constexpr int TZ = Tiles<T>::TZ, NPAIR = TZ / 2;
+  constexpr int THREADS = KMomLaunch<T, N>::THREADS;
+  static_assert(THREADS % 32 == 0, "the reduction uses whole warps");
+  constexpr int L = LS<N>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* bufU = tw + FFTPlan<T, N>::TWSIZE;
+  __shared__ double red[THREADS / 32 + 1][16];
+  load_twiddles<T, N>(tw, tw_g);
+  const int zt = blockIdx.x, y = blockIdx.y, kxn = g.kxn;
+  for (int e = threadIdx.x; e < 2 * NPAIR * N; e += THREADS) {
+    const int k = e % N;
+    if (k >= kxn && k <= N - kxn) bufU[(e / N) * L + pad32(k)] = cmk<C>(0, 0);
+  }
+  xchain_pack<T, N, 2, THREADS>(g, uz, 0, y, zt, bufU, L);
+  cp_async_wait_all();
+  __syncthreads();
+  fft_lines<T, N, THREADS>(bufU, 2 * NPAIR, L, tw);
+  // buffer = conj(a + i b): real line z = 2p is re, 2p+1 is -im
+  double s[16];
+#pragma unroll
+  for (int m = 0; m < 16; m++) s[m] = 0.0;
+  for (int e = threadIdx.x; e < TZ * N; e += THREADS) {
+    const int zz = e / N, x = e % N, p = zz / 2;
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      const C z = bufU[(f * NPAIR + p) * L + pad32(x)];
+      const double v = (zz & 1) ? -(double)z.y : (double)z.x, sq = v * v;
+      s[8 * f + 0] += v;
+      s[8 * f + 1] += sq;
+      s[8 * f + 2] += sq * v;
+      s[8 * f + 3] += sq * sq;
+      s[8 * f + 4] += sq * sq * v;
+      s[8 * f + 5] += sq * sq * sq;
+      s[8 * f + 6] += sq * sq * sq * v;
+      s[8 * f + 7] += sq * sq * sq * sq;
+    }
+  }
+  // fixed-order block reduction: warps by shuffles, then warp sums in order
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int m = 0; m < 16; m++) {
+    double v = s[m];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[wid][m] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 16) {
+    double v = 0.0;
+    for (int w = 0; w < THREADS / 32; w++) v += red[w][threadIdx.x];
+    partial[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 16 + threadIdx.x] = v;
+  }
+}
+
+// out[m] = (sum over blocks of partial[.][m]) * scale, one block per m
+static __global__ void __launch_bounds__(256) k_moments_reduce(const double* __restrict__ partial, long long nblocks,
+                                                        double scale, double* __restrict__ out) {
+  __shared__ double red[256];
+  const int m = blockIdx.x;
+  double v = 0.0;
+  for (long long b = threadIdx.x; b < nblocks; b += 256) v += partial[b * 16 + m];
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[m] = red[0] * scale;
 }
 
 // ---------------------------------------------------------------------------

@@ -96,6 +96,14 @@ module psdns_gpu_mod
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
     end function
+    integer(c_int) function psdns_gpu_gradient_moments(ctx, which, gsh, out) &
+        bind(c, name='psdns_gpu_gradient_moments')
+      import :: c_int, c_ptr, c_int32_t, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: which
+      real(c_double), intent(in) :: gsh(3)
+      real(c_double), intent(out) :: out(16)
+    end function
     ! ensembles of independent boxes (params(count): one psdns_params per box)
     integer(c_int) function psdns_gpu_ensemble_create(params, count, ens) bind(c, name='psdns_gpu_ensemble_create')
       import :: c_int, c_ptr, c_int32_t, psdns_params

@@ -27,6 +27,7 @@ FIELD_UN = 1
 
 # every entry point declared in include/psdns_gpu.h
 EXPORTS = (
+    "psdns_gpu_gradient_moments",
     "psdns_gpu_set_state_async",
     "psdns_gpu_get_state_async",
     "psdns_gpu_sync",
@@ -113,6 +114,7 @@ def load():
     L.psdns_gpu_spectra.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
+    L.psdns_gpu_gradient_moments.argtypes = [vp, ctypes.c_int32, dp, dp]
     L.psdns_gpu_set_state_async.argtypes = [vp, dp, ctypes.c_int32]
     L.psdns_gpu_get_state_async.argtypes = [vp, dp, ctypes.c_int32, ctypes.c_int32]
     L.psdns_gpu_sync.argtypes = [vp]
@@ -310,6 +312,13 @@ class Solver:
         ek = np.zeros(n); dk = np.zeros(n); e6 = np.zeros(n * 6); st = np.zeros(7)
         _check(load().psdns_gpu_spectra(self._ctx, int(which), _dp(ek), _dp(dk), _dp(e6), _dp(st)), "spectra")
         return ek, dk, e6.reshape(n, 6), dict(zip(["tke", "eps", "skew", "klen", "kvel", "ktime", "ekl"], st))
+
+    def gradient_moments(self, which=FIELD_UN, gsh=(0.0, 0.0, 0.0)):
+        """vgmomt.f: (moments 1..8 of du/dx, of dw/dz) on the grid shifted by gsh."""
+        g = np.ascontiguousarray(gsh, dtype=np.float64)
+        out = np.zeros(16, np.float64)
+        _check(load().psdns_gpu_gradient_moments(self._ctx, int(which), _dp(g), _dp(out)), "gradient_moments")
+        return out[:8].copy(), out[8:].copy()
 
     def forcing_table(self):
         """for(kfor,k2fo,k2fo,3) of the last step as an array [3][k2fo][k2fo][kfor]."""

@@ -58,6 +58,7 @@ def lib():
         L.orc_spectra.argtypes = [vp, ctypes.c_int, dp, dp, dp, dp]
         L.orc_particles_set.argtypes = [vp, ctypes.c_long, dp]
         L.orc_particles_get.argtypes = [vp, dp, dp]
+        L.orc_gradient_moments.argtypes = [vp, ctypes.c_int, dp, dp]
         L.orc_set_scalar.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_double]
         _LIB = L
@@ -196,6 +197,13 @@ class Oracle:
         x = np.zeros(n, np.float64)
         lib().orc_rann2(self._c, int(seq), _dp(x), int(n))
         return x
+
+    def gradient_moments(self, which=1, gsh=(0.0, 0.0, 0.0)):
+        """vgmomt.f: (moments 1..8 of du/dx, of dw/dz) on the grid shifted by gsh."""
+        g = np.ascontiguousarray(gsh, dtype=np.float64)
+        out = np.zeros(16, np.float64)
+        lib().orc_gradient_moments(self._c, int(which), _dp(g), _dp(out))
+        return out[:8].copy(), out[8:].copy()
 
     def itransform(self, ucyl, kstep=1):
         a = np.ascontiguousarray(ucyl, dtype=np.complex128)

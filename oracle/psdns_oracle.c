@@ -1280,6 +1280,42 @@ int orc_stage(orc_ctx *c, int kstep)
     return rk_stage(c, kstep);
 }
 
+/* vgmomt.f:50-143 (itransform.f:222-230, :385): moments of order 1..8 of
+ * du/dx and dw/dz on the grid shifted by gsh[3] (the stage-1 shifts of an I/O
+ * step), of u (which = 0) or un (which = 1), each sum divided by n^3.
+ * out[0..7] = du/dx, out[8..15] = dw/dz.  The derivative factors are applied
+ * in the z pencils as the reference does (itransform's nv = 6 path). */
+void orc_gradient_moments(orc_ctx *c, int which, const double *gsh, double *out)
+{
+    int n = c->n, tot = c->xz_tot;
+    size_t vs = (size_t)tot * n, np = (size_t)n * n * n;
+    double save[3][2];
+    memcpy(save, c->gsh, sizeof save);
+    double g6[6] = {gsh[0], 0., gsh[1], 0., gsh[2], 0.};
+    orc_set_shifts(c, g6);
+    const cx *src = which == 0 ? c->u : c->un;
+    cx *w = (cx *)calloc(6 * vs, sizeof(cx));
+    memcpy(w + 4 * vs, src, sizeof(cx) * vs);             /* u -> x gradient slot */
+    memcpy(w + 5 * vs, src + 2 * vs, sizeof(cx) * vs);    /* w -> z gradient slot */
+    phase_shift(c, w, 6, 0);
+    double *p = (double *)malloc(sizeof(double) * 6 * np);
+    itransform(c, w, 6, p);
+    for (int f = 0; f < 2; f++) {
+        const double *g = p + (size_t)(4 + f) * np;
+        double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (size_t i = 0; i < np; i++) {
+            double v = g[i], sq = v * v;
+            s[0] += v; s[1] += sq; s[2] += sq * v; s[3] += sq * sq;
+            s[4] += sq * sq * v; s[5] += sq * sq * sq; s[6] += sq * sq * sq * v; s[7] += sq * sq * sq * sq;
+        }
+        for (int m = 0; m < 8; m++) out[8 * f + m] = s[m] / (double)np;
+    }
+    free(p);
+    free(w);
+    double g6b[6] = {save[0][0], save[0][1], save[1][0], save[1][1], save[2][0], save[2][1]};
+    orc_set_shifts(c, g6b);
+}
+
 /* Piecewise hooks for tests: the inverse transform of u (3 vars) into
  * physical space p[3][y][z][x] (after the phase shift of stage kstep). */
 void orc_itransform_only(orc_ctx *c, int kstep, const double *ucyl, double *p)

@@ -274,3 +274,33 @@ def test_async_state_copies_match_sync(oracle_mod, gpu_mod, prec):
     np.testing.assert_array_equal(view, cur)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("prec,tol", [(1, 1e-10), (0, 1e-4)])
+def test_gradient_moments_match_oracle(oracle_mod, gpu_mod, prec, tol):
+    """vgmomt.f moments of du/dx and dw/dz, shifted grid, after two steps."""
+    n = 32
+    o = oracle_mod.Oracle(n, 0.01, cfl=1.0, kshift=1)
+    un0 = o.field_init(8)
+    o.set_state(un0)
+    s = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=1.0, kshift=1)
+    s.set_state(un0)
+    for _ in range(2):
+        o.step()
+        s.step()
+    gsh = (0.3, 0.71, 0.05)
+    for which in (gpu_mod.FIELD_U, gpu_mod.FIELD_UN):
+        mo = o.gradient_moments(which, gsh)
+        mg = s.gradient_moments(which, gsh)
+        for f in range(2):
+            # even moments relative; odd ones against the scale of the even ones
+            for m in range(8):
+                scale = mo[f][m] if m % 2 == 1 else mo[f][1] ** ((m + 1) / 2)
+                assert abs(mg[f][m] - mo[f][m]) <= tol * abs(scale), (which, f, m, mg[f][m], mo[f][m])
+    # the diagnostic leaves the run untouched
+    o.step()
+    s.step()
+    _, un_o = o.get_state()
+    assert rel_l2(s.get_state(gpu_mod.FIELD_UN), un_o) < (1e-11 if prec == 1 else 2e-5)
+    o.close()
+    s.close()

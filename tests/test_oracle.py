@@ -245,3 +245,27 @@ def test_particle_heun_step_in_uniform_flow(oracle_mod):
     assert np.all(np.abs(p1[:, 1] - pos[:, 1]) > 0)
     np.testing.assert_allclose(p1[:, 0], pos[:, 0], atol=1e-14)
     o.close()
+
+
+def test_gradient_moments_of_a_single_mode(oracle_mod):
+    """u = A sin(2x) (a kx = 2 mode of u, varying along x is not solenoidal,
+    but vgmomt only transforms): du/dx = 2A cos(2x), whose grid averages
+    equal the continuous ones while 2 * 8 < n: <g^2> = g^2/2, <g^4> = 3g^4/8,
+    <g^6> = 5g^6/16, <g^8> = 35g^8/128 (g = 2A), odd moments 0; dw/dz = 0."""
+    n = 32
+    o = oracle_mod.Oracle(n, 0.01)
+    un = np.zeros(o.state_shape(), complex)
+    geo = o.geometry()
+    a = geo["colstart"][2]          # column (kx, kz) = (2, 0)
+    A = 0.3
+    un[0, a, 0] = -0.5j * A         # A sin(2x) = A (e^{2ix} - e^{-2ix}) / 2i; kx > 0 half stored
+    o.set_state(un)
+    mu, mw = o.gradient_moments(1, (0.0, 0.0, 0.0))
+    g = 2 * A
+    np.testing.assert_allclose(mu[[0, 2, 4, 6]], 0, atol=1e-13)
+    np.testing.assert_allclose(mu[1], g ** 2 / 2, rtol=1e-11)
+    np.testing.assert_allclose(mu[3], 3 * g ** 4 / 8, rtol=1e-11)
+    np.testing.assert_allclose(mu[5], 5 * g ** 6 / 16, rtol=1e-11)
+    np.testing.assert_allclose(mu[7], 35 * g ** 8 / 128, rtol=1e-11)
+    assert np.abs(mw).max() < 1e-28
+    o.close()
