@@ -214,8 +214,20 @@ __host__ __device__ constexpr int plan_e(int N, bool dbl) {
 __host__ __device__ constexpr int plan_ns(int N, bool dbl, int p) {
   int s = 1; for (int i = 0; i < p; i++) s *= plan_rad(N, dbl, i); return s;
 }
+// Passes p >= 1 of radix >= 16 (a multiple of 8) keep factored twiddles:
+// W^(r k) = W^(8 (r/8) k) * W^((r%8) k), rows [0..7] of W^(r0 k) then rows
+// [8 .. 8 + R/8 - 1] of W^(8 r1 k), so a thread loads 8 + R/8 twiddles
+// instead of R (radix 32: 12 instead of 32) and forms the rest with one
+// complex product each.
+__host__ __device__ constexpr bool plan_fact(int N, bool dbl, int p) {
+  return p >= 1 && plan_rad(N, dbl, p) >= 16 && plan_rad(N, dbl, p) % 8 == 0;
+}
+__host__ __device__ constexpr int plan_twsz(int N, bool dbl, int p) {
+  return plan_fact(N, dbl, p) ? (8 + plan_rad(N, dbl, p) / 8) * plan_ns(N, dbl, p)
+                              : plan_rad(N, dbl, p) * plan_ns(N, dbl, p);
+}
 __host__ __device__ constexpr int plan_twoff(int N, bool dbl, int p) {
-  int o = 0; for (int i = 1; i < p; i++) o += plan_rad(N, dbl, i) * plan_ns(N, dbl, i); return o;
+  int o = 0; for (int i = 1; i < p; i++) o += plan_twsz(N, dbl, i); return o;
 }
 
 template <typename T, int N> struct FFTPlan {
@@ -229,6 +241,7 @@ template <typename T, int N> struct FFTPlan {
   static_assert(P * E == N, "operands per thread must divide the line");
   static constexpr int ns(int p) { return plan_ns(N, DBL, p); }
   static constexpr int twoff(int p) { return plan_twoff(N, DBL, p); }
+  static constexpr bool fact(int p) { return plan_fact(N, DBL, p); }
   static constexpr int TWSIZE = plan_twoff(N, DBL, plan_npass(N, DBL)) > 0 ? plan_twoff(N, DBL, plan_npass(N, DBL)) : 1;
 };
 
@@ -248,7 +261,7 @@ __device__ __forceinline__ void line_sync() {
 }
 
 // One Stockham pass over nlines lines (rounds of LPR lines).
-template <typename C, int N, int R, int NS, int E, int P, int THREADS>
+template <typename C, int N, int R, int NS, int E, int P, int THREADS, bool FACT>
 __device__ __forceinline__ void fft_pass(C* buf, int nlines, int ls, const C* __restrict__ twp) {
   constexpr int LPR = THREADS / P;
   constexpr int NB = E / R;   // butterflies per thread
@@ -267,7 +280,20 @@ __device__ __forceinline__ void fft_pass(C* buf, int nlines, int ls, const C* __
         const int k = j % NS;
 #pragma unroll
         for (int r = 0; r < R; r++) v[q * R + r] = line[pad32(j + r * (N / R))];
-        if constexpr (NS > 1) {
+        if constexpr (FACT) {
+          C t0[8];
+#pragma unroll
+          for (int r0 = 1; r0 < 8; r0++) t0[r0] = twp[r0 * NS + k];
+#pragma unroll
+          for (int r0 = 1; r0 < 8; r0++) v[q * R + r0] = cmul(v[q * R + r0], t0[r0]);
+#pragma unroll
+          for (int r1 = 1; r1 < R / 8; r1++) {
+            const C t1 = twp[(8 + r1) * NS + k];
+            v[q * R + 8 * r1] = cmul(v[q * R + 8 * r1], t1);
+#pragma unroll
+            for (int r0 = 1; r0 < 8; r0++) v[q * R + 8 * r1 + r0] = cmul(v[q * R + 8 * r1 + r0], cmul(t1, t0[r0]));
+          }
+        } else if constexpr (NS > 1) {
 #pragma unroll
           for (int r = 1; r < R; r++) v[q * R + r] = cmul(v[q * R + r], twp[r * NS + k]);
         }
@@ -295,7 +321,7 @@ __device__ __forceinline__ void fft_passes(C2<T>* buf, int nlines, int ls, const
   if constexpr (PASS < PL::NPASS) {
     constexpr int R = PL::rad(PASS);
     constexpr int NS = PL::ns(PASS);
-    fft_pass<C2<T>, N, R, NS, PL::E, PL::P, THREADS>(buf, nlines, ls, tw + PL::twoff(PASS));
+    fft_pass<C2<T>, N, R, NS, PL::E, PL::P, THREADS, PL::fact(PASS)>(buf, nlines, ls, tw + PL::twoff(PASS));
     fft_passes<T, N, THREADS, PASS + 1>(buf, nlines, ls, tw);
   }
 }
@@ -312,20 +338,29 @@ __device__ __forceinline__ void fft_lines(C2<T>* buf, int nlines, int ls, const 
 }
 
 // Host: build the twiddle table of FFTPlan<T,N> (pass p >= 1 table is
-// [r][k] = W_N^(r k N/(Ns R)), r < R, k < Ns).
+// [r][k] = W_N^(r k N/(Ns R)), r < R, k < Ns; factored passes hold the rows
+// r0 = 0..7 and 8 r1, r1 = 0..R/8-1, see plan_fact).
 template <typename T, int N>
 void build_twiddles(C2<T>* out) {
   using PL = FFTPlan<T, N>;
+  auto w = [](long m) {
+    // accurate angle: reduce m/N to [0,1) exactly in integers
+    m %= N;
+    long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)N;
+    return cmk<C2<T>>((T)cosl(ang), (T)sinl(ang));
+  };
   for (int p = 1; p < PL::NPASS; p++) {
     const int R = PL::rad(p), NS = PL::ns(p), off = PL::twoff(p);
-    for (int r = 0; r < R; r++)
+    const long s = N / (NS * R);
+    if (PL::fact(p)) {
       for (int k = 0; k < NS; k++) {
-        long m = (long)r * k * (N / (NS * R));
-        // accurate angle: reduce m/N to [0,1) exactly in integers
-        m %= N;
-        long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)N;
-        out[off + r * NS + k] = cmk<C2<T>>((T)cosl(ang), (T)sinl(ang));
+        for (int r0 = 0; r0 < 8; r0++) out[off + r0 * NS + k] = w((long)r0 * k * s);
+        for (int r1 = 0; r1 < R / 8; r1++) out[off + (8 + r1) * NS + k] = w((long)8 * r1 * k * s);
       }
+    } else {
+      for (int r = 0; r < R; r++)
+        for (int k = 0; k < NS; k++) out[off + r * NS + k] = w((long)r * k * s);
+    }
   }
 }
 
