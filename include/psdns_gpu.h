@@ -226,6 +226,15 @@ int psdns_gpu_ensemble_step(void *ens, int32_t nsteps, double *info);
 int psdns_gpu_ensemble_spectra(void *ens, int32_t box, int32_t which, double *ek, double *dk, double *eijk,
                                double *stats);
 
+/* Checkpoints in the reference's own file format: one task's pencil file
+ * as homogeneous/outpen_write_r.f writes it (big-endian unformatted
+ * records, real(8) pairs, kx = 0..nx/2-1, Nyquist y and z planes left out),
+ * e.g. outpen/0/outpenc.p0.  write: u or un of the context; read: sets un
+ * and u (modes outside the truncation cylinder are dropped).  path is a
+ * NUL-terminated file name. */
+int psdns_gpu_write_checkpoint(void *ctx, const char *path, int32_t which);
+int psdns_gpu_read_checkpoint(void *ctx, const char *path);
+
 /* Moments of the velocity gradients (replaces PSDNS/vgmomt.f, called from
  * itransform.f:385 on I/O steps): out[0..7] = <(du/dx)^m>, m = 1..8, and
  * out[8..15] = <(dw/dz)^m> of u or un, averaged over the n^3 points of the

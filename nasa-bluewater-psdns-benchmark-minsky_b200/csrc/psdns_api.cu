@@ -721,6 +721,41 @@ static void chunk_range(const Ctx& c, int k, size_t& off, size_t& cnt) {
   cnt = std::min(tot, off + per) - off;
 }
 
+// big-endian Fortran record helpers for the checkpoint files
+static void be32(std::vector<unsigned char>& b, uint32_t v) {
+  for (int s = 24; s >= 0; s -= 8) b.push_back((unsigned char)(v >> s));
+}
+static void be64(unsigned char* p, double d) {
+  uint64_t v;
+  std::memcpy(&v, &d, 8);
+  for (int i = 0; i < 8; i++) p[i] = (unsigned char)(v >> (56 - 8 * i));
+}
+static double rd_be64(const unsigned char* p) {
+  uint64_t v = 0;
+  for (int i = 0; i < 8; i++) v = (v << 8) | p[i];
+  double d;
+  std::memcpy(&d, &v, 8);
+  return d;
+}
+static uint32_t rd_be32(const unsigned char* p) {
+  return ((uint32_t)p[0] << 24) | ((uint32_t)p[1] << 16) | ((uint32_t)p[2] << 8) | p[3];
+}
+static bool write_record(FILE* f, const unsigned char* data, size_t bytes) {
+  std::vector<unsigned char> m;
+  be32(m, (uint32_t)bytes);
+  return fwrite(m.data(), 1, 4, f) == 4 && fwrite(data, 1, bytes, f) == bytes && fwrite(m.data(), 1, 4, f) == 4;
+}
+static bool read_record(FILE* f, std::vector<unsigned char>& out) {
+  unsigned char m[4];
+  if (fread(m, 1, 4, f) != 4) return false;
+  const uint32_t len = rd_be32(m);
+  out.resize(len);
+  if (fread(out.data(), 1, len, f) != len) return false;
+  unsigned char m2[4];
+  return fread(m2, 1, 4, f) == 4 && rd_be32(m2) == len;
+}
+
+
 }  // namespace psdns
 
 using namespace psdns;
@@ -991,6 +1026,104 @@ int psdns_gpu_sync(void* ctx) {
 }
 
 // host (complex double, YCYL) -> device state, through ub as staging
+// ---------------------------------------------------------------------------
+// Checkpoint files in the reference's single-task pencil format
+// (homogeneous/outpen_write_r.f, compiled with -fconvert=big-endian and
+// -fdefault-real-8, makefile:249-256): Fortran unformatted sequential
+// records with 4-byte big-endian length markers; per variable i = 1..3+nc
+// the records (i, nx, ny, nz), (xist, xisz, zjst, zjsz, 1, ny) as int32,
+// then for every z but the Nyquist plane two records of real(8) pairs
+// (re, im) with x fastest: rows y = 1..ny/2, then y = ny/2+2..ny.  One task
+// holds kx = 0..nx/2-1 (xisz = nx/2, mpisetup.f:179) and every z.
+// ---------------------------------------------------------------------------
+int psdns_gpu_write_checkpoint(void* ctx, const char* path, int32_t which) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !path) return set_error("null argument");
+  if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
+  const int n = c->n, nxh = n / 2 + 1, xisz = n / 2;
+  const size_t fs = (size_t)nxh * n * n;
+  std::vector<double> full(2 * fs * c->nv);
+  if (psdns_gpu_get_state(ctx, full.data(), which, PSDNS_LAYOUT_FULL)) return 1;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return set_error("cannot open %s for writing", path);
+  bool ok = true;
+  std::vector<unsigned char> rec;
+  std::vector<unsigned char> row((size_t)16 * xisz * (n / 2 - 1 + 1));
+  for (int v = 0; v < c->nv && ok; v++) {
+    rec.clear();
+    for (uint32_t x : {(uint32_t)(v + 1), (uint32_t)n, (uint32_t)n, (uint32_t)n}) be32(rec, x);
+    ok = ok && write_record(f, rec.data(), rec.size());
+    rec.clear();
+    for (uint32_t x : {1u, (uint32_t)xisz, 1u, (uint32_t)n, 1u, (uint32_t)n}) be32(rec, x);
+    ok = ok && write_record(f, rec.data(), rec.size());
+    const double* u = full.data() + 2 * fs * v;
+    for (int z = 0; z < n && ok; z++) {
+      if (z == n / 2) continue;   // nzhp
+      for (int half = 0; half < 2 && ok; half++) {
+        const int y0 = half == 0 ? 0 : n / 2 + 1, y1 = half == 0 ? n / 2 : n;
+        size_t o = 0;
+        for (int y = y0; y < y1; y++)
+          for (int x = 0; x < xisz; x++) {
+            const double* e = u + 2 * (((size_t)z * n + y) * nxh + x);
+            be64(&row[o], e[0]);
+            be64(&row[o + 8], e[1]);
+            o += 16;
+          }
+        ok = write_record(f, row.data(), o);
+      }
+    }
+  }
+  if (std::fclose(f) != 0) ok = false;
+  return ok ? 0 : set_error("write to %s failed", path);
+}
+
+int psdns_gpu_read_checkpoint(void* ctx, const char* path) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !path) return set_error("null argument");
+  const int n = c->n, nxh = n / 2 + 1, xisz = n / 2;
+  const size_t fs = (size_t)nxh * n * n;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return set_error("cannot open %s", path);
+  std::vector<double> full(2 * fs * c->nv, 0.0);
+  std::vector<unsigned char> rec;
+  int err = 0;
+  for (int v = 0; v < c->nv && !err; v++) {
+    if (!read_record(f, rec) || rec.size() != 16) { err = set_error("%s: bad header of variable %d", path, v + 1); break; }
+    if ((int)rd_be32(&rec[0]) != v + 1 || (int)rd_be32(&rec[4]) != n || (int)rd_be32(&rec[8]) != n ||
+        (int)rd_be32(&rec[12]) != n) {
+      err = set_error("%s: variable %d is not a %d^3 field", path, v + 1, n);
+      break;
+    }
+    if (!read_record(f, rec) || rec.size() != 24 || rd_be32(&rec[0]) != 1 || (int)rd_be32(&rec[4]) != xisz ||
+        rd_be32(&rec[8]) != 1 || (int)rd_be32(&rec[12]) != n) {
+      err = set_error("%s: not a single-task pencil (xist 1, xisz %d, zjst 1, zjsz %d)", path, xisz, n);
+      break;
+    }
+    double* u = full.data() + 2 * fs * v;
+    for (int z = 0; z < n && !err; z++) {
+      if (z == n / 2) continue;
+      for (int half = 0; half < 2; half++) {
+        const int y0 = half == 0 ? 0 : n / 2 + 1, y1 = half == 0 ? n / 2 : n;
+        if (!read_record(f, rec) || rec.size() != (size_t)16 * xisz * (y1 - y0)) {
+          err = set_error("%s: short record at z = %d", path, z + 1);
+          break;
+        }
+        size_t o = 0;
+        for (int y = y0; y < y1; y++)
+          for (int x = 0; x < xisz; x++) {
+            double* e = u + 2 * (((size_t)z * n + y) * nxh + x);
+            e[0] = rd_be64(&rec[o]);
+            e[1] = rd_be64(&rec[o + 8]);
+            o += 16;
+          }
+      }
+    }
+  }
+  std::fclose(f);
+  if (err) return err;
+  return psdns_gpu_set_state(ctx, full.data(), PSDNS_LAYOUT_FULL);
+}
+
 int psdns_gpu_set_state(void* ctx, const double* un, int32_t layout) {
   Ctx* c = (Ctx*)ctx;
   if (!c || !un) return set_error("null argument");

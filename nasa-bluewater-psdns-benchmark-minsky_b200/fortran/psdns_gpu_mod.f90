@@ -96,6 +96,17 @@ module psdns_gpu_mod
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
     end function
+    integer(c_int) function psdns_gpu_write_checkpoint(ctx, path, which) bind(c, name='psdns_gpu_write_checkpoint')
+      import :: c_int, c_ptr, c_int32_t, c_char
+      type(c_ptr), value :: ctx
+      character(kind=c_char), intent(in) :: path(*)   ! terminated by c_null_char
+      integer(c_int32_t), value :: which
+    end function
+    integer(c_int) function psdns_gpu_read_checkpoint(ctx, path) bind(c, name='psdns_gpu_read_checkpoint')
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: ctx
+      character(kind=c_char), intent(in) :: path(*)
+    end function
     integer(c_int) function psdns_gpu_gradient_moments(ctx, which, gsh, out) &
         bind(c, name='psdns_gpu_gradient_moments')
       import :: c_int, c_ptr, c_int32_t, c_double

@@ -27,6 +27,8 @@ FIELD_UN = 1
 
 # every entry point declared in include/psdns_gpu.h
 EXPORTS = (
+    "psdns_gpu_write_checkpoint",
+    "psdns_gpu_read_checkpoint",
     "psdns_gpu_gradient_moments",
     "psdns_gpu_set_state_async",
     "psdns_gpu_get_state_async",
@@ -114,6 +116,8 @@ def load():
     L.psdns_gpu_spectra.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
+    L.psdns_gpu_write_checkpoint.argtypes = [vp, ctypes.c_char_p, ctypes.c_int32]
+    L.psdns_gpu_read_checkpoint.argtypes = [vp, ctypes.c_char_p]
     L.psdns_gpu_gradient_moments.argtypes = [vp, ctypes.c_int32, dp, dp]
     L.psdns_gpu_set_state_async.argtypes = [vp, dp, ctypes.c_int32]
     L.psdns_gpu_get_state_async.argtypes = [vp, dp, ctypes.c_int32, ctypes.c_int32]
@@ -312,6 +316,13 @@ class Solver:
         ek = np.zeros(n); dk = np.zeros(n); e6 = np.zeros(n * 6); st = np.zeros(7)
         _check(load().psdns_gpu_spectra(self._ctx, int(which), _dp(ek), _dp(dk), _dp(e6), _dp(st)), "spectra")
         return ek, dk, e6.reshape(n, 6), dict(zip(["tke", "eps", "skew", "klen", "kvel", "ktime", "ekl"], st))
+
+    def write_checkpoint(self, path, which=FIELD_UN):
+        """One-task pencil file in the reference's format (outpen_write_r.f)."""
+        _check(load().psdns_gpu_write_checkpoint(self._ctx, os.fsencode(path), int(which)), "write_checkpoint")
+
+    def read_checkpoint(self, path):
+        _check(load().psdns_gpu_read_checkpoint(self._ctx, os.fsencode(path)), "read_checkpoint")
 
     def gradient_moments(self, which=FIELD_UN, gsh=(0.0, 0.0, 0.0)):
         """vgmomt.f: (moments 1..8 of du/dx, of dw/dz) on the grid shifted by gsh."""

@@ -304,3 +304,62 @@ def test_gradient_moments_match_oracle(oracle_mod, gpu_mod, prec, tol):
     assert rel_l2(s.get_state(gpu_mod.FIELD_UN), un_o) < (1e-11 if prec == 1 else 2e-5)
     o.close()
     s.close()
+
+
+def _read_pencil_file(path, n, nv):
+    """Independent reader of the single-task outpen_write_r.f layout:
+    big-endian records with 4-byte markers; per variable (i,nx,ny,nz),
+    (xist,xisz,zjst,zjsz,1,ny), then two records per z (not Nyquist)."""
+    import struct
+    raw = open(path, "rb").read()
+    pos = 0
+    recs = []
+    while pos < len(raw):
+        (ln,) = struct.unpack(">i", raw[pos:pos + 4])
+        recs.append(raw[pos + 4:pos + 4 + ln])
+        (ln2,) = struct.unpack(">i", raw[pos + 4 + ln:pos + 8 + ln])
+        assert ln2 == ln
+        pos += 8 + ln
+    out = np.zeros((nv, n, n, n // 2), complex)    # [v][z][y][kx < n/2]
+    r = 0
+    for v in range(nv):
+        assert struct.unpack(">4i", recs[r]) == (v + 1, n, n, n)
+        assert struct.unpack(">6i", recs[r + 1]) == (1, n // 2, 1, n, 1, n)
+        r += 2
+        for z in range(n):
+            if z == n // 2:
+                continue
+            for ys in (range(0, n // 2), range(n // 2 + 1, n)):
+                a = np.frombuffer(recs[r], dtype=">f8").reshape(len(ys), n // 2, 2)
+                out[v, z, ys.start:ys.stop, :] = a[..., 0] + 1j * a[..., 1]
+                r += 1
+    assert r == len(recs)
+    return out
+
+
+@pytest.mark.parametrize("nc", [0, 1])
+def test_checkpoint_files_in_reference_format(tmp_path, oracle_mod, gpu_mod, nc):
+    n = 32
+    o = oracle_mod.Oracle(n, 0.01)
+    un0 = o.field_init(5)
+    o.close()
+    s = gpu_mod.Solver(n=n, precision=gpu_mod.PREC_FP64, viscos=0.01, cfl=1.0, nc=nc, pr=0.7, grad=(0, 1, 0))
+    st = np.zeros(s.state_shape(), complex)
+    st[:3] = un0
+    if nc:
+        st[3] = un0[0] * 0.3
+    s.set_state(st)
+    s.step()
+    path = str(tmp_path / "outpenc.p0")
+    s.write_checkpoint(path)
+    got = _read_pencil_file(path, n, 3 + nc)
+    full = s.get_state(gpu_mod.FIELD_UN, layout=gpu_mod.LAYOUT_FULL)
+    expect = full[..., : n // 2].copy()
+    expect[:, n // 2, :, :] = 0
+    expect[:, :, n // 2, :] = 0
+    np.testing.assert_array_equal(got, expect)
+    s2 = gpu_mod.Solver(n=n, precision=gpu_mod.PREC_FP64, viscos=0.01, cfl=1.0, nc=nc, pr=0.7, grad=(0, 1, 0))
+    s2.read_checkpoint(path)
+    np.testing.assert_array_equal(s2.get_state(gpu_mod.FIELD_UN), s.get_state(gpu_mod.FIELD_UN))
+    s.close()
+    s2.close()
