@@ -226,6 +226,13 @@ int psdns_gpu_ensemble_step(void *ens, int32_t nsteps, double *info);
 int psdns_gpu_ensemble_spectra(void *ens, int32_t box, int32_t which, double *ek, double *dk, double *eijk,
                                double *stats);
 
+/* Initial particle positions as partin (hooks/LAG_LOCAL/partin.f) makes
+ * them, at the first particle phase of the next step (with that step's
+ * stage-1 shifts): pstart = 0, nop uniform random positions, nearly equal
+ * numbers per y-slice, from RNG sequence kipran (compart_set.f:160 sets 11);
+ * pstart = -1, a cubic lattice of nop^3 grid nodes. */
+int psdns_gpu_particles_init(void *ctx, int64_t nop, int32_t pstart, int32_t kipran);
+
 /* Checkpoints in the reference's own file format: one task's pencil file
  * as homogeneous/outpen_write_r.f writes it (big-endian unformatted
  * records, real(8) pairs, kx = 0..nx/2-1, Nyquist y and z planes left out),

@@ -161,6 +161,8 @@ struct Ctx {
   double *d_pos = nullptr, *d_vel = nullptr;
   void *d_bs = nullptr, *d_spf = nullptr;
   bool part_first = true;
+  long long pin_nop = 0;           // partin request, made at the first particle phase
+  int pin_pstart = 0, pin_kipran = 11;
   void* h_forc = nullptr;          // pinned staging of the forcing table (device precision)
   std::vector<double> efk_host;    // energy input per shell of the last step (forcdt.f)
   double erate = 0, eirate[3] = {0, 0, 0};
@@ -606,7 +608,64 @@ static int collect_forcing_stats(Ctx& c) {
   return 0;
 }
 
+// hooks/LAG_LOCAL/partin.f:93-131 (pstart = 0: nop uniform random positions,
+// nearly equal numbers per y-slice, from RNG sequence kipran; ranu2.f with
+// RANDOM_SEED shares the seed of ranu) and :141-190 (pstart = -1: a cubic
+// lattice of nop^3 grid nodes).  Grid planes gx(i) = 1 + (i-1)/beta1 +
+// gsh(1,1) (partsp.f:44-53) with this step's stage-1 shifts.
+static int make_partin(Ctx& c) {
+  const int n = c.n;
+  const double ps1 = std::sqrt(c.p.beta1 * c.p.beta1), ps2 = std::sqrt(c.p.beta2 * c.p.beta2),
+               ps3 = std::sqrt(c.p.beta3 * c.p.beta3);
+  long long nop = c.pin_pstart == -1 ? c.pin_nop * c.pin_nop * c.pin_nop : c.pin_nop;
+  std::vector<double> pos(3 * (size_t)nop);
+  if (c.pin_pstart == 0) {
+    const double gx1 = 1. + 0. / ps1 + c.gsh[0][0], gz1 = 1. + 0. / ps3 + c.gsh[2][0];
+    const long long npy = nop / n, npe = nop - npy * n;
+    long long niny = 0;
+    c.rng.ranseq(c.pin_kipran);
+    for (int y = 1; y <= n; y++) {
+      const long long ni = npy + (y <= npe ? 1 : 0);
+      for (int k = 0; k < 3; k++)
+        for (long long i = 0; i < ni; i++) pos[k * nop + niny + i] = c.rng.ranu();
+      const double gy = 1. + (double)(y - 1) / ps2 + c.gsh[1][0];
+      for (long long i = 0; i < ni; i++) {
+        const long long m = niny + i;
+        pos[m] = pos[m] * (double)n + gx1;
+        pos[nop + m] = pos[nop + m] / ps2 + gy;
+        pos[2 * nop + m] = pos[2 * nop + m] * (double)n + gz1;
+      }
+      niny += ni;
+    }
+  } else {
+    const long long npu = c.pin_nop;
+    long long it[3], i1[3], i2[3];
+    for (int d = 0; d < 3; d++) {
+      it[d] = n / npu + (n % npu ? 1 : 0);
+      i1[d] = std::max(1LL, n / 2 + 1 - npu / 2 * it[d] + it[d] / 2);
+      i2[d] = std::min((long long)n, n / 2 + 1 + npu / 2 * it[d] - it[d] / 2);
+    }
+    const double psv[3] = {ps1, ps2, ps3};
+    long long idx = 0;
+    for (long long k = i1[2]; k <= i2[2]; k += it[2])
+      for (long long j = i1[1]; j <= i2[1]; j += it[1])
+        for (long long i = i1[0]; i <= i2[0]; i += it[0]) {
+          if (idx < nop) {
+            pos[idx] = 1. + (double)(i - 1) / psv[0] + c.gsh[0][0];
+            pos[nop + idx] = 1. + (double)(j - 1) / psv[1] + c.gsh[1][0];
+            pos[2 * nop + idx] = 1. + (double)(k - 1) / psv[2] + c.gsh[2][0];
+          }
+          idx++;
+        }
+    if (idx != nop) return set_error("partin: the lattice has %lld nodes, not %lld (partin.f:129)", idx, nop);
+  }
+  c.pin_nop = 0;
+  if (psdns_gpu_particles_set(&c, nop, pos.data())) return 1;
+  return 0;
+}
+
 static int run_stage(Ctx& c, const Ops& o, int kstep, int* ctl_err) {
+  if (kstep == 1 && c.pin_nop > 0 && make_partin(c)) return 1;
   if (kstep == 1 && c.np > 0 && o.particles(c)) return 1;
   if (kstep == 1) CK(cudaMemsetAsync(c.d_velmax, 0, sizeof(unsigned long long), c.stream));
   if (o.stage_a(c, kstep)) return 1;
@@ -1343,6 +1402,21 @@ int psdns_gpu_particles_set(void* ctx, int64_t np, const double* pos) {
   CK(cudaMemset(c->d_vel, 0, sizeof(double) * 3 * (size_t)np));
   c->np = np;
   c->part_first = true;
+  return 0;
+}
+
+int psdns_gpu_particles_init(void* ctx, int64_t nop, int32_t pstart, int32_t kipran) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return set_error("null context");
+  if (pstart != 0 && pstart != -1) return set_error("pstart must be 0 (random) or -1 (lattice)");
+  if (nop <= 0) return set_error("nop must be positive");
+  if (kipran < 1 || kipran > 20) return set_error("kipran must be 1..20 (ranseq.f:131)");
+  const long long tot = pstart == -1 ? (long long)nop * nop * nop : nop;
+  if (tot > (long long)c->n * c->n * c->n && pstart == -1)
+    return set_error("a lattice of %lld particles exceeds the %d^3 grid (partin.f:167)", tot, c->n);
+  c->pin_nop = nop;
+  c->pin_pstart = pstart;
+  c->pin_kipran = kipran;
   return 0;
 }
 

@@ -96,6 +96,12 @@ module psdns_gpu_mod
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
     end function
+    integer(c_int) function psdns_gpu_particles_init(ctx, nop, pstart, kipran) bind(c, name='psdns_gpu_particles_init')
+      import :: c_int, c_ptr, c_int32_t, c_int64_t
+      type(c_ptr), value :: ctx
+      integer(c_int64_t), value :: nop
+      integer(c_int32_t), value :: pstart, kipran
+    end function
     integer(c_int) function psdns_gpu_write_checkpoint(ctx, path, which) bind(c, name='psdns_gpu_write_checkpoint')
       import :: c_int, c_ptr, c_int32_t, c_char
       type(c_ptr), value :: ctx

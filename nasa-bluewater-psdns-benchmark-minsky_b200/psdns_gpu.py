@@ -27,6 +27,7 @@ FIELD_UN = 1
 
 # every entry point declared in include/psdns_gpu.h
 EXPORTS = (
+    "psdns_gpu_particles_init",
     "psdns_gpu_write_checkpoint",
     "psdns_gpu_read_checkpoint",
     "psdns_gpu_gradient_moments",
@@ -116,6 +117,7 @@ def load():
     L.psdns_gpu_spectra.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
+    L.psdns_gpu_particles_init.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32]
     L.psdns_gpu_write_checkpoint.argtypes = [vp, ctypes.c_char_p, ctypes.c_int32]
     L.psdns_gpu_read_checkpoint.argtypes = [vp, ctypes.c_char_p]
     L.psdns_gpu_gradient_moments.argtypes = [vp, ctypes.c_int32, dp, dp]
@@ -304,6 +306,11 @@ class Solver:
         flat = np.ascontiguousarray(a.T)   # (3, np): column-major (np,3)
         self._np = flat.shape[1]
         _check(load().psdns_gpu_particles_set(self._ctx, self._np, _dp(flat)), "particles_set")
+
+    def particles_init(self, nop, pstart=0, kipran=11):
+        """partin.f positions, made at the next step's particle phase."""
+        _check(load().psdns_gpu_particles_init(self._ctx, int(nop), int(pstart), int(kipran)), "particles_init")
+        self._np = int(nop) if pstart == 0 else int(nop) ** 3
 
     def particles_get(self):
         pos = np.zeros((3, self._np)); vel = np.zeros((3, self._np))

@@ -58,6 +58,7 @@ def lib():
         L.orc_spectra.argtypes = [vp, ctypes.c_int, dp, dp, dp, dp]
         L.orc_particles_set.argtypes = [vp, ctypes.c_long, dp]
         L.orc_particles_get.argtypes = [vp, dp, dp]
+        L.orc_particles_init.argtypes = [vp, ctypes.c_long, ctypes.c_int, ctypes.c_int]
         L.orc_gradient_moments.argtypes = [vp, ctypes.c_int, dp, dp]
         L.orc_set_scalar.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_double]
@@ -187,6 +188,12 @@ class Oracle:
         flat = np.ascontiguousarray(np.asarray(pos, np.float64).T)
         self._np = flat.shape[1]
         lib().orc_particles_set(self._c, self._np, _dp(flat))
+
+    def particles_init(self, nop, pstart=0, kipran=11):
+        """partin.f: positions made at the first particle phase (pstart 0:
+        nop uniform random, -1: a lattice of nop^3 nodes)."""
+        lib().orc_particles_init(self._c, int(nop), int(pstart), int(kipran))
+        self._np = int(nop) if pstart == 0 else int(nop) ** 3
 
     def particles_get(self):
         pos = np.zeros((3, self._np)); vel = np.zeros((3, self._np))

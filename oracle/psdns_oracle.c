@@ -194,6 +194,8 @@ typedef struct {
     long np;
     double *pp;            /* [9][np] */
     int part_first;
+    long pin_nop;          /* partin request pending at the first particle phase */
+    int pin_pstart, pin_kipran;
 } orc_ctx;
 
 static int mask_ok(const orc_ctx *c, int a, int y)
@@ -1165,6 +1167,76 @@ static double binterp(const double *bs, int n, const double p[3], const double g
     return sum;
 }
 
+/* hooks/LAG_LOCAL/partin.f:93-131 (pstart = 0: uniform random positions,
+ * nearly equal numbers per y-slice, from the kipran sequence through ranu2,
+ * ranu2.f with RANDOM_SEED sharing the seed of ranu) and :141-190 (pstart =
+ * -1: a cubic lattice of nop^3 grid nodes); grid planes gx(i) = 1 + (i-1)/
+ * beta1 + gsh(1,1) (partsp.f:44-53), box lengths nx, ny, nz (partsp.f:61).
+ * Made when the first particle phase runs (partsp.f:147-149), with that
+ * step's stage-1 shifts. */
+static void partin(orc_ctx *c)
+{
+    int n = c->n;
+    double ps1 = sqrt(c->b11), ps2 = sqrt(c->b22), ps3 = sqrt(c->b33);
+    double gx1 = 1. + 0. / ps1 + c->gsh[0][0];
+    double gz1 = 1. + 0. / ps3 + c->gsh[2][0];
+    long nop = c->pin_nop;
+    if (c->pin_pstart == -1) nop = nop * nop * nop;
+    free(c->pp);
+    c->pp = calloc((size_t)9 * nop, sizeof(double));
+    c->np = nop;
+    double *pp = c->pp;
+    if (c->pin_pstart == 0) {
+        long npy = nop / n, npe = nop - npy * n, niny = 0;
+        rng_ranseq(&c->rng, c->pin_kipran);
+        for (int y = 1; y <= n; y++) {
+            long ni = npy + (y <= npe ? 1 : 0);
+            for (int k = 0; k < 3; k++)
+                for (long i = 0; i < ni; i++) pp[k * nop + niny + i] = rng_ranu(&c->rng);
+            double gy = 1. + (double)(y - 1) / ps2 + c->gsh[1][0];
+            for (long i = 0; i < ni; i++) {
+                long m = niny + i;
+                pp[m] = pp[m] * (double)n + gx1;
+                pp[nop + m] = pp[nop + m] / ps2 + gy;
+                pp[2 * nop + m] = pp[2 * nop + m] * (double)n + gz1;
+            }
+            niny += ni;
+        }
+    } else {
+        long npu = c->pin_nop;
+        long it[3], i1[3], i2[3];
+        for (int d = 0; d < 3; d++) {
+            it[d] = n / npu + (n % npu ? 1 : 0);
+            i1[d] = n / 2 + 1 - npu / 2 * it[d] + it[d] / 2;
+            i2[d] = n / 2 + 1 + npu / 2 * it[d] - it[d] / 2;
+            if (i1[d] < 1) i1[d] = 1;
+            if (i2[d] > n) i2[d] = n;
+        }
+        double psv[3] = {ps1, ps2, ps3};
+        long idx = 0;
+        for (long k = i1[2]; k <= i2[2]; k += it[2])
+            for (long j = i1[1]; j <= i2[1]; j += it[1])
+                for (long i = i1[0]; i <= i2[0]; i += it[0]) {
+                    if (idx < nop) {
+                        pp[idx] = 1. + (double)(i - 1) / psv[0] + c->gsh[0][0];
+                        pp[nop + idx] = 1. + (double)(j - 1) / psv[1] + c->gsh[1][0];
+                        pp[2 * nop + idx] = 1. + (double)(k - 1) / psv[2] + c->gsh[2][0];
+                    }
+                    idx++;
+                }
+        if (idx != nop) c->status = 5;   /* partin.f:129-135 stops here */
+    }
+    c->part_first = 1;
+    c->pin_nop = 0;
+}
+
+void orc_particles_init(orc_ctx *c, long nop, int pstart, int kipran)
+{
+    c->pin_nop = nop;
+    c->pin_pstart = pstart;
+    c->pin_kipran = kipran;
+}
+
 void orc_particles_set(orc_ctx *c, long np, const double *pos)
 {
     free(c->pp);
@@ -1246,6 +1318,7 @@ static int rk_stage(orc_ctx *c, int kstep)
     }
     double *p = (double *)malloc(sizeof(double) * (5 + nc) * np);
     itransform(c, w, 3 + 3 * nc, p);
+    if (kstep == 1 && c->pin_nop > 0) partin(c);
     if (kstep == 1 && c->np > 0) particles_stage1(c, p);   /* realspace -> lagpart */
     double vm = realspace(c, p, kstep == 1);
     if (kstep == 1) c->velmax = vm;

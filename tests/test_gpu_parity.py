@@ -363,3 +363,31 @@ def test_checkpoint_files_in_reference_format(tmp_path, oracle_mod, gpu_mod, nc)
     np.testing.assert_array_equal(s2.get_state(gpu_mod.FIELD_UN), s.get_state(gpu_mod.FIELD_UN))
     s.close()
     s2.close()
+
+
+@pytest.mark.parametrize("pstart,nop", [(0, 500), (-1, 4)])
+def test_partin_matches_oracle(oracle_mod, gpu_mod, pstart, nop):
+    """partin.f positions from the kipran RNG sequence (bit-exact: host
+    arithmetic on both sides), then 3 particle steps (FP64 device)."""
+    n, nu = 32, 0.01
+    o = oracle_mod.Oracle(n, nu, cfl=-1, dt=0.01, kshift=1)
+    un0 = o.field_init(9)
+    o.set_state(un0)
+    o.particles_init(nop, pstart, 11)
+    s = gpu_mod.Solver(n=n, precision=gpu_mod.PREC_FP64, viscos=nu, cfl=-1, dt=0.01, kshift=1)
+    s.set_state(un0)
+    s.particles_init(nop, pstart, 11)
+    o.step()
+    s.step()
+    po, vo = o.particles_get()
+    pg, vg = s.particles_get()
+    np.testing.assert_array_equal(pg, po)
+    assert np.abs(vg - vo).max() < 1e-9 * np.abs(vo).max()
+    for _ in range(2):
+        o.step()
+        s.step()
+    po, _ = o.particles_get()
+    pg, _ = s.particles_get()
+    assert np.abs(pg - po).max() < 1e-11 * n
+    o.close()
+    s.close()

@@ -269,3 +269,34 @@ def test_gradient_moments_of_a_single_mode(oracle_mod):
     np.testing.assert_allclose(mu[7], 35 * g ** 8 / 128, rtol=1e-11)
     assert np.abs(mw).max() < 1e-28
     o.close()
+
+
+def test_partin_positions(oracle_mod):
+    """partin.f pstart = 0: nearly equal numbers per y-slice, each inside its
+    slice [gy(y), gy(y) + 1) and inside the box in x and z; pstart = -1: the
+    lattice nodes are grid planes."""
+    n = 16
+    o = oracle_mod.Oracle(n, 0.01, cfl=-1, dt=0.001, kshift=1)
+    un = o.field_init(3)
+    o.set_state(un)
+    o.particles_init(100, 0, 11)
+    o.step()
+    pos, vel = o.particles_get()
+    assert pos.shape == (100, 3)
+    g = o.scalars()["gsh"][:, 0]
+    counts = np.bincount(np.floor(pos[:, 1] - 1 - g[1]).astype(int), minlength=n)
+    assert counts.max() - counts.min() <= 1 and counts.sum() == 100
+    for d in (0, 2):
+        assert np.all(pos[:, d] >= 1 + g[d]) and np.all(pos[:, d] < 1 + g[d] + n)
+    assert np.abs(vel).max() > 0
+    o.close()
+    o = oracle_mod.Oracle(n, 0.01, cfl=-1, dt=0.001, kshift=1)
+    o.set_state(un)
+    o.particles_init(4, -1, 11)
+    o.step()
+    pos, _ = o.particles_get()
+    g = o.scalars()["gsh"][:, 0]
+    assert pos.shape == (64, 3)
+    frac = pos - 1 - g
+    np.testing.assert_allclose(frac, np.round(frac), atol=1e-12)
+    o.close()
