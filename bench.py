@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--cpu-n", type=int, default=256)
     ap.add_argument("--particles", type=int, default=1 << 24)
     ap.add_argument("--unforced", action="store_true")
+    ap.add_argument("--nc", type=int, default=0, choices=[0, 1],
+                    help="1: also advance a passive scalar (Sc = 1, mean gradient (0, 1, 0))")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="instead: B boxes of n in {32,48,64,96}, log-uniform viscosity, fixed dt")
     return ap.parse_args()
@@ -253,7 +255,7 @@ def main():
     kforce = 0.0 if args.unforced else 2.99                          # shells |k| < 3
     epsfor = eps_target / (4.0 * (4.0 * math.pi / 3.0) * 3.0 ** 3)   # epfor_param.f: eps/(4 N_f)
     s = P.Solver(n=n, precision=prec, viscos=nu, cfl=math.pi, dt=0.0, kshift=1,
-                 kforce=kforce, tforce=0.5, epsfor=epsfor, tfiuo=0.0)
+                 kforce=kforce, tforce=0.5, epsfor=epsfor, tfiuo=0.0, nc=args.nc, pr=1.0, grad=(0.0, 1.0, 0.0))
     s.field_init(1234 + rank)
     npart = args.particles
     if npart > 0:
@@ -334,7 +336,7 @@ def main():
     # from pinned host memory and back every step
     e2e = None
     if not args.no_e2e:
-        nbytes = 3 * s.xz_tot * n * 16
+        nbytes = (3 + args.nc) * s.xz_tot * n * 16
         try:
             host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
             ptr = host.data_ptr()
@@ -382,8 +384,8 @@ def main():
             "data": "synthetic: seeded random solenoidal field, E(k)~k^4 exp(-2(k/3)^2), u'=1",
             "config": {"workload": f"{'unforced' if kforce == 0 else 'forced'} RK2 step of one {n}^3 periodic box "
                                    f"per GPU, {args.prec} state, kshift=1 phase shifts, cfl=pi (Courant 0.5), "
-                                   f"{npart} particles",
-                       "n": n, "precision": args.prec, "viscosity": nu, "kforce": kforce, "tforce": 0.5,
+                                   f"{npart} particles" + (", one passive scalar (Sc 1, G (0,1,0))" if args.nc else ""),
+                       "nc": args.nc, "n": n, "precision": args.prec, "viscosity": nu, "kforce": kforce, "tforce": 0.5,
                        "epsfor": epsfor, "particles": npart, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (state >= 9 GB per variable set), no flush needed"},
             "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
