@@ -242,6 +242,16 @@ int psdns_gpu_particles_init(void *ctx, int64_t nop, int32_t pstart, int32_t kip
 int psdns_gpu_write_checkpoint(void *ctx, const char *path, int32_t which);
 int psdns_gpu_read_checkpoint(void *ctx, const char *path);
 
+/* One-dimensional spectra and the length/time scales of sptr
+ * (homogeneous/sptr.f:119-218, :311-468), FP64: xr, yr, zr [6][nx/2+1] are
+ * the normalised spectra along x, y, z of the pairs 11,12,13,22,23,33;
+ * stats[55] = corr[6], integral scales lijk[6][3], rms[3], integral-scale
+ * Reynolds numbers raak[3], eddy turnover times ett[3], mean square
+ * derivatives tmij[3][3] (component i, direction a), grdiss, Taylor
+ * microscales taak[3][3], Taylor Reynolds numbers tmre[3].  Any output may
+ * be null. */
+int psdns_gpu_spectra_scales(void *ctx, int32_t which, double *xr, double *yr, double *zr, double *stats);
+
 /* Moments of the velocity gradients (replaces PSDNS/vgmomt.f, called from
  * itransform.f:385 on I/O steps): out[0..7] = <(du/dx)^m>, m = 1..8, and
  * out[8..15] = <(dw/dz)^m> of u or un, averaged over the n^3 points of the

@@ -780,6 +780,111 @@ static void chunk_range(const Ctx& c, int k, size_t& off, size_t& cnt) {
   cnt = std::min(tot, off + per) - off;
 }
 
+// sptr.f:199-218, :311-346 and :351-468 for the velocity: the normalised
+// one-dimensional spectra xr, yr, zr ([6][n/2+1], pairs 11,12,13,22,23,33),
+// and stats[55] = corr[6], lijk[6][3] (integral scales), rms[3], raak[3]
+// (integral-scale Reynolds numbers), ett[3] (eddy turnover times),
+// tmij[3][3] (mean square derivative of u_i along direction a), grdiss,
+// taak[3][3] (Taylor microscales taylor(i,j,j)), tmre[3] (Taylor Reynolds
+// numbers).  scratch holds 3 * 6 * (n/2+1) + 6 doubles.
+static int spectra_scales_of(const Geo& g, const void* src, int prec, const psdns_params& p, cudaStream_t stream,
+                             void* scratch, double* xr_out, double* yr_out, double* zr_out, double* stats) {
+  const int n = g.n, nh = n / 2 + 1, NP = kSpec1dPairs;
+  const size_t nv = (size_t)3 * NP * nh + NP;
+  double* d_out = (double*)scratch;
+  CK(cudaMemsetAsync(d_out, 0, nv * sizeof(double), stream));
+  const double b22 = p.beta2 * p.beta2;
+  const size_t smem = nv * sizeof(double);
+  if (prec == PSDNS_PREC_FP64) {
+    CK(cudaFuncSetAttribute(k_spectra_1d<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_spectra_1d<double><<<148, 512, smem, stream>>>(g, (const double2*)src, b22, d_out);
+  } else {
+    CK(cudaFuncSetAttribute(k_spectra_1d<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_spectra_1d<float><<<148, 512, smem, stream>>>(g, (const float2*)src, b22, d_out);
+  }
+  CK(cudaGetLastError());
+  std::vector<double> h(nv);
+  CK(cudaMemcpyAsync(h.data(), d_out, nv * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  double* xr = h.data();
+  double* yr = xr + NP * nh;
+  double* zr = yr + NP * nh;
+  double* der2 = zr + NP * nh;
+  const double sv[3] = {p.beta1, p.beta2, p.beta3};
+  const double s23 = sv[1] * sv[2], s31 = sv[2] * sv[0], s12 = sv[0] * sv[1], size = sv[0] * sv[1] * sv[2];
+  const int pi_[NP] = {0, 0, 0, 1, 1, 2}, pj_[NP] = {0, 1, 2, 1, 2, 2};
+  for (int ij = 0; ij < NP; ij++) {
+    const double factor = sv[pi_[ij]] * sv[pj_[ij]];
+    der2[ij] = der2[ij] * factor;
+    for (int k = 0; k < nh; k++) {
+      xr[ij * nh + k] = factor * xr[ij * nh + k] / size;
+      yr[ij * nh + k] = factor * yr[ij * nh + k] / size;
+      zr[ij * nh + k] = factor * zr[ij * nh + k] / size;
+    }
+  }
+  const double pi = 4. * std::atan(1.), nu = p.viscos;
+  double corr[NP];
+  for (int ij = 0; ij < NP; ij++) {
+    for (int k = 0; k < nh; k++) {
+      xr[ij * nh + k] = s23 * xr[ij * nh + k];
+      yr[ij * nh + k] = s31 * yr[ij * nh + k];
+      zr[ij * nh + k] = s12 * zr[ij * nh + k];
+    }
+    double ssum = xr[ij * nh];
+    for (int x = 1; x < n / 2; x++) ssum = ssum + 2. * xr[ij * nh + x];
+    corr[ij] = sv[0] * ssum;
+  }
+  double lijk[NP][3] = {};
+  for (int ij = 0; ij < NP; ij++)
+    if (corr[ij] != 0.) {
+      lijk[ij][0] = pi * xr[ij * nh] / corr[ij];
+      lijk[ij][1] = pi * yr[ij * nh] / corr[ij];
+      lijk[ij][2] = pi * zr[ij * nh] / corr[ij];
+    }
+  const int kt[3] = {0, 3, 5};
+  double rms[3], raak[3] = {0, 0, 0}, ett[3] = {0, 0, 0}, tmij[3][3], taak[3][3], tmre[3] = {0, 0, 0};
+  for (int i = 0; i < 3; i++) rms[i] = std::sqrt(corr[kt[i]]);
+  if (nu > 0.)
+    for (int i = 0; i < 3; i++) raak[i] = lijk[kt[i]][i] * rms[i] / nu;
+  for (int i = 0; i < 3; i++)
+    if (rms[i] != 0) ett[i] = lijk[kt[i]][i] / rms[i];
+  for (int i = 0; i < 3; i++) {
+    double ssum = 0.;
+    for (int x = 1; x < n / 2; x++) ssum = ssum + (double)x * (double)x * xr[kt[i] * nh + x];
+    tmij[i][0] = 2. * sv[0] * sv[0] * sv[0] * ssum;
+    tmij[i][1] = der2[kt[i]];
+    ssum = 0.;
+    for (int z = 1; z < n / 2; z++) ssum = ssum + (double)z * (double)z * zr[kt[i] * nh + z];
+    tmij[i][2] = 2. * sv[2] * sv[2] * sv[2] * ssum;
+  }
+  double grdiss = tmij[0][0] + tmij[1][1] + tmij[2][2] + tmij[0][1] + tmij[1][0] + tmij[0][2] + tmij[2][0] +
+                  tmij[1][2] + tmij[2][1];
+  grdiss = grdiss * nu;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) taak[i][j] = tmij[j][j] != 0. ? std::sqrt(corr[kt[i]] / tmij[j][j]) : 0.;
+  if (nu > 0.)
+    for (int i = 0; i < 3; i++) tmre[i] = taak[i][i] * rms[i] / nu;
+  if (xr_out) std::memcpy(xr_out, xr, sizeof(double) * NP * nh);
+  if (yr_out) std::memcpy(yr_out, yr, sizeof(double) * NP * nh);
+  if (zr_out) std::memcpy(zr_out, zr, sizeof(double) * NP * nh);
+  if (stats) {
+    double* o = stats;
+    for (int ij = 0; ij < NP; ij++) *o++ = corr[ij];
+    for (int ij = 0; ij < NP; ij++)
+      for (int a = 0; a < 3; a++) *o++ = lijk[ij][a];
+    for (int i = 0; i < 3; i++) *o++ = rms[i];
+    for (int i = 0; i < 3; i++) *o++ = raak[i];
+    for (int i = 0; i < 3; i++) *o++ = ett[i];
+    for (int i = 0; i < 3; i++)
+      for (int a = 0; a < 3; a++) *o++ = tmij[i][a];
+    *o++ = grdiss;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) *o++ = taak[i][j];
+    for (int i = 0; i < 3; i++) *o++ = tmre[i];
+  }
+  return 0;
+}
+
 // big-endian Fortran record helpers for the checkpoint files
 static void be32(std::vector<unsigned char>& b, uint32_t v) {
   for (int s = 24; s >= 0; s -= 8) b.push_back((unsigned char)(v >> s));
@@ -1445,6 +1550,14 @@ int psdns_gpu_gradient_moments(void* ctx, int32_t which, const double* gsh, doub
   Ops o;
   if (!get_ops(c->prec, c->n, c->nc, o)) return set_error("bad context");
   return o.moments(*c, which, gsh, out);
+}
+
+int psdns_gpu_spectra_scales(void* ctx, int32_t which, double* xr, double* yr, double* zr, double* stats) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return set_error("null context");
+  if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
+  return spectra_scales_of(make_geo(*c), which == PSDNS_FIELD_U ? c->d_u : c->d_un, c->prec, c->p, c->stream,
+                           c->d_ub, xr, yr, zr, stats);
 }
 
 int psdns_gpu_forcing_stats(void* ctx, double* efk, double* eirate, double* erate) {

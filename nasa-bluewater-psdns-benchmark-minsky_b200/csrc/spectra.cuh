@@ -53,4 +53,73 @@ __global__ void k_spectra(Geo g, const C2<T>* __restrict__ un, double b11, doubl
     if (hist[i] != 0.0) atomicAdd(out + i, hist[i]);
 }
 
+// One-dimensional spectra and the derivative variance of sptr.f:119-218 for
+// the 6 velocity products ij (11,12,13,22,23,33): per column a (kx, kz) the
+// y-sum of Re(u_i u_j*) over the sphere goes to xr[ij][kx] and to
+// zr[ij][|kz|] (conjugate-symmetric halves folded as sptr.f:198-205), each
+// mode to yr[ij][|ky|] (:150-159), and ky2 Re(u_i u_j*) tfact to der2[ij].
+// out layout: xr[6][n/2+1], yr[6][n/2+1], zr[6][n/2+1], der2[6].  One warp
+// per column; shared-memory FP64 histograms, added to out once per block.
+constexpr int kSpec1dPairs = 6;
+
+template <typename T>
+__global__ void __launch_bounds__(512) k_spectra_1d(Geo g, const C2<T>* __restrict__ un, double b22,
+                                                    double* __restrict__ out) {
+  extern __shared__ double h1[];
+  const int n = g.n, nh = n / 2 + 1;
+  const int nv = 3 * kSpec1dPairs * nh + kSpec1dPairs;
+  for (int i = threadIdx.x; i < nv; i += blockDim.x) h1[i] = 0.0;
+  __syncthreads();
+  double* xr = h1;
+  double* yr = h1 + kSpec1dPairs * nh;
+  double* zr = h1 + 2 * kSpec1dPairs * nh;
+  double* d2 = h1 + 3 * kSpec1dPairs * nh;
+  const size_t vs = (size_t)g.xz_tot * n;
+  const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+  double der2[kSpec1dPairs] = {0, 0, 0, 0, 0, 0};
+  for (int a = blockIdx.x * warps + (threadIdx.x >> 5); a < g.xz_tot; a += gridDim.x * warps) {
+    const int x = __ldg(g.ax + a), z = __ldg(g.az + a), km = __ldg(g.kymax + a);
+    const double tf = x == 0 ? 1.0 : 2.0;
+    double ysum[kSpec1dPairs] = {0, 0, 0, 0, 0, 0};
+    for (int y = lane; y < n; y += 32) {
+      const int ky = y > n / 2 ? n - y : y;
+      if (y == n / 2 || ky > km) continue;
+      const size_t o = (size_t)a * n + y;
+      const C2<T> u1 = un[o], u2 = un[vs + o], u3 = un[2 * vs + o];
+      const double a1 = u1.x, c1 = u1.y, a2 = u2.x, c2 = u2.y, a3 = u3.x, c3 = u3.y;
+      const double p[kSpec1dPairs] = {a1 * a1 + c1 * c1, a1 * a2 + c1 * c2, a1 * a3 + c1 * c3,
+                                      a2 * a2 + c2 * c2, a2 * a3 + c2 * c3, a3 * a3 + c3 * c3};
+      const double ky2 = b22 * (double)ky * (double)ky;
+#pragma unroll
+      for (int ij = 0; ij < kSpec1dPairs; ij++) {
+        ysum[ij] += p[ij];
+        der2[ij] += ky2 * (tf * p[ij]);
+        if (y == 0) atomicAdd(yr + ij * nh, tf * p[ij]);
+        else if (y < n / 2) atomicAdd(yr + ij * nh + y, p[ij]);
+        else if (tf > 1.0) atomicAdd(yr + ij * nh + (n - y), p[ij]);
+      }
+    }
+#pragma unroll
+    for (int ij = 0; ij < kSpec1dPairs; ij++) {
+      double v = ysum[ij];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) {
+        atomicAdd(xr + ij * nh + x, v);
+        if (z == 0) atomicAdd(zr + ij * nh, tf * v);
+        else if (z < n / 2) atomicAdd(zr + ij * nh + z, v);
+        else if (z > n / 2 && tf > 1.0) atomicAdd(zr + ij * nh + (n - z), v);
+      }
+    }
+  }
+#pragma unroll
+  for (int ij = 0; ij < kSpec1dPairs; ij++) {
+    double v = der2[ij];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) atomicAdd(d2 + ij, v);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nv; i += blockDim.x)
+    if (h1[i] != 0.0) atomicAdd(out + i, h1[i]);
+}
+
 }  // namespace psdns

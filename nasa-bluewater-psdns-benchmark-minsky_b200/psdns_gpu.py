@@ -27,6 +27,7 @@ FIELD_UN = 1
 
 # every entry point declared in include/psdns_gpu.h
 EXPORTS = (
+    "psdns_gpu_spectra_scales",
     "psdns_gpu_particles_init",
     "psdns_gpu_write_checkpoint",
     "psdns_gpu_read_checkpoint",
@@ -117,6 +118,7 @@ def load():
     L.psdns_gpu_spectra.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
+    L.psdns_gpu_spectra_scales.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_particles_init.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32]
     L.psdns_gpu_write_checkpoint.argtypes = [vp, ctypes.c_char_p, ctypes.c_int32]
     L.psdns_gpu_read_checkpoint.argtypes = [vp, ctypes.c_char_p]
@@ -337,6 +339,17 @@ class Solver:
         out = np.zeros(16, np.float64)
         _check(load().psdns_gpu_gradient_moments(self._ctx, int(which), _dp(g), _dp(out)), "gradient_moments")
         return out[:8].copy(), out[8:].copy()
+
+    def spectra_scales(self, which=FIELD_UN):
+        """sptr.f one-dimensional spectra ([6, n/2+1] each) and scale statistics."""
+        nh = self.n // 2 + 1
+        xr = np.zeros(6 * nh); yr = np.zeros(6 * nh); zr = np.zeros(6 * nh); st = np.zeros(55)
+        _check(load().psdns_gpu_spectra_scales(self._ctx, int(which), _dp(xr), _dp(yr), _dp(zr), _dp(st)),
+               "spectra_scales")
+        return xr.reshape(6, nh), yr.reshape(6, nh), zr.reshape(6, nh), {
+            "corr": st[0:6], "lijk": st[6:24].reshape(6, 3), "rms": st[24:27], "raak": st[27:30],
+            "ett": st[30:33], "tmij": st[33:42].reshape(3, 3), "grdiss": st[42],
+            "taak": st[43:52].reshape(3, 3), "tmre": st[52:55]}
 
     def forcing_table(self):
         """for(kfor,k2fo,k2fo,3) of the last step as an array [3][k2fo][k2fo][kfor]."""

@@ -58,6 +58,7 @@ def lib():
         L.orc_spectra.argtypes = [vp, ctypes.c_int, dp, dp, dp, dp]
         L.orc_particles_set.argtypes = [vp, ctypes.c_long, dp]
         L.orc_particles_get.argtypes = [vp, dp, dp]
+        L.orc_spectra_scales.argtypes = [vp, ctypes.c_int, dp, dp, dp, dp]
         L.orc_particles_init.argtypes = [vp, ctypes.c_long, ctypes.c_int, ctypes.c_int]
         L.orc_gradient_moments.argtypes = [vp, ctypes.c_int, dp, dp]
         L.orc_set_scalar.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -87,6 +88,13 @@ def set_threads(n):
 
 def get_threads():
     return lib().orc_get_threads()
+
+
+def scales_dict(st):
+    """The 55 scale statistics of sptr (psdns_gpu_spectra_scales order)."""
+    return {"corr": st[0:6], "lijk": st[6:24].reshape(6, 3), "rms": st[24:27], "raak": st[27:30],
+            "ett": st[30:33], "tmij": st[33:42].reshape(3, 3), "grdiss": st[42],
+            "taak": st[43:52].reshape(3, 3), "tmre": st[52:55]}
 
 
 class Oracle:
@@ -204,6 +212,14 @@ class Oracle:
         x = np.zeros(n, np.float64)
         lib().orc_rann2(self._c, int(seq), _dp(x), int(n))
         return x
+
+    def spectra_scales(self, which=1):
+        """sptr.f one-dimensional spectra (xr, yr, zr: [6, n/2+1]) and the
+        scale statistics (dict of arrays)."""
+        nh = self.n // 2 + 1
+        xr = np.zeros(6 * nh); yr = np.zeros(6 * nh); zr = np.zeros(6 * nh); st = np.zeros(55)
+        lib().orc_spectra_scales(self._c, int(which), _dp(xr), _dp(yr), _dp(zr), _dp(st))
+        return xr.reshape(6, nh), yr.reshape(6, nh), zr.reshape(6, nh), scales_dict(st)
 
     def gradient_moments(self, which=1, gsh=(0.0, 0.0, 0.0)):
         """vgmomt.f: (moments 1..8 of du/dx, of dw/dz) on the grid shifted by gsh."""

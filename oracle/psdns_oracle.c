@@ -1353,6 +1353,107 @@ int orc_stage(orc_ctx *c, int kstep)
     return rk_stage(c, kstep);
 }
 
+/* sptr.f:119-218 (one-dimensional spectra xrij, yrij, zrij and der2ij of
+ * the velocity pairs 11,12,13,22,23,33), :311-346 (normalisation) and
+ * :351-468 (correlations, integral scales, rms, Reynolds numbers, eddy
+ * turnover times, derivative variances tmij, grdiss, Taylor microscales).
+ * xr, yr, zr: [6][n/2+1]; stats[55] in the order corr[6], lijk[6][3],
+ * rms[3], raak[3], ett[3], tmij[3][3], grdiss, taak[3][3], tmre[3]. */
+void orc_spectra_scales(orc_ctx *c, int which, double *xr, double *yr, double *zr, double *stats)
+{
+    int n = c->n, tot = c->xz_tot, nh = n / 2 + 1;
+    size_t vs = (size_t)tot * n;
+    const cx *u = which == 0 ? c->u : c->un;
+    int pi_[6] = {0, 0, 0, 1, 1, 2}, pj_[6] = {0, 1, 2, 1, 2, 2};
+    double der2[6] = {0, 0, 0, 0, 0, 0};
+    memset(xr, 0, sizeof(double) * 6 * nh);
+    memset(yr, 0, sizeof(double) * 6 * nh);
+    memset(zr, 0, sizeof(double) * 6 * nh);
+    for (int a = 0; a < tot; a++) {
+        int x = c->ax[a], z = c->az[a];
+        double tf = x == 0 ? 1. : 2.;
+        for (int ij = 0; ij < 6; ij++) {
+            double ysum = 0.;
+            for (int y = 0; y < n; y++) {
+                if (!mask_ok(c, a, y)) continue;
+                cx vi = u[pi_[ij] * vs + (size_t)a * n + y], vj = u[pj_[ij] * vs + (size_t)a * n + y];
+                double uiuj = vi.re * vj.re + vi.im * vj.im;
+                ysum += uiuj;
+                if (y == 0) yr[ij * nh] += uiuj + (tf - 1.) * uiuj;
+                else if (y < n / 2) yr[ij * nh + y] += uiuj;
+                else yr[ij * nh + (n - y)] += (tf - 1.) * uiuj;
+                double ky2 = (y == n / 2) ? 0. : c->b22 * c->ky[y] * c->ky[y];
+                der2[ij] += ky2 * (tf * uiuj);
+            }
+            if (z == 0) zr[ij * nh] += ysum + (tf - 1.) * ysum;
+            else if (z < n / 2) zr[ij * nh + z] += ysum;
+            else if (z > n / 2) zr[ij * nh + (n - z)] += (tf - 1.) * ysum;
+            xr[ij * nh + x] += ysum;
+        }
+    }
+    double sv[3] = {sqrt(c->b11), sqrt(c->b22), sqrt(c->b33)};
+    double s23 = sv[1] * sv[2], s31 = sv[2] * sv[0], s12 = sv[0] * sv[1], size = sv[0] * sv[1] * sv[2];
+    double pi = 4. * atan(1.), nu = c->viscos, corr[6];
+    for (int ij = 0; ij < 6; ij++) {
+        double factor = sv[pi_[ij]] * sv[pj_[ij]];
+        der2[ij] = der2[ij] * factor;
+        for (int k = 0; k < nh; k++) {
+            xr[ij * nh + k] = factor * xr[ij * nh + k] / size;
+            yr[ij * nh + k] = factor * yr[ij * nh + k] / size;
+            zr[ij * nh + k] = factor * zr[ij * nh + k] / size;
+        }
+    }
+    for (int ij = 0; ij < 6; ij++) {
+        for (int k = 0; k < nh; k++) {
+            xr[ij * nh + k] = s23 * xr[ij * nh + k];
+            yr[ij * nh + k] = s31 * yr[ij * nh + k];
+            zr[ij * nh + k] = s12 * zr[ij * nh + k];
+        }
+        double ssum = xr[ij * nh];
+        for (int x = 1; x < n / 2; x++) ssum = ssum + 2. * xr[ij * nh + x];
+        corr[ij] = sv[0] * ssum;
+    }
+    double lijk[6][3];
+    memset(lijk, 0, sizeof lijk);
+    for (int ij = 0; ij < 6; ij++)
+        if (corr[ij] != 0.) {
+            lijk[ij][0] = pi * xr[ij * nh] / corr[ij];
+            lijk[ij][1] = pi * yr[ij * nh] / corr[ij];
+            lijk[ij][2] = pi * zr[ij * nh] / corr[ij];
+        }
+    int kt[3] = {0, 3, 5};
+    double rms[3], raak[3] = {0, 0, 0}, ett[3] = {0, 0, 0}, tmij[3][3], taak[3][3], tmre[3] = {0, 0, 0};
+    for (int i = 0; i < 3; i++) rms[i] = sqrt(corr[kt[i]]);
+    for (int i = 0; i < 3; i++) {
+        if (nu > 0.) raak[i] = lijk[kt[i]][i] * rms[i] / nu;
+        if (rms[i] != 0.) ett[i] = lijk[kt[i]][i] / rms[i];
+        double ssum = 0.;
+        for (int x = 1; x < n / 2; x++) ssum = ssum + c->kx[x] * c->kx[x] * xr[kt[i] * nh + x];
+        tmij[i][0] = 2. * sv[0] * sv[0] * sv[0] * ssum;
+        tmij[i][1] = der2[kt[i]];
+        ssum = 0.;
+        for (int z = 1; z < n / 2; z++) ssum = ssum + c->kz[z] * c->kz[z] * zr[kt[i] * nh + z];
+        tmij[i][2] = 2. * sv[2] * sv[2] * sv[2] * ssum;
+    }
+    double grdiss = tmij[0][0] + tmij[1][1] + tmij[2][2] + tmij[0][1] + tmij[1][0] + tmij[0][2] + tmij[2][0] +
+                    tmij[1][2] + tmij[2][1];
+    grdiss = grdiss * nu;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) taak[i][j] = tmij[j][j] != 0. ? sqrt(corr[kt[i]] / tmij[j][j]) : 0.;
+    for (int i = 0; i < 3; i++)
+        if (nu > 0.) tmre[i] = taak[i][i] * rms[i] / nu;
+    double *o = stats;
+    for (int ij = 0; ij < 6; ij++) *o++ = corr[ij];
+    for (int ij = 0; ij < 6; ij++) for (int a = 0; a < 3; a++) *o++ = lijk[ij][a];
+    for (int i = 0; i < 3; i++) *o++ = rms[i];
+    for (int i = 0; i < 3; i++) *o++ = raak[i];
+    for (int i = 0; i < 3; i++) *o++ = ett[i];
+    for (int i = 0; i < 3; i++) for (int a = 0; a < 3; a++) *o++ = tmij[i][a];
+    *o++ = grdiss;
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) *o++ = taak[i][j];
+    for (int i = 0; i < 3; i++) *o++ = tmre[i];
+}
+
 /* vgmomt.f:50-143 (itransform.f:222-230, :385): moments of order 1..8 of
  * du/dx and dw/dz on the grid shifted by gsh[3] (the stage-1 shifts of an I/O
  * step), of u (which = 0) or un (which = 1), each sum divided by n^3.

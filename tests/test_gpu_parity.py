@@ -391,3 +391,27 @@ def test_partin_matches_oracle(oracle_mod, gpu_mod, pstart, nop):
     assert np.abs(pg - po).max() < 1e-11 * n
     o.close()
     s.close()
+
+
+@pytest.mark.parametrize("prec,tol", [(1, 1e-11), (0, 1e-5)])
+def test_spectra_scales_match_oracle(oracle_mod, gpu_mod, prec, tol):
+    """sptr.f one-dimensional spectra and scales after two steps."""
+    n = 32
+    o = oracle_mod.Oracle(n, 0.01, cfl=1.0, kshift=1)
+    un0 = o.field_init(71)
+    o.set_state(un0)
+    s = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=1.0, kshift=1)
+    s.set_state(un0)
+    for _ in range(2):
+        o.step()
+        s.step()
+    for which in (gpu_mod.FIELD_U, gpu_mod.FIELD_UN):
+        xo, yo, zo, so = o.spectra_scales(which)
+        xg, yg, zg, sg = s.spectra_scales(which)
+        for a, b in ((xg, xo), (yg, yo), (zg, zo)):
+            m = np.abs(b) > 1e-6 * np.abs(b).max()
+            assert np.max(np.abs(a[m] - b[m]) / np.abs(b[m])) < tol
+        for k in so:
+            np.testing.assert_allclose(sg[k], so[k], rtol=tol, atol=tol * np.abs(so[k]).max() * 1e-3)
+    o.close()
+    s.close()

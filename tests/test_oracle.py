@@ -300,3 +300,27 @@ def test_partin_positions(oracle_mod):
     frac = pos - 1 - g
     np.testing.assert_allclose(frac, np.round(frac), atol=1e-12)
     o.close()
+
+
+def test_spectra_scales_consistency(oracle_mod):
+    """sptr.f scales: the 1-D spectra integrate to the variances (x, y and z
+    alike), grdiss equals epsilon of the shell spectrum (both are
+    nu <du_i/dx_j du_i/dx_j>), and the Taylor microscale satisfies
+    lambda^2 = <u^2> / <(du/dx)^2>."""
+    n = 32
+    o = oracle_mod.Oracle(n, 0.02)
+    un = o.field_init(44)
+    o.set_state(un)
+    xr, yr, zr, sc = o.spectra_scales(1)
+    _, _, _, st = o.spectra(1)
+    nh = n // 2 + 1
+    for ij in (0, 3, 5):
+        cx = xr[ij, 0] + 2 * xr[ij, 1:n // 2].sum()
+        cy = yr[ij, 0] + 2 * yr[ij, 1:n // 2].sum()
+        cz = zr[ij, 0] + 2 * zr[ij, 1:n // 2].sum()
+        np.testing.assert_allclose([cx, cy, cz], sc["corr"][ij], rtol=1e-12)
+    np.testing.assert_allclose(0.5 * sc["corr"][[0, 3, 5]].sum(), st["tke"], rtol=1e-12)
+    np.testing.assert_allclose(sc["grdiss"], st["eps"], rtol=1e-12)
+    np.testing.assert_allclose(sc["taak"][0, 0] ** 2, sc["corr"][0] / sc["tmij"][0, 0], rtol=1e-12)
+    assert np.all(sc["lijk"][[0, 3, 5]] > 0)
+    o.close()
