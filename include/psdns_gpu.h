@@ -242,6 +242,13 @@ int psdns_gpu_particles_init(void *ctx, int64_t nop, int32_t pstart, int32_t kip
 int psdns_gpu_write_checkpoint(void *ctx, const char *path, int32_t which);
 int psdns_gpu_read_checkpoint(void *ctx, const char *path);
 
+/* Transfer spectrum (replaces homogeneous/trfsp.f, called at stage 1 of
+ * I/O steps): tk[k-1] = sum over shell k = 1..nx/2 (int(|k|/min(beta) +
+ * 1.5)) of tfact Re(conj(un) . N(u)), with N(u) the convective term
+ * evaluated on the grid shifted by gsh[3] (the step's gsh(:,1); null =
+ * unshifted).  FP64 sums; the state is not changed. */
+int psdns_gpu_transfer_spectrum(void *ctx, const double *gsh, double *tk);
+
 /* One-dimensional spectra and the length/time scales of sptr
  * (homogeneous/sptr.f:119-218, :311-468), FP64: xr, yr, zr [6][nx/2+1] are
  * the normalised spectra along x, y, z of the pairs 11,12,13,22,23,33;

@@ -280,6 +280,8 @@ template <typename T, int N, int NC> struct Impl {
     CK(cudaFuncSetAttribute(k_yfwd<T, N, 1, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
     CK(cudaFuncSetAttribute(k_yfwd<T, N, 2, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
     CK(cudaFuncSetAttribute(k_zinv<T, N, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2()));
+    CK(cudaFuncSetAttribute(k_yfwd<T, N, 0, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(sm5() + sizeof(double) * (N / 2))));
     CK(cudaFuncSetAttribute(k_xmoments<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)KMomLaunch<T, N>::SMEM));
     // the particle path transforms the velocity only (NC = 0 instances)
@@ -353,6 +355,46 @@ template <typename T, int N, int NC> struct Impl {
     // the next step refills its tables from c.gsh; restore the uploaded ones too
     fill_shift_tables<T>(c);
     return upload_tables(c);
+  }
+
+  // trfsp.f: transfer spectrum T(k) = sum over shell k of tfact
+  // Re(conj(un) . N(u)), N the convective term of a stage-1 evaluation on the
+  // grid shifted by gsh (stage-1 shifts of the step; null = unshifted).  The
+  // reference divides w = (dt/2) N by dt/2 (fmult = 2/dt); here the stage
+  // runs with dt/2 = 1.
+  static int transfer(Ctx& c, const double* gsh, double* tk) {
+    double save[3][2];
+    std::memcpy(save, c.gsh, sizeof save);
+    const double dt2 = c.dt2;
+    for (int i = 0; i < 3; i++) c.gsh[i][0] = gsh ? gsh[i] : 0.0;
+    fill_shift_tables<T>(c);
+    int rc = upload_tables(c);
+    std::memcpy(c.gsh, save, sizeof save);
+    if (rc) return 1;
+    c.dt2 = 1.0;
+    rc = stage_a(c, 1);
+    if (!rc) {
+      Geo g = make_geo(c);
+      StageTables<T> st = make_tables<T>(c, 0);
+      st.tdk = std::min(c.p.beta1, std::min(c.p.beta2, c.p.beta3));
+      double* d_tk = (double*)c.d_efkz;   // n/2 + 2 shells of 3 doubles: room for n/2
+      if (cudaMemsetAsync(d_tk, 0, sizeof(double) * (N / 2), c.stream) != cudaSuccess) rc = set_error("memset");
+      if (!rc) {
+        k_yfwd<T, N, 0, NC><<<c.nab_f, K5Launch<T, N, NC>::THREADS, sm5() + sizeof(double) * (N / 2), c.stream>>>(
+            g, st, (const C*)c.d_ub, (C*)c.d_u, (C*)c.d_un, (const C*)c.d_tw, d_tk);
+        if (cudaGetLastError() != cudaSuccess) rc = set_error("transfer launch failed");
+      }
+      if (!rc && (cudaMemcpyAsync(tk, d_tk, sizeof(double) * (N / 2), cudaMemcpyDeviceToHost, c.stream) !=
+                      cudaSuccess ||
+                  cudaStreamSynchronize(c.stream) != cudaSuccess))
+        rc = set_error("transfer copy failed");
+      // efkz is zeroed again by the next forced stage 1
+      if (!rc && cudaMemsetAsync(d_tk, 0, sizeof(double) * (N / 2), c.stream) != cudaSuccess) rc = set_error("memset");
+    }
+    c.dt2 = dt2;
+    fill_shift_tables<T>(c);
+    if (upload_tables(c)) return 1;
+    return rc;
   }
 
   static int twiddles(Ctx& c) {
@@ -432,11 +474,12 @@ struct Ops {
   int (*stage_b)(Ctx&, int);
   int (*particles)(Ctx&);
   int (*moments)(Ctx&, int, const double*, double*);
+  int (*transfer)(Ctx&, const double*, double*);
 };
 
 template <typename T, int N, int NC> static Ops ops_for() {
   using I = Impl<T, N, NC>;
-  return Ops{&I::setup, &I::twiddles, &I::stage_a, &I::stage_b, &I::particles, &I::moments};
+  return Ops{&I::setup, &I::twiddles, &I::stage_a, &I::stage_b, &I::particles, &I::moments, &I::transfer};
 }
 
 template <int N> static Ops ops_n(int prec, int nc) {
@@ -1550,6 +1593,14 @@ int psdns_gpu_gradient_moments(void* ctx, int32_t which, const double* gsh, doub
   Ops o;
   if (!get_ops(c->prec, c->n, c->nc, o)) return set_error("bad context");
   return o.moments(*c, which, gsh, out);
+}
+
+int psdns_gpu_transfer_spectrum(void* ctx, const double* gsh, double* tk) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !tk) return set_error("null argument");
+  Ops o;
+  if (!get_ops(c->prec, c->n, c->nc, o)) return set_error("bad context");
+  return o.transfer(*c, gsh, tk);
 }
 
 int psdns_gpu_spectra_scales(void* ctx, int32_t which, double* xr, double* yr, double* zr, double* stats) {

@@ -57,6 +57,7 @@ template <typename T> struct StageTables {
   // norm is normv[b] (normv null: one box, norm above)
   size_t tbox = 0;
   const T* normv = nullptr;
+  double tdk = 1.0;  // shell width of the transfer spectrum, min(beta) (trfsp.f:43)
 
   __device__ __forceinline__ StageTables at_box(int b) const {
     StageTables t = *this;
@@ -687,7 +688,10 @@ template <typename T, int N, int KSTEP, int NC = 0>
 __global__ void __launch_bounds__(K5Launch<T, N, NC>::THREADS)
 k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __restrict__ u,
        C2<T>* __restrict__ un, const C2<T>* __restrict__ tw_g, double* __restrict__ efkz) {
-  // grid (nab_f, boxes); forcing (efkz) is for single boxes only
+  // grid (nab_f, boxes); forcing (efkz) is for single boxes only.
+  // KSTEP = 0: transfer spectrum only (trfsp.f:62-83): the shell sums of
+  // tfact Re(conj(un) . w) go to efkz[n/2] (shell ik = int(|k|/st.tdk + 1.5));
+  // u and un are not written.
   const int box = blockIdx.y;
   const StageTables<T> st = st_all.at_box(box);
   ub += box * g.bbox;
@@ -704,7 +708,10 @@ k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __rest
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   C* buf = tw + FFTPlan<T, N>::TWSIZE;   // [4][TB] lines
+  double* thist = reinterpret_cast<double*>(buf + NVF * TB * L);   // KSTEP = 0: [n/2] shells
   load_twiddles<T, N>(tw, tw_g);
+  if constexpr (KSTEP == 0)
+    for (int i = threadIdx.x; i < N / 2; i += THREADS) thist[i] = 0.0;
   const int at = blockIdx.x, a0 = at * TB;
   for (int v = 0; v < NVF; v++) {
     constexpr int TBL = Tiles<T>::TBL_F, R = TBL / TB;
@@ -744,10 +751,12 @@ k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __rest
     if (a >= g.xz_tot) continue;
     const size_t o = (size_t)a * N + y;
     if (!mask_ok(g, a, y, N)) {
-      u[o] = cmk<C>(0, 0);
-      u[vs + o] = cmk<C>(0, 0);
-      u[2 * vs + o] = cmk<C>(0, 0);
-      if constexpr (NC > 0) u[3 * vs + o] = cmk<C>(0, 0);
+      if constexpr (KSTEP != 0) {
+        u[o] = cmk<C>(0, 0);
+        u[vs + o] = cmk<C>(0, 0);
+        u[2 * vs + o] = cmk<C>(0, 0);
+        if constexpr (NC > 0) u[3 * vs + o] = cmk<C>(0, 0);
+      }
       continue;
     }
     const int x = __ldg(g.ax + a), z = __ldg(g.az + a);
@@ -769,6 +778,14 @@ k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __rest
     C w3 = cadd(cmul(sxyz, V3), cmul(ut1, V4));
     const bool k0 = (a == 0 && y == 0);
     C n1 = nb[q][0], n2 = nb[q][1], n3 = nb[q][2];
+    if constexpr (KSTEP == 0) {
+      const double term = ((double)n1.x * w1.x + (double)n1.y * w1.y) + ((double)n2.x * w2.x + (double)n2.y * w2.y) +
+                          ((double)n3.x * w3.x + (double)n3.y * w3.y);
+      const double ksq = (double)st.b11 * x * x + (double)st.b22 * iky * iky + (double)st.b33 * ikz * ikz;
+      const int ik = (int)(sqrt(ksq) / st.tdk + 1.5);
+      if (ik >= 1 && ik <= N / 2) atomicAdd(thist + ik - 1, term * (x == 0 ? 1.0 : 2.0));
+      continue;
+    }
     C u1, u2, u3;
     if constexpr (KSTEP == 1) {
       // proc4a.f:427, 479-486
@@ -845,6 +862,11 @@ k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __rest
     }
     u[o] = u1; u[vs + o] = u2; u[2 * vs + o] = u3;
     un[o] = n1; un[vs + o] = n2; un[2 * vs + o] = n3;
+  }
+  if constexpr (KSTEP == 0) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < N / 2; i += THREADS)
+      if (thist[i] != 0.0) atomicAdd(efkz + i, thist[i]);
   }
 }
 

@@ -113,6 +113,19 @@ module psdns_gpu_mod
       type(c_ptr), value :: ctx
       character(kind=c_char), intent(in) :: path(*)
     end function
+    integer(c_int) function psdns_gpu_transfer_spectrum(ctx, gsh, tk) bind(c, name='psdns_gpu_transfer_spectrum')
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: gsh(3)
+      real(c_double), intent(out) :: tk(*)
+    end function
+    integer(c_int) function psdns_gpu_spectra_scales(ctx, which, xr, yr, zr, stats) &
+        bind(c, name='psdns_gpu_spectra_scales')
+      import :: c_int, c_ptr, c_int32_t, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: which
+      real(c_double), intent(out) :: xr(*), yr(*), zr(*), stats(55)
+    end function
     integer(c_int) function psdns_gpu_gradient_moments(ctx, which, gsh, out) &
         bind(c, name='psdns_gpu_gradient_moments')
       import :: c_int, c_ptr, c_int32_t, c_double

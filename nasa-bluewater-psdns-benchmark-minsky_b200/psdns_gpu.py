@@ -27,6 +27,7 @@ FIELD_UN = 1
 
 # every entry point declared in include/psdns_gpu.h
 EXPORTS = (
+    "psdns_gpu_transfer_spectrum",
     "psdns_gpu_spectra_scales",
     "psdns_gpu_particles_init",
     "psdns_gpu_write_checkpoint",
@@ -118,6 +119,7 @@ def load():
     L.psdns_gpu_spectra.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
+    L.psdns_gpu_transfer_spectrum.argtypes = [vp, dp, dp]
     L.psdns_gpu_spectra_scales.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_particles_init.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32]
     L.psdns_gpu_write_checkpoint.argtypes = [vp, ctypes.c_char_p, ctypes.c_int32]
@@ -339,6 +341,13 @@ class Solver:
         out = np.zeros(16, np.float64)
         _check(load().psdns_gpu_gradient_moments(self._ctx, int(which), _dp(g), _dp(out)), "gradient_moments")
         return out[:8].copy(), out[8:].copy()
+
+    def transfer_spectrum(self, gsh=(0.0, 0.0, 0.0)):
+        """trfsp.f: T(k), k = 1..n/2, on the grid shifted by gsh."""
+        g = np.ascontiguousarray(gsh, dtype=np.float64)
+        tk = np.zeros(self.n // 2)
+        _check(load().psdns_gpu_transfer_spectrum(self._ctx, _dp(g), _dp(tk)), "transfer_spectrum")
+        return tk
 
     def spectra_scales(self, which=FIELD_UN):
         """sptr.f one-dimensional spectra ([6, n/2+1] each) and scale statistics."""

@@ -58,6 +58,7 @@ def lib():
         L.orc_spectra.argtypes = [vp, ctypes.c_int, dp, dp, dp, dp]
         L.orc_particles_set.argtypes = [vp, ctypes.c_long, dp]
         L.orc_particles_get.argtypes = [vp, dp, dp]
+        L.orc_transfer_spectrum.argtypes = [vp, dp, dp]
         L.orc_spectra_scales.argtypes = [vp, ctypes.c_int, dp, dp, dp, dp]
         L.orc_particles_init.argtypes = [vp, ctypes.c_long, ctypes.c_int, ctypes.c_int]
         L.orc_gradient_moments.argtypes = [vp, ctypes.c_int, dp, dp]
@@ -212,6 +213,13 @@ class Oracle:
         x = np.zeros(n, np.float64)
         lib().orc_rann2(self._c, int(seq), _dp(x), int(n))
         return x
+
+    def transfer_spectrum(self, gsh=(0.0, 0.0, 0.0)):
+        """trfsp.f: T(k), k = 1..n/2, of u (convective term) against un."""
+        g = np.ascontiguousarray(gsh, dtype=np.float64)
+        tk = np.zeros(self.n // 2)
+        lib().orc_transfer_spectrum(self._c, _dp(g), _dp(tk))
+        return tk
 
     def spectra_scales(self, which=1):
         """sptr.f one-dimensional spectra (xr, yr, zr: [6, n/2+1]) and the

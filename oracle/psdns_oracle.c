@@ -1454,6 +1454,56 @@ void orc_spectra_scales(orc_ctx *c, int which, double *xr, double *yr, double *z
     for (int i = 0; i < 3; i++) *o++ = tmre[i];
 }
 
+/* trfsp.f:62-83,163-170: transfer spectrum of the convective term of u
+ * evaluated as at stage 1 on the grid shifted by gsh[3] (itransform,
+ * realspace, transform, wavespace with dt/2 = 1, i.e. fmult folded in), dotted
+ * with conj(un); tk[k-1], k = 1..n/2. */
+void orc_transfer_spectrum(orc_ctx *c, const double *gsh, double *tk)
+{
+    int n = c->n, tot = c->xz_tot;
+    size_t vs = (size_t)tot * n, np = (size_t)n * n * n;
+    double save[3][2];
+    memcpy(save, c->gsh, sizeof save);
+    double g6[6] = {gsh[0], 0., gsh[1], 0., gsh[2], 0.};
+    orc_set_shifts(c, g6);
+    double dt2 = c->dt2;
+    c->dt2 = 1.0;
+    cx *w = (cx *)calloc(4 * vs, sizeof(cx));
+    memcpy(w, c->u, sizeof(cx) * 3 * vs);
+    phase_shift(c, w, 3, 0);
+    double *p = (double *)malloc(sizeof(double) * 5 * np);
+    itransform(c, w, 3, p);
+    int nc = c->nc;
+    c->nc = 0;                 /* the velocity path only */
+    realspace(c, p, 0);
+    transform(c, p, w);
+    wavespace(c, w, 0);
+    c->nc = nc;
+    free(p);
+    double bmin = sqrt(c->b11);
+    if (sqrt(c->b22) < bmin) bmin = sqrt(c->b22);
+    if (sqrt(c->b33) < bmin) bmin = sqrt(c->b33);
+    for (int k = 0; k < n / 2; k++) tk[k] = 0.;
+    for (int a = 0; a < tot; a++) {
+        int x = c->ax[a], z = c->az[a];
+        double tf = x == 0 ? 1. : 2.;
+        for (int y = 0; y < n; y++) {
+            if (!mask_ok(c, a, y)) continue;
+            size_t o = (size_t)a * n + y;
+            double ksq = c->b11 * c->kx[x] * c->kx[x] + c->b22 * c->ky[y] * c->ky[y] + c->b33 * c->kz[z] * c->kz[z];
+            int ik = (int)(sqrt(ksq) / bmin + 1.5);
+            if (ik < 1 || ik > n / 2) continue;
+            double term = 0.;
+            for (int i = 0; i < 3; i++) term += c->un[i * vs + o].re * w[i * vs + o].re + c->un[i * vs + o].im * w[i * vs + o].im;
+            tk[ik - 1] += term * tf;
+        }
+    }
+    free(w);
+    c->dt2 = dt2;
+    double g6b[6] = {save[0][0], save[0][1], save[1][0], save[1][1], save[2][0], save[2][1]};
+    orc_set_shifts(c, g6b);
+}
+
 /* vgmomt.f:50-143 (itransform.f:222-230, :385): moments of order 1..8 of
  * du/dx and dw/dz on the grid shifted by gsh[3] (the stage-1 shifts of an I/O
  * step), of u (which = 0) or un (which = 1), each sum divided by n^3.

@@ -415,3 +415,28 @@ def test_spectra_scales_match_oracle(oracle_mod, gpu_mod, prec, tol):
             np.testing.assert_allclose(sg[k], so[k], rtol=tol, atol=tol * np.abs(so[k]).max() * 1e-3)
     o.close()
     s.close()
+
+
+@pytest.mark.parametrize("prec,tol", [(1, 1e-10), (0, 1e-4)])
+def test_transfer_spectrum_matches_oracle(oracle_mod, gpu_mod, prec, tol):
+    """trfsp.f transfer spectrum after one step, shifted grid; the state is
+    unchanged by the diagnostic."""
+    n = 32
+    o = oracle_mod.Oracle(n, 0.01, cfl=1.0, kshift=1)
+    un0 = o.field_init(13)
+    o.set_state(un0)
+    s = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=1.0, kshift=1)
+    s.set_state(un0)
+    o.step()
+    s.step()
+    gsh = (0.25, 0.5, 0.8)
+    to = o.transfer_spectrum(gsh)
+    tg = s.transfer_spectrum(gsh)
+    scale = np.abs(to).max()
+    assert np.abs(tg - to).max() < tol * scale
+    o.step()
+    s.step()
+    _, un_o = o.get_state()
+    assert rel_l2(s.get_state(gpu_mod.FIELD_UN), un_o) < (1e-11 if prec == 1 else 2e-5)
+    o.close()
+    s.close()

@@ -324,3 +324,17 @@ def test_spectra_scales_consistency(oracle_mod):
     np.testing.assert_allclose(sc["taak"][0, 0] ** 2, sc["corr"][0] / sc["tmij"][0, 0], rtol=1e-12)
     assert np.all(sc["lijk"][[0, 3, 5]] > 0)
     o.close()
+
+
+def test_transfer_spectrum_conserves_energy(oracle_mod):
+    """The convective term only moves energy between shells: T(k) sums to
+    zero (to the dealiasing error, which the spherical truncation and phase
+    shift keep at roundoff for the energy-conserving rotational form)."""
+    n = 32
+    o = oracle_mod.Oracle(n, 0.01)
+    un = o.field_init(12)
+    o.set_state(un)
+    tk = o.transfer_spectrum((0.3, 0.1, 0.7))
+    assert np.abs(tk).max() > 0
+    assert abs(tk.sum()) < 1e-3 * np.abs(tk).sum()
+    o.close()
