@@ -31,8 +31,18 @@ struct EnsClass {
   bool fixed_dt = true;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
-  int (*stage_a)(EnsClass&, int) = nullptr;
-  int (*stage_b)(EnsClass&, int) = nullptr;
+  int (*stage_a)(EnsClass&, int, int, int) = nullptr;
+  int (*stage_b)(EnsClass&, int, int, int) = nullptr;
+  // boxes per launch of the fixed-dt step (0: all).  A sub-batch runs its
+  // whole step (both stages) before the next starts, so that its work
+  // arrays can stay in the 126 MB L2; the first steps try candidate sizes
+  // (they are real steps: the batching does not change any result) and the
+  // fastest is kept for the captured graph.
+  int sub = 0;
+  bool tuned = false;
+  int trial = -1;
+  std::vector<int> cands;
+  std::vector<float> cand_ms;
 };
 
 struct Ensemble {
@@ -51,9 +61,9 @@ static Geo ens_geo(const EnsClass& e) {
 }
 
 template <typename T>
-static StageTables<T> ens_tables(const EnsClass& e, int ks) {
+static StageTables<T> ens_tables(const EnsClass& e, int ks, int b0) {
   TabLayout<T> L(e.n);
-  const char* b = (const char*)e.d_tabs;
+  const char* b = (const char*)e.d_tabs + (size_t)b0 * e.tab_bytes;
   const psdns_params& p = e.box[0]->p;
   StageTables<T> st;
   st.sx = (const C2<T>*)(b + L.sx[ks]);
@@ -73,7 +83,7 @@ static StageTables<T> ens_tables(const EnsClass& e, int ks) {
   st.norm = T(0);
   st.spf = nullptr;
   st.tbox = e.tab_bytes;
-  st.normv = (const T*)e.d_normv;
+  st.normv = (const T*)e.d_normv + b0;
   return st;
 }
 
@@ -82,35 +92,37 @@ template <typename T, int N> struct EnsImpl {
   using TL = Tiles<T>;
   using I = Impl<T, N, 0>;
 
-  static int stage_a(EnsClass& e, int kstep) {
+  // boxes b0 .. b0 + nb - 1
+  static int stage_a(EnsClass& e, int kstep, int b0, int nb) {
     const Geo g = ens_geo(e);
-    const StageTables<T> st = ens_tables<T>(e, kstep - 1);
+    const StageTables<T> st = ens_tables<T>(e, kstep - 1, b0);
     const C* tw = (const C*)e.d_tw;
-    C* u = (C*)e.d_u;
-    C* ub = (C*)e.d_ub;
-    C* uz = (C*)e.d_uz;
-    const int kxn = e.g.kxn, nb = e.nb;
+    C* u = (C*)e.d_u + (size_t)b0 * e.st_elems;
+    C* ub = (C*)e.d_ub + (size_t)b0 * e.ub_elems;
+    C* uz = (C*)e.d_uz + (size_t)b0 * e.uz_elems;
+    const int kxn = e.g.kxn;
     k_yinv<T, N><<<dim3(k1_blocks<T>(e.nab_i), 3, nb), K1Launch<T, N>::THREADS, I::sm1(), e.stream>>>(g, st, u, ub, tw);
     k_zinv<T, N><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3 * nb), Launch<T, N, TL::XT2>::THREADS, I::sm2(),
                    e.stream>>>(g, ub, uz, tw, st.b11, st.b33);
     k_xchain<T, N><<<dim3(e.nzt, N, nb), K3Launch<T, N, 0>::THREADS, I::sm3(), e.stream>>>(
-        g, uz, tw, st.b11, st.b22, st.b33, e.d_velmax, kstep == 1 ? 1 : 0);
+        g, uz, tw, st.b11, st.b22, st.b33, e.d_velmax + b0, kstep == 1 ? 1 : 0);
     k_zfwd<T, N><<<dim3(N / TL::YT4, (kxn + TL::XT4 - 1) / TL::XT4, nb), K4Launch<T, N>::THREADS, I::sm4(),
                    e.stream>>>(g, uz, ub, tw, st.b11, st.b33);
     CK(cudaGetLastError());
     return 0;
   }
 
-  static int stage_b(EnsClass& e, int kstep) {
+  static int stage_b(EnsClass& e, int kstep, int b0, int nb) {
     const Geo g = ens_geo(e);
-    const StageTables<T> st = ens_tables<T>(e, kstep - 1);
+    const StageTables<T> st = ens_tables<T>(e, kstep - 1, b0);
     constexpr int TH = K5Launch<T, N, 0>::THREADS;
+    const C* ub = (const C*)e.d_ub + (size_t)b0 * e.ub_elems;
+    C* u = (C*)e.d_u + (size_t)b0 * e.st_elems;
+    C* un = (C*)e.d_un + (size_t)b0 * e.st_elems;
     if (kstep == 1)
-      k_yfwd<T, N, 1><<<dim3(e.nab_f, e.nb), TH, I::sm5(), e.stream>>>(g, st, (const C*)e.d_ub, (C*)e.d_u,
-                                                                       (C*)e.d_un, (const C*)e.d_tw, nullptr);
+      k_yfwd<T, N, 1><<<dim3(e.nab_f, nb), TH, I::sm5(), e.stream>>>(g, st, ub, u, un, (const C*)e.d_tw, nullptr);
     else
-      k_yfwd<T, N, 2><<<dim3(e.nab_f, e.nb), TH, I::sm5(), e.stream>>>(g, st, (const C*)e.d_ub, (C*)e.d_u,
-                                                                       (C*)e.d_un, (const C*)e.d_tw, nullptr);
+      k_yfwd<T, N, 2><<<dim3(e.nab_f, nb), TH, I::sm5(), e.stream>>>(g, st, ub, u, un, (const C*)e.d_tw, nullptr);
     CK(cudaGetLastError());
     return 0;
   }
@@ -263,7 +275,12 @@ static int ens_upload_tables(EnsClass& e) {
 static int ens_step_body(EnsClass& e) {
   if (ens_upload_tables(e)) return 1;
   CK(cudaMemsetAsync(e.d_velmax, 0, sizeof(unsigned long long) * e.nb, e.stream));
-  if (e.stage_a(e, 1) || e.stage_b(e, 1) || e.stage_a(e, 2) || e.stage_b(e, 2)) return 1;
+  const int sub = e.sub > 0 ? e.sub : e.nb;
+  for (int b0 = 0; b0 < e.nb; b0 += sub) {
+    const int m = std::min(sub, e.nb - b0);
+    if (e.stage_a(e, 1, b0, m) || e.stage_b(e, 1, b0, m) || e.stage_a(e, 2, b0, m) || e.stage_b(e, 2, b0, m))
+      return 1;
+  }
   CK(cudaMemcpyAsync(e.h_velmax, e.d_velmax, sizeof(unsigned long long) * e.nb, cudaMemcpyDeviceToHost, e.stream));
   return 0;
 }
@@ -284,8 +301,40 @@ static int ens_step_fixed(EnsClass& e) {
   // dt, time and dt2 of the step (step.f:247-262); the Courant check needs
   // this step's velmax and is made after the step
   for (Ctx* c : e.box) step_control(*c);
+  if (!e.tuned) {
+    // tuning steps: one candidate sub-batch size per step, the first twice
+    // (its first run also warms up), timed with events on the class stream
+    if (e.cands.empty()) {
+      for (int s = e.nb; s >= 1; s /= 2) e.cands.push_back(s);
+      e.cand_ms.assign(e.cands.size(), 0.f);
+      ens_fill_factors(e);   // dt is fixed: the factor tables never change
+    }
+    const int t = std::max(0, e.trial);
+    e.sub = e.cands[t];
+    cudaEvent_t t0, t1;
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    CK(cudaEventRecord(t0, e.stream));
+    const int rc = ens_step_body(e);
+    CK(cudaEventRecord(t1, e.stream));
+    CK(cudaEventSynchronize(t1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, t0, t1));
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc) return 1;
+    if (e.trial >= 0) e.cand_ms[t] = ms;
+    e.trial += 1;
+    if (e.trial == (int)e.cands.size()) {
+      int best = 0;
+      for (size_t i = 1; i < e.cands.size(); i++)
+        if (e.cand_ms[i] < e.cand_ms[best]) best = (int)i;
+      e.sub = e.cands[best];
+      e.tuned = true;
+    }
+    return 0;
+  }
   if (!e.gexec) {
-    ens_fill_factors(e);   // dt is fixed: the factor tables never change
     CK(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
     const int rc = ens_step_body(e);
     cudaGraph_t gr = nullptr;
@@ -476,7 +525,7 @@ int psdns_gpu_ensemble_step(void* ens, int32_t nsteps, double* info) {
       ens_fill_shifts(*e);
       if (ens_upload_tables(*e)) return 1;
       CK(cudaMemsetAsync(e->d_velmax, 0, sizeof(unsigned long long) * e->nb, e->stream));
-      if (e->stage_a(*e, 1)) return 1;
+      if (e->stage_a(*e, 1, 0, e->nb)) return 1;
       CK(cudaMemcpyAsync(e->h_velmax, e->d_velmax, sizeof(unsigned long long) * e->nb, cudaMemcpyDeviceToHost,
                          e->stream));
     }
@@ -488,7 +537,7 @@ int psdns_gpu_ensemble_step(void* ens, int32_t nsteps, double* info) {
         if (step_control(*c)) status = 2;
       ens_fill_factors(*e);
       if (ens_upload_tables(*e)) return 1;
-      if (e->stage_b(*e, 1) || e->stage_a(*e, 2) || e->stage_b(*e, 2)) return 1;
+      if (e->stage_b(*e, 1, 0, e->nb) || e->stage_a(*e, 2, 0, e->nb) || e->stage_b(*e, 2, 0, e->nb)) return 1;
     }
     // the pinned tables are refilled next step: wait for every class
     for (EnsClass* e : en->cls) {
