@@ -12,6 +12,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -928,6 +930,40 @@ static int spectra_scales_of(const Geo& g, const void* src, int prec, const psdn
   return 0;
 }
 
+// one variable v of the state <-> the full half-complex layout on the host
+// (complex(8) u(nxh, ny, nz)), staged in uz
+static int full_var_set(Ctx& c, int v, const double* host) {
+  const size_t fs = full_elems(c), vs = (size_t)c.g.xz_tot * c.n;
+  if (fs * sizeof(double2) > c.uz_elems * c.csz) return set_error("full-layout staging does not fit");
+  const Geo g = make_geo(c);
+  CK(cudaMemcpyAsync(c.d_uz, host, sizeof(double2) * fs, cudaMemcpyHostToDevice, c.stream));
+  if (c.prec == PSDNS_PREC_FP64)
+    k_full_to_cyl<double><<<148 * 8, 256, 0, c.stream>>>(g, (const double2*)c.d_uz, (double2*)c.d_un + v * vs,
+                                                           (double2*)c.d_u + v * vs);
+  else
+    k_full_to_cyl<float><<<148 * 8, 256, 0, c.stream>>>(g, (const double2*)c.d_uz, (float2*)c.d_un + v * vs,
+                                                          (float2*)c.d_u + v * vs);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c.stream));
+  return 0;
+}
+
+static int full_var_get(Ctx& c, int which, int v, double* host) {
+  const size_t fs = full_elems(c), vs = (size_t)c.g.xz_tot * c.n;
+  if (fs * sizeof(double2) > c.uz_elems * c.csz) return set_error("full-layout staging does not fit");
+  const Geo g = make_geo(c);
+  const void* src = which == PSDNS_FIELD_U ? c.d_u : c.d_un;
+  CK(cudaMemsetAsync(c.d_uz, 0, sizeof(double2) * fs, c.stream));
+  if (c.prec == PSDNS_PREC_FP64)
+    k_cyl_to_full<double><<<148 * 8, 256, 0, c.stream>>>(g, (const double2*)src + v * vs, (double2*)c.d_uz);
+  else
+    k_cyl_to_full<float><<<148 * 8, 256, 0, c.stream>>>(g, (const float2*)src + v * vs, (double2*)c.d_uz);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, c.d_uz, sizeof(double2) * fs, cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  return 0;
+}
+
 // big-endian Fortran record helpers for the checkpoint files
 static void be32(std::vector<unsigned char>& b, uint32_t v) {
   for (int s = 24; s >= 0; s -= 8) b.push_back((unsigned char)(v >> s));
@@ -1249,21 +1285,27 @@ int psdns_gpu_write_checkpoint(void* ctx, const char* path, int32_t which) {
   if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
   const int n = c->n, nxh = n / 2 + 1, xisz = n / 2;
   const size_t fs = (size_t)nxh * n * n;
-  std::vector<double> full(2 * fs * c->nv);
-  if (psdns_gpu_get_state(ctx, full.data(), which, PSDNS_LAYOUT_FULL)) return 1;
+  // one variable of the full spectrum on the host at a time
+  std::vector<double> full;
+  std::vector<unsigned char> rec, row;
+  try {
+    full.resize(2 * fs);
+    row.resize((size_t)16 * xisz * (n / 2));
+  } catch (const std::bad_alloc&) {
+    return set_error("checkpoint: cannot allocate %.2f GB of host memory", 16.0 * fs / 1e9);
+  }
   FILE* f = std::fopen(path, "wb");
   if (!f) return set_error("cannot open %s for writing", path);
   bool ok = true;
-  std::vector<unsigned char> rec;
-  std::vector<unsigned char> row((size_t)16 * xisz * (n / 2 - 1 + 1));
   for (int v = 0; v < c->nv && ok; v++) {
+    if (full_var_get(*c, which, v, full.data())) { std::fclose(f); return 1; }
     rec.clear();
     for (uint32_t x : {(uint32_t)(v + 1), (uint32_t)n, (uint32_t)n, (uint32_t)n}) be32(rec, x);
     ok = ok && write_record(f, rec.data(), rec.size());
     rec.clear();
     for (uint32_t x : {1u, (uint32_t)xisz, 1u, (uint32_t)n, 1u, (uint32_t)n}) be32(rec, x);
     ok = ok && write_record(f, rec.data(), rec.size());
-    const double* u = full.data() + 2 * fs * v;
+    const double* u = full.data();
     for (int z = 0; z < n && ok; z++) {
       if (z == n / 2) continue;   // nzhp
       for (int half = 0; half < 2 && ok; half++) {
@@ -1289,12 +1331,18 @@ int psdns_gpu_read_checkpoint(void* ctx, const char* path) {
   if (!c || !path) return set_error("null argument");
   const int n = c->n, nxh = n / 2 + 1, xisz = n / 2;
   const size_t fs = (size_t)nxh * n * n;
+  std::vector<double> full;
+  try {
+    full.resize(2 * fs);
+  } catch (const std::bad_alloc&) {
+    return set_error("checkpoint: cannot allocate %.2f GB of host memory", 16.0 * fs / 1e9);
+  }
   FILE* f = std::fopen(path, "rb");
   if (!f) return set_error("cannot open %s", path);
-  std::vector<double> full(2 * fs * c->nv, 0.0);
   std::vector<unsigned char> rec;
   int err = 0;
   for (int v = 0; v < c->nv && !err; v++) {
+    std::fill(full.begin(), full.end(), 0.0);
     if (!read_record(f, rec) || rec.size() != 16) { err = set_error("%s: bad header of variable %d", path, v + 1); break; }
     if ((int)rd_be32(&rec[0]) != v + 1 || (int)rd_be32(&rec[4]) != n || (int)rd_be32(&rec[8]) != n ||
         (int)rd_be32(&rec[12]) != n) {
@@ -1306,7 +1354,7 @@ int psdns_gpu_read_checkpoint(void* ctx, const char* path) {
       err = set_error("%s: not a single-task pencil (xist 1, xisz %d, zjst 1, zjsz %d)", path, xisz, n);
       break;
     }
-    double* u = full.data() + 2 * fs * v;
+    double* u = full.data();
     for (int z = 0; z < n && !err; z++) {
       if (z == n / 2) continue;
       for (int half = 0; half < 2; half++) {
@@ -1325,10 +1373,10 @@ int psdns_gpu_read_checkpoint(void* ctx, const char* path) {
           }
       }
     }
+    if (!err && full_var_set(*c, v, full.data())) err = 1;
   }
   std::fclose(f);
-  if (err) return err;
-  return psdns_gpu_set_state(ctx, full.data(), PSDNS_LAYOUT_FULL);
+  return err;
 }
 
 int psdns_gpu_set_state(void* ctx, const double* un, int32_t layout) {
@@ -1339,19 +1387,8 @@ int psdns_gpu_set_state(void* ctx, const double* un, int32_t layout) {
   if (layout == PSDNS_LAYOUT_FULL) {
     // one variable of the full half-complex array at a time, staged in uz
     const size_t fs = full_elems(*c);
-    if (fs * sizeof(double2) > c->uz_elems * c->csz) return set_error("full-layout staging does not fit");
-    const Geo g = make_geo(*c);
-    for (int v = 0; v < c->nv; v++) {
-      CK(cudaMemcpyAsync(c->d_uz, un + 2 * v * fs, sizeof(double2) * fs, cudaMemcpyHostToDevice, c->stream));
-      if (c->prec == PSDNS_PREC_FP64)
-        k_full_to_cyl<double><<<148 * 8, 256, 0, c->stream>>>(g, (const double2*)c->d_uz,
-                                                               (double2*)c->d_un + v * vs, (double2*)c->d_u + v * vs);
-      else
-        k_full_to_cyl<float><<<148 * 8, 256, 0, c->stream>>>(g, (const double2*)c->d_uz, (float2*)c->d_un + v * vs,
-                                                              (float2*)c->d_u + v * vs);
-      CK(cudaGetLastError());
-    }
-    CK(cudaStreamSynchronize(c->stream));
+    for (int v = 0; v < c->nv; v++)
+      if (full_var_set(*c, v, un + 2 * v * fs)) return 1;
     return 0;
   }
   // stage one variable at a time: ub holds >= 2 variables of complex double
@@ -1379,18 +1416,8 @@ int psdns_gpu_get_state(void* ctx, double* out, int32_t which, int32_t layout) {
   void* src = which == PSDNS_FIELD_U ? c->d_u : c->d_un;
   if (layout == PSDNS_LAYOUT_FULL) {
     const size_t fs = full_elems(*c);
-    if (fs * sizeof(double2) > c->uz_elems * c->csz) return set_error("full-layout staging does not fit");
-    const Geo g = make_geo(*c);
-    for (int v = 0; v < c->nv; v++) {
-      CK(cudaMemsetAsync(c->d_uz, 0, sizeof(double2) * fs, c->stream));
-      if (c->prec == PSDNS_PREC_FP64)
-        k_cyl_to_full<double><<<148 * 8, 256, 0, c->stream>>>(g, (const double2*)src + v * vs, (double2*)c->d_uz);
-      else
-        k_cyl_to_full<float><<<148 * 8, 256, 0, c->stream>>>(g, (const float2*)src + v * vs, (double2*)c->d_uz);
-      CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(out + 2 * v * fs, c->d_uz, sizeof(double2) * fs, cudaMemcpyDeviceToHost, c->stream));
-    }
-    CK(cudaStreamSynchronize(c->stream));
+    for (int v = 0; v < c->nv; v++)
+      if (full_var_get(*c, which, v, out + 2 * v * fs)) return 1;
     return 0;
   }
   for (int v = 0; v < c->nv; v++) {
