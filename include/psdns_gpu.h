@@ -99,6 +99,15 @@ int psdns_gpu_set_state(void *ctx, const double *un, int32_t layout);
  * integral 3/2 (u' = 1); seed starts the ranu stream (PSDNS/ranu.f). */
 int psdns_gpu_field_init(void *ctx, int32_t seed);
 
+/* The sinusoidal initial field of the shipped example runs, kinit(1) = -2
+ * (replaces PSDNS/incond.f:196-209 -> inpvf.f:26-57 -> the hook
+ * PSDNS/hooks/initial_conditions/pfield.f): u = au sin x cos y cos z,
+ * v = av cos x sin y cos z, w = -(au + av) cos x cos y sin z (pfield uses
+ * au = av = 1), transformed with the 1/n^3 forward normalisation; un = u,
+ * other variables zero.  The reference requires zero shifts (kshift = 4)
+ * with this field. */
+int psdns_gpu_field_sinusoidal(void *ctx, double au, double av);
+
 /* Copy u or un back to a host array (complex(8), 3+nc variables). */
 int psdns_gpu_get_state(void *ctx, double *out, int32_t which, int32_t layout);
 

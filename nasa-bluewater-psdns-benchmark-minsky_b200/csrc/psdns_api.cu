@@ -1554,6 +1554,43 @@ int psdns_gpu_field_init(void* ctx, int32_t seed) {
   return 0;
 }
 
+int psdns_gpu_field_sinusoidal(void* ctx, double au, double av) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return set_error("null context");
+  const Geometry& g = c->g;
+  const int n = c->n;
+  if (g.kxn < 2) return set_error("grid too small for the sinusoidal field");
+  // u = au sin x cos y cos z, v = av cos x sin y cos z, w = aw cos x cos y
+  // sin z, aw = -(au + av) (pfield.f:34-78): the modes (+-1, +-1, +-1), of
+  // which the kx = 1 half is stored: u = -i au/8, v = -i sgn(ky) av/8,
+  // w = -i sgn(kz) aw/8; everything else zero
+  const double aw = -(au + av);
+  const size_t vs = (size_t)g.xz_tot * n;
+  CK(cudaMemsetAsync(c->d_u, 0, c->csz * c->st_elems, c->stream));
+  CK(cudaMemsetAsync(c->d_un, 0, c->csz * c->st_elems, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const int kc1 = (g.colstart[2] - g.colstart[1] - 1) / 2;
+  for (int sz = -1; sz <= 1; sz += 2)
+    for (int sy = -1; sy <= 1; sy += 2) {
+      const int a = g.colstart[1] + (sz > 0 ? 1 : 2 * kc1);
+      const int y = sy > 0 ? 1 : n - 1;
+      const double val[3] = {-au / 8., -sy * av / 8., -sz * aw / 8.};   // imaginary parts
+      for (int v = 0; v < 3; v++) {
+        const size_t o = v * vs + (size_t)a * n + y;
+        if (c->prec == PSDNS_PREC_FP64) {
+          const double2 e = make_double2(0.0, val[v]);
+          CK(cudaMemcpy((double2*)c->d_u + o, &e, sizeof e, cudaMemcpyHostToDevice));
+          CK(cudaMemcpy((double2*)c->d_un + o, &e, sizeof e, cudaMemcpyHostToDevice));
+        } else {
+          const float2 e = make_float2(0.f, (float)val[v]);
+          CK(cudaMemcpy((float2*)c->d_u + o, &e, sizeof e, cudaMemcpyHostToDevice));
+          CK(cudaMemcpy((float2*)c->d_un + o, &e, sizeof e, cudaMemcpyHostToDevice));
+        }
+      }
+    }
+  return 0;
+}
+
 int psdns_gpu_particles_set(void* ctx, int64_t np, const double* pos) {
   Ctx* c = (Ctx*)ctx;
   if (!c) return set_error("null context");

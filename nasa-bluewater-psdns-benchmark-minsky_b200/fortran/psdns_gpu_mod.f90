@@ -96,6 +96,11 @@ module psdns_gpu_mod
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
     end function
+    integer(c_int) function psdns_gpu_field_sinusoidal(ctx, au, av) bind(c, name='psdns_gpu_field_sinusoidal')
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), value :: au, av
+    end function
     integer(c_int) function psdns_gpu_particles_init(ctx, nop, pstart, kipran) bind(c, name='psdns_gpu_particles_init')
       import :: c_int, c_ptr, c_int32_t, c_int64_t
       type(c_ptr), value :: ctx

@@ -27,6 +27,7 @@ FIELD_UN = 1
 
 # every entry point declared in include/psdns_gpu.h
 EXPORTS = (
+    "psdns_gpu_field_sinusoidal",
     "psdns_gpu_transfer_spectrum",
     "psdns_gpu_spectra_scales",
     "psdns_gpu_particles_init",
@@ -119,6 +120,7 @@ def load():
     L.psdns_gpu_spectra.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
+    L.psdns_gpu_field_sinusoidal.argtypes = [vp, ctypes.c_double, ctypes.c_double]
     L.psdns_gpu_transfer_spectrum.argtypes = [vp, dp, dp]
     L.psdns_gpu_spectra_scales.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_particles_init.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32]
@@ -287,6 +289,10 @@ class Solver:
     def field_init(self, seed):
         """Random solenoidal field (field.f restated) written to u and un on the device."""
         _check(load().psdns_gpu_field_init(self._ctx, int(seed)), "field_init")
+
+    def field_sinusoidal(self, au=1.0, av=1.0):
+        """pfield.f sinusoidal field u = au sin x cos y cos z, ..."""
+        _check(load().psdns_gpu_field_sinusoidal(self._ctx, float(au), float(av)), "field_sinusoidal")
 
     def stream(self):
         """cudaStream_t (as int) on which the context launches its kernels."""
