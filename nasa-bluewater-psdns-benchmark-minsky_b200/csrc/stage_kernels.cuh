@@ -1009,17 +1009,17 @@ static __global__ void __launch_bounds__(256) k_moments_reduce(const double* __r
 // stencil, and the partial sums are reduced with warp shuffles.
 // first != 0: interpolate only (first step, partsp.f:206).
 // ---------------------------------------------------------------------------
-template <typename V4>
+// spcal_local.f:175-181, :211-231: cell index and cubic B-spline weights
+// along one axis.  jloc = ipx mod n in [0, n) (the reference adds 1000 n to
+// a negative ipx before its modulo), taken as fl - n floor(fl / n): exact in
+// FP64 while |ipx| < 2^52 / n, so bfp has the reference's value bit for bit.
 __device__ __forceinline__ void spline_weights(double pos, double gfn, int n, int& ib, double w[4]) {
-  // spcal_local.f:175-181, :211-231
   const double px1 = pos - gfn;
   const double px = px1 - (double)n;
   const double fl = floor(px);
-  long long ipx = (long long)fl;
-  long long jpx = ipx;
-  if (ipx < 0) jpx = ipx + 1000LL * n;
-  const long long jloc = jpx % n;
-  const double bfp = ((double)jloc + px) - (double)ipx;
+  const double dn = (double)n;
+  const double jloc = fl - dn * floor(fl / dn);
+  const double bfp = (jloc + px) - fl;
   ib = (int)bfp;
   const double t = bfp - ib;
   const double d6 = 1. / 6., tt = 2. / 3.;
@@ -1030,28 +1030,42 @@ __device__ __forceinline__ void spline_weights(double pos, double gfn, int n, in
   w[2] = 1. - w[0] - w[1] - w[3];
 }
 
+// periodic index of stencil point ib + k - 1, k = 0..3 (ib in [0, n])
+__device__ __forceinline__ int wrap_n(int v, int n) {
+  v += (v < 0) ? n : 0;
+  return v - ((v >= n) ? n : 0);
+}
+
+// spcal_local.f:234-367: the 4x4x4 stencil sum of one particle by 16 lanes,
+// lane (jy, jz) summing one x row of 4 points.  A warp instruction touches
+// the stencils of two particles only, which keeps its gathers within a few
+// pages (one thread per particle was 50% slower on random positions).
 template <typename V4>
 __device__ __forceinline__ void spline_interp(const V4* __restrict__ bs, int n, const double p[3],
                                               const double gfn[3], int lane16, unsigned mask16, double out[3]) {
   int ib[3];
   double wx[4], wy[4], wz[4];
-  spline_weights<V4>(p[0], gfn[0], n, ib[0], wx);
-  spline_weights<V4>(p[1], gfn[1], n, ib[1], wy);
-  spline_weights<V4>(p[2], gfn[2], n, ib[2], wz);
+  spline_weights(p[0], gfn[0], n, ib[0], wx);
+  spline_weights(p[1], gfn[1], n, ib[1], wy);
+  spline_weights(p[2], gfn[2], n, ib[2], wz);
   const int jy = lane16 >> 2, jz = lane16 & 3;
   // bs index ib+k (k = 1..4) holds grid point ib+k-2 (splx.f:29-35)
-  const int yy = (ib[1] + jy - 1 + n) % n, zz = (ib[2] + jz - 1 + n) % n;
+  const int yy = wrap_n(ib[1] + jy - 1, n), zz = wrap_n(ib[2] + jz - 1, n);
   const V4* row = bs + ((size_t)yy * n + zz) * n;
+  V4 c[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) c[k] = row[wrap_n(ib[0] + k - 1, n)];
   double sx = 0, sy = 0, sz = 0;
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    const int xx = (ib[0] + k - 1 + n) % n;
-    const V4 c = row[xx];
-    sx += wx[k] * (double)c.x;
-    sy += wx[k] * (double)c.y;
-    sz += wx[k] * (double)c.z;
+    sx += wx[k] * (double)c[k].x;
+    sy += wx[k] * (double)c[k].y;
+    sz += wx[k] * (double)c[k].z;
   }
-  const double wyz = wy[jy] * wz[jz];
+  // register selects (an indexed array would live in local memory)
+  const double wyj = jy == 0 ? wy[0] : jy == 1 ? wy[1] : jy == 2 ? wy[2] : wy[3];
+  const double wzj = jz == 0 ? wz[0] : jz == 1 ? wz[1] : jz == 2 ? wz[2] : wz[3];
+  const double wyz = wyj * wzj;
   sx *= wyz; sy *= wyz; sz *= wyz;
 #pragma unroll
   for (int o = 8; o > 0; o >>= 1) {
@@ -1062,6 +1076,8 @@ __device__ __forceinline__ void spline_interp(const V4* __restrict__ bs, int n, 
   out[0] = sx; out[1] = sy; out[2] = sz;
 }
 
+// Heun step of rk_advpos.f (rk_advpos(1,.5,.5) then rk_advpos(2,0,.5)),
+// 16 lanes per particle
 template <typename T>
 __global__ void __launch_bounds__(256) k_particles(const typename V4T<T>::type* __restrict__ bs, int n, long long np,
                                                    double* __restrict__ pos, double* __restrict__ vel, double g1,
@@ -1077,7 +1093,7 @@ __global__ void __launch_bounds__(256) k_particles(const typename V4T<T>::type* 
       spline_interp(bs, n, x, gfn, lane16, mask16, v);
     } else {
       // rk_advpos(1,.5,.5): pp7 = x + fact1 v, x = pp7 + fact2 v
-      double u0[3] = {vel[m], vel[np + m], vel[2 * np + m]};
+      const double u0[3] = {vel[m], vel[np + m], vel[2 * np + m]};
       double h[3], xs[3], vs[3];
       for (int k = 0; k < 3; k++) { h[k] = x[k] + fact1 * u0[k]; xs[k] = h[k] + fact2 * u0[k]; }
       spline_interp(bs, n, xs, gfn, lane16, mask16, vs);
