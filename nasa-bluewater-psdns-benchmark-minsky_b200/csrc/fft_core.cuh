@@ -337,6 +337,54 @@ __device__ __forceinline__ void fft_lines(C2<T>* buf, int nlines, int ls, const 
   __syncthreads();
 }
 
+// Pass 0 of the plan with operands that the caller supplies from registers:
+// s = begin(l) describes line l, load(s, i) returns its element i (typically
+// a global load, issued for all of a thread's operands before the first
+// butterfly).  Pass 0 has no twiddles; its output goes to the line in shared
+// memory, so the staging copy of the input (a shared-memory write and read
+// per element) disappears.
+template <typename T, int N, int THREADS, typename Begin, typename Load>
+__device__ __forceinline__ void fft_pass0_load(C2<T>* buf, int nlines, int ls, Begin begin, Load load) {
+  using C = C2<T>;
+  using PL = FFTPlan<T, N>;
+  constexpr int R = PL::rad(0), E = PL::E, P = PL::P;
+  constexpr int LPR = THREADS / P;
+  constexpr int NB = E / R;
+  const int lr = threadIdx.x / P, t = threadIdx.x % P;
+  for (int l0 = 0; l0 < nlines; l0 += LPR) {
+    const int l = l0 + lr;
+    if (l < nlines) {
+      const auto s = begin(l);
+      C v[E];
+#pragma unroll
+      for (int q = 0; q < NB; q++)
+#pragma unroll
+        for (int r = 0; r < R; r++) v[q * R + r] = load(s, t + q * P + r * (N / R));
+      C* line = buf + (size_t)l * ls;
+#pragma unroll
+      for (int q = 0; q < NB; q++) {
+        const int j = t + q * P;
+        dft_s<R, 1>(v + q * R);
+#pragma unroll
+        for (int r = 0; r < R; r++) line[pad32(j * R + r)] = v[q * R + r];
+      }
+    }
+  }
+}
+
+// fft_lines with pass 0 fed by fft_pass0_load; waits for the caller's
+// cp.async twiddle copies before the passes that use them.
+template <typename T, int N, int THREADS, typename Begin, typename Load>
+__device__ __forceinline__ void fft_lines_load(C2<T>* buf, int nlines, int ls, const C2<T>* tw, Begin begin,
+                                               Load load) {
+  static_assert(THREADS % FFTPlan<T, N>::P == 0, "THREADS must be a multiple of threads per line");
+  fft_pass0_load<T, N, THREADS>(buf, nlines, ls, begin, load);
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+  fft_passes<T, N, THREADS, 1>(buf, nlines, ls, tw);
+  __syncthreads();
+}
+
 // Host: build the twiddle table of FFTPlan<T,N> (pass p >= 1 table is
 // [r][k] = W_N^(r k N/(Ns R)), r < R, k < Ns; factored passes hold the rows
 // r0 = 0..7 and 8 r1, r1 = 0..R/8-1, see plan_fact).

@@ -192,64 +192,39 @@ k_yinv(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ u, C2<T>* __restr
   const int src = v < 3 ? v : 3;
   const int a0 = at * TB;
   const size_t vs = (size_t)g.xz_tot * N;
-  // the TB columns are contiguous in u: copy them raw, then shift in place
-  const C* col = u + src * vs + (size_t)a0 * N;
-  const int lim = min(TB, g.xz_tot - a0) * N;
-  for (int e = threadIdx.x; e < lim; e += THREADS) cp_async_elem(buf + (e / N) * L + pad32(e % N), col + e);
-  cp_async_wait_all();
-  // shift (and mask, gradient, prefilter) the entries this thread copied;
-  // sxz, fx, fz are constants of column a0 + l
-  auto finish = [&](int l, int y, bool ok, C sxz, T fx, T fz) {
+  // the TB columns are contiguous in u; pass 0 of the transform loads its
+  // operands straight from them, shifted (and masked, differentiated,
+  // prefiltered) in registers; masked entries are not read
+  const C* colbase = u + src * vs + (size_t)a0 * N;
+  struct Col { const C* col; C sxz; T fx, fz; int kym; };
+  auto begin = [&](int l) {
+    Col s{colbase + (size_t)l * N, cmk<C>(0, 0), T(0), T(0), -1};
+    const int a = a0 + l;
+    if (a < g.xz_tot) {
+      const int x = __ldg(g.ax + a), z = __ldg(g.az + a);
+      s.sxz = cmul(__ldg(st.sx + x), __ldg(st.sz + z));
+      s.kym = __ldg(g.kymax + a);
+      if constexpr (SPL) { s.fx = __ldg(st.spf + x); s.fz = __ldg(st.spf + (N / 2 + 1) + N + z); }
+    }
+    return s;
+  };
+  auto load = [&](const Col& s, int y) {
+    const int ky = y > N / 2 ? N - y : y;
     C val = cmk<C>(0, 0);
-    if (ok) {
-      const C sh = cmul(__ldg(st.sy + y), sxz);
-      val = cmul(buf[l * L + pad32(y)], sh);
+    if (y != N / 2 && ky <= s.kym) {
+      const C sh = cmul(__ldg(st.sy + y), s.sxz);
+      val = cmul(__ldg(s.col + y), sh);
       if constexpr (NC > 0) {
         if (v == 4) {
           const T bk = st.b22 * T(kwave<N>(y));
           val = cmk<C>(-bk * val.y, bk * val.x);
         }
       }
-      if constexpr (SPL) val = cscale(fx * __ldg(st.spf + (N / 2 + 1) + y) * fz, val);
+      if constexpr (SPL) val = cscale(s.fx * __ldg(st.spf + (N / 2 + 1) + y) * s.fz, val);
     }
-    buf[l * L + pad32(y)] = cconj(val);
+    return cconj(val);
   };
-  if constexpr (N % THREADS == 0) {
-#pragma unroll
-    for (int l = 0; l < TB; l++) {
-      const int a = a0 + l;
-      C sxz = cmk<C>(0, 0);
-      T fx = T(0), fz = T(0);
-      int kym = -1;
-      if (a < g.xz_tot) {
-        const int x = __ldg(g.ax + a), z = __ldg(g.az + a);
-        sxz = cmul(__ldg(st.sx + x), __ldg(st.sz + z));
-        kym = __ldg(g.kymax + a);
-        if constexpr (SPL) { fx = __ldg(st.spf + x); fz = __ldg(st.spf + (N / 2 + 1) + N + z); }
-      }
-#pragma unroll
-      for (int k = 0; k < N / THREADS; k++) {
-        const int y = threadIdx.x + k * THREADS;
-        const int ky = y > N / 2 ? N - y : y;
-        finish(l, y, y != N / 2 && ky <= kym, sxz, fx, fz);
-      }
-    }
-  } else {
-    for (int e = threadIdx.x; e < TB * N; e += THREADS) {
-      const int l = e / N, y = e % N, a = a0 + l;
-      const bool ok = e < lim && mask_ok(g, a, y, N);
-      C sxz = cmk<C>(0, 0);
-      T fx = T(0), fz = T(0);
-      if (ok) {
-        const int x = __ldg(g.ax + a), z = __ldg(g.az + a);
-        sxz = cmul(__ldg(st.sx + x), __ldg(st.sz + z));
-        if constexpr (SPL) { fx = __ldg(st.spf + x); fz = __ldg(st.spf + (N / 2 + 1) + N + z); }
-      }
-      finish(l, y, ok, sxz, fx, fz);
-    }
-  }
-  __syncthreads();
-  fft_lines<T, N, THREADS>(buf, TB, L, tw);
+  fft_lines_load<T, N, THREADS>(buf, TB, L, tw, begin, load);
   // columns a0 + l sit at ((a / TBL) n + y) TBL + a % TBL of variable v: a
   // block writes 64-byte halves of the 128-byte runs (a sequential pair of
   // groups per block measured slower than independent blocks)
@@ -296,46 +271,33 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
   const int sv = GRAD ? (v == 0 ? 0 : 2) : (v < 3 ? v : (v == 3 ? 4 : 3));
   constexpr int TBL = Tiles<T>::TBL_I;
   const C* src = ub + (size_t)sv * ubi_var_elems<T>(g.nab_i, N);
-  // slot (l, z): column x0 + l holds kz = 0..kc then -kc..-1 (count 2 kc + 1,
-  // mpisetup.f:322-357), so its cylinder index follows from colstart alone.
-  // Cylinder entries are copied raw, the cut band is zeroed, then each
-  // thread conjugates the entries it copied.
-  for (int e = threadIdx.x; e < XT * N; e += THREADS) {
-    const int l = e / N, z = e % N;
-    int kc = -1, ac = 0;
-    if (l < nl) {
-      ac = __ldg(g.colstart + x0 + l);
-      kc = (__ldg(g.colstart + x0 + l + 1) - ac - 1) / 2;
-    }
-    C* p = buf + l * L + pad32(z);
-    if (z <= kc || z >= N - kc) {
-      const int a = ac + (z <= kc ? z : z - N + 2 * kc + 1);
-      cp_async_elem(p, src + ((size_t)((unsigned)a / TBL) * N + y) * TBL + ((unsigned)a % TBL));
-    } else {
-      *p = cmk<C>(0, 0);
-    }
-  }
-  cp_async_wait_all();
-  for (int e = threadIdx.x; e < nl * N; e += THREADS) {
-    const int l = e / N, z = e % N;
-    const int kc = (__ldg(g.colstart + x0 + l + 1) - __ldg(g.colstart + x0 + l) - 1) / 2;
-    if (z <= kc || z >= N - kc) {
-      C* p = buf + l * L + pad32(z);
-      C val = *p;
+  // line l, entry z: column x0 + l holds kz = 0..kc then -kc..-1 (count
+  // 2 kc + 1, mpisetup.f:322-357), so its cylinder index follows from
+  // colstart alone; pass 0 of the transform reads the entries straight from
+  // ub (consecutive z of a warp are consecutive columns), the cut band is zero
+  struct Line { int ac, kc, x; };
+  auto begin = [&](int l) {
+    const int ac = __ldg(g.colstart + x0 + l);
+    return Line{ac, (__ldg(g.colstart + x0 + l + 1) - ac - 1) / 2, x0 + l};
+  };
+  auto load = [&](const Line& s, int z) {
+    C val = cmk<C>(0, 0);
+    if (z <= s.kc || z >= N - s.kc) {
+      const int a = s.ac + (z <= s.kc ? z : z - N + 2 * s.kc + 1);
+      val = __ldg(src + ((size_t)((unsigned)a / TBL) * N + y) * TBL + ((unsigned)a % TBL));
       if constexpr (GRAD) {
-        const T bk = v == 0 ? b11 * T(x0 + l) : b33 * T(kwave<N>(z));
+        const T bk = v == 0 ? b11 * T(s.x) : b33 * T(kwave<N>(z));
         val = cmk<C>(-bk * val.y, bk * val.x);
       } else if constexpr (NC > 0) {
         if (v >= 4) {
-          const T bk = v == 4 ? b11 * T(x0 + l) : b33 * T(kwave<N>(z));
+          const T bk = v == 4 ? b11 * T(s.x) : b33 * T(kwave<N>(z));
           val = cmk<C>(-bk * val.y, bk * val.x);
         }
       }
-      *p = cconj(val);
     }
-  }
-  __syncthreads();
-  fft_lines<T, N, THREADS>(buf, nl, L, tw);
+    return cconj(val);
+  };
+  fft_lines_load<T, N, THREADS>(buf, nl, L, tw, begin, load);
   const size_t vbase = ((size_t)v * N + y) * g.nzt;
   for (int e = threadIdx.x; e < XT * N; e += THREADS) {
     const int zt = e / (XT * TZ), rem = e % (XT * TZ), l = rem / TZ, zz = rem % TZ;
