@@ -16,6 +16,7 @@
 // inter-pass twiddles of pass p are stored as a table [r][k] (k = j mod Ns)
 // so that consecutive threads read consecutive words.
 #pragma once
+#include <type_traits>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -260,6 +261,38 @@ __device__ __forceinline__ void line_sync() {
   }
 }
 
+// Operands of butterfly set q of thread t in one Stockham pass: read from the
+// line, twiddled, transformed in registers (v[q R .. q R + R - 1]).
+template <typename C, int N, int R, int NS, int E, int P, bool FACT>
+__device__ __forceinline__ void pass_butterflies(const C* line, int t, const C* __restrict__ twp, C* v) {
+  constexpr int NB = E / R;
+#pragma unroll
+  for (int q = 0; q < NB; q++) {
+    const int j = t + q * P;
+    const int k = j % NS;
+#pragma unroll
+    for (int r = 0; r < R; r++) v[q * R + r] = line[pad32(j + r * (N / R))];
+    if constexpr (FACT) {
+      C t0[8];
+#pragma unroll
+      for (int r0 = 1; r0 < 8; r0++) t0[r0] = twp[r0 * NS + k];
+#pragma unroll
+      for (int r0 = 1; r0 < 8; r0++) v[q * R + r0] = cmul(v[q * R + r0], t0[r0]);
+#pragma unroll
+      for (int r1 = 1; r1 < R / 8; r1++) {
+        const C t1 = twp[(8 + r1) * NS + k];
+        v[q * R + 8 * r1] = cmul(v[q * R + 8 * r1], t1);
+#pragma unroll
+        for (int r0 = 1; r0 < 8; r0++) v[q * R + 8 * r1 + r0] = cmul(v[q * R + 8 * r1 + r0], cmul(t1, t0[r0]));
+      }
+    } else if constexpr (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; r++) v[q * R + r] = cmul(v[q * R + r], twp[r * NS + k]);
+    }
+    dft_s<R, 1>(v + q * R);
+  }
+}
+
 // One Stockham pass over nlines lines (rounds of LPR lines).
 template <typename C, int N, int R, int NS, int E, int P, int THREADS, bool FACT>
 __device__ __forceinline__ void fft_pass(C* buf, int nlines, int ls, const C* __restrict__ twp) {
@@ -273,33 +306,7 @@ __device__ __forceinline__ void fft_pass(C* buf, int nlines, int ls, const C* __
     const bool act = (lr < LPR) && (l < nlines);
     C v[E];
     C* line = buf + (size_t)l * ls;
-    if (act) {
-#pragma unroll
-      for (int q = 0; q < NB; q++) {
-        const int j = t + q * P;
-        const int k = j % NS;
-#pragma unroll
-        for (int r = 0; r < R; r++) v[q * R + r] = line[pad32(j + r * (N / R))];
-        if constexpr (FACT) {
-          C t0[8];
-#pragma unroll
-          for (int r0 = 1; r0 < 8; r0++) t0[r0] = twp[r0 * NS + k];
-#pragma unroll
-          for (int r0 = 1; r0 < 8; r0++) v[q * R + r0] = cmul(v[q * R + r0], t0[r0]);
-#pragma unroll
-          for (int r1 = 1; r1 < R / 8; r1++) {
-            const C t1 = twp[(8 + r1) * NS + k];
-            v[q * R + 8 * r1] = cmul(v[q * R + 8 * r1], t1);
-#pragma unroll
-            for (int r0 = 1; r0 < 8; r0++) v[q * R + 8 * r1 + r0] = cmul(v[q * R + 8 * r1 + r0], cmul(t1, t0[r0]));
-          }
-        } else if constexpr (NS > 1) {
-#pragma unroll
-          for (int r = 1; r < R; r++) v[q * R + r] = cmul(v[q * R + r], twp[r * NS + k]);
-        }
-        dft_s<R, 1>(v + q * R);
-      }
-    }
+    if (act) pass_butterflies<C, N, R, NS, E, P, FACT>(line, t, twp, v);
     line_sync<P>();
     if (act) {
 #pragma unroll
@@ -383,6 +390,64 @@ __device__ __forceinline__ void fft_lines_load(C2<T>* buf, int nlines, int ls, c
   __syncthreads();
   fft_passes<T, N, THREADS, 1>(buf, nlines, ls, tw);
   __syncthreads();
+}
+
+// The last pass of the plan with its outputs handed to the caller:
+// store(s, base, vals, R, NS) with s = begin(l) receives elements base +
+// r NS (r < R, natural order) of line l in vals[r] (R and NS as
+// std::integral_constant), typically as global stores, so the pass output is
+// not written to shared memory and read back.
+template <typename T, int N, int THREADS, typename Begin, typename Store>
+__device__ __forceinline__ void fft_pass_last_store(const C2<T>* buf, int nlines, int ls, const C2<T>* tw,
+                                                    Begin begin, Store store) {
+  using C = C2<T>;
+  using PL = FFTPlan<T, N>;
+  constexpr int PASS = PL::NPASS - 1;
+  constexpr int R = PL::rad(PASS), NS = PL::ns(PASS), E = PL::E, P = PL::P;
+  constexpr int LPR = THREADS / P, NB = E / R;
+  const int lr = threadIdx.x / P, t = threadIdx.x % P;
+  for (int l0 = 0; l0 < nlines; l0 += LPR) {
+    const int l = l0 + lr;
+    if (l < nlines) {
+      C v[E];
+      pass_butterflies<C, N, R, NS, E, P, PL::fact(PASS)>(buf + (size_t)l * ls, t, tw + PL::twoff(PASS), v);
+      const auto s = begin(l);
+#pragma unroll
+      for (int q = 0; q < NB; q++) {
+        const int j = t + q * P;
+        const int k = j % NS;
+        store(s, (j / NS) * NS * R + k, v + q * R, std::integral_constant<int, R>(),
+              std::integral_constant<int, NS>());
+      }
+    }
+  }
+}
+
+template <typename T, int N, int THREADS, int PASS, int LAST>
+__device__ __forceinline__ void fft_passes_until(C2<T>* buf, int nlines, int ls, const C2<T>* tw) {
+  using PL = FFTPlan<T, N>;
+  if constexpr (PASS < LAST) {
+    constexpr int R = PL::rad(PASS);
+    constexpr int NS = PL::ns(PASS);
+    fft_pass<C2<T>, N, R, NS, PL::E, PL::P, THREADS, PL::fact(PASS)>(buf, nlines, ls, tw + PL::twoff(PASS));
+    fft_passes_until<T, N, THREADS, PASS + 1, LAST>(buf, nlines, ls, tw);
+  }
+}
+
+// Whole transform with pass 0 fed by load (fft_pass0_load) and the last pass
+// handing its outputs to store: shared memory holds only the exchanges
+// between passes.  Needs a plan of two passes or more.
+template <typename T, int N, int THREADS, typename LBegin, typename Load, typename SBegin, typename Store>
+__device__ __forceinline__ void fft_lines_load_store(C2<T>* buf, int nlines, int ls, const C2<T>* tw,
+                                                     LBegin lbegin, Load load, SBegin sbegin, Store store) {
+  using PL = FFTPlan<T, N>;
+  static_assert(PL::NPASS >= 2, "load and store passes must differ");
+  static_assert(THREADS % PL::P == 0, "THREADS must be a multiple of threads per line");
+  fft_pass0_load<T, N, THREADS>(buf, nlines, ls, lbegin, load);
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+  fft_passes_until<T, N, THREADS, 1, PL::NPASS - 1>(buf, nlines, ls, tw);
+  fft_pass_last_store<T, N, THREADS>(buf, nlines, ls, tw, sbegin, store);
 }
 
 // Host: build the twiddle table of FFTPlan<T,N> (pass p >= 1 table is

@@ -54,9 +54,9 @@ void build_geometry(int n, Geometry& g) {
   for (int x = 0; x <= n / 2; x++) g.kx[x] = x;
   for (int y = 0; y < n; y++) g.ky[y] = (y > n / 2) ? y - n : y;
   for (int z = 0; z < n; z++) g.kz[z] = (z > n / 2) ? z - n : z;
-  const int ikmax = (int)((double)n * std::sqrt(2.0) / 3.0);
-  int kxn = ikmax + 1;
-  if (kxn > n / 2) kxn = n / 2;
+  // kxn = min(n/2, (int)(n sqrt(2)/3) + 1) (init.f:29), in integer
+  // arithmetic so that the kernels can use it as a compile-time constant
+  const int kxn = kxn_of(n);
   g.kxn = kxn;
   g.cut.assign(kxn, 0);
   g.colstart.assign(kxn + 1, 0);

@@ -37,6 +37,15 @@ struct Geo {
   size_t sbox = 0, bbox = 0, zbox = 0;
 };
 
+// kx columns kept for a box of n: kxn = min(n/2, floor(kmax) + 1) with kmax
+// = sqrt(2) n / 3 (init.f:29); floor(sqrt(2) n / 3) is the largest m with
+// 9 m^2 <= 2 n^2.  A compile-time constant of the kernels' template n.
+__host__ __device__ constexpr int kxn_of(int n) {
+  int m = 0;
+  while (9LL * (m + 1) * (m + 1) <= 2LL * n * n) m++;
+  return m + 1 < n / 2 ? m + 1 : n / 2;
+}
+
 template <typename T> struct StageTables {
   const C2<T>* sx;   // [n/2+1] shift factors of this stage
   const C2<T>* sy;   // [n]
@@ -297,12 +306,20 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
     }
     return cconj(val);
   };
-  fft_lines_load<T, N, THREADS>(buf, nl, L, tw, begin, load);
+  // the last pass stores its outputs straight to uz: line l, entry z at
+  // ((v n + y) nzt + z / TZ) kxn + x0 + l) TZ + z % TZ (consecutive z of a
+  // warp fill whole 32-byte sectors)
   const size_t vbase = ((size_t)v * N + y) * g.nzt;
-  for (int e = threadIdx.x; e < XT * N; e += THREADS) {
-    const int zt = e / (XT * TZ), rem = e % (XT * TZ), l = rem / TZ, zz = rem % TZ;
-    if (l < nl) uz[((vbase + zt) * g.kxn + x0 + l) * TZ + zz] = cconj(buf[l * L + pad32(zt * TZ + zz)]);
-  }
+  constexpr size_t zstride = (size_t)kxn_of(N) * TZ;   // g.kxn, as a constant
+  auto sbegin = [&](int l) { return uz + (vbase * g.kxn + x0 + l) * TZ; };
+  auto store = [&](C* d, int base, const C* vals, auto Rc, auto NSc) {
+    constexpr int R = decltype(Rc)::value, NS = decltype(NSc)::value;
+    static_assert(NS % TZ == 0, "last-pass stride must keep z % TZ");
+    C* p = d + ((unsigned)base / TZ) * zstride + (unsigned)base % TZ;
+#pragma unroll
+    for (int r = 0; r < R; r++) p[(size_t)(r * (NS / TZ)) * zstride] = cconj(vals[r]);
+  };
+  fft_lines_load_store<T, N, THREADS>(buf, nl, L, tw, begin, load, sbegin, store);
 }
 
 // ---------------------------------------------------------------------------

@@ -31,7 +31,10 @@ def test_library_exports_every_declared_symbol(gpu_mod):
 
 
 def test_geometry_entry_point(gpu_mod, oracle_mod):
-    for n in (16, 64, 256):
+    # kxn = min(n/2, (int)(n sqrt(2)/3) + 1) (init.f:29) for every compiled n
+    for n in (16, 32, 48, 64, 96, 128, 256, 512, 1024):
+        assert gpu_mod.geometry(n)["kxn"] == min(n // 2, int(n * np.sqrt(2) / 3) + 1)
+    for n in (16, 48, 64, 96, 256):
         g = gpu_mod.geometry(n)
         o = oracle_mod.Oracle(n, 0.01, kshift=4)
         og = o.geometry()
