@@ -345,13 +345,15 @@ __device__ __forceinline__ void fft_lines(C2<T>* buf, int nlines, int ls, const 
 }
 
 // Pass 0 of the plan with operands that the caller supplies from registers:
-// s = begin(l) describes line l, load(s, i) returns its element i (typically
-// a global load, issued for all of a thread's operands before the first
-// butterfly).  Pass 0 has no twiddles; its output goes to the line in shared
-// memory, so the staging copy of the input (a shared-memory write and read
-// per element) disappears.
-template <typename T, int N, int THREADS, typename Begin, typename Load>
-__device__ __forceinline__ void fft_pass0_load(C2<T>* buf, int nlines, int ls, Begin begin, Load load) {
+// s = begin(l) describes line l, fetch(s, i) loads its element i (typically
+// a predicated global load) and fix(s, i, raw) turns the raw value into the
+// operand (shift, mask, derivative ...).  A thread issues the fetches of all
+// its operands before the first fix, so that its loads are in flight
+// together whatever branches fix takes.  Pass 0 has no twiddles; its output
+// goes to the line in shared memory, so the staging copy of the input (a
+// shared-memory write and read per element) disappears.
+template <typename T, int N, int THREADS, typename Begin, typename Fetch, typename Fix>
+__device__ __forceinline__ void fft_pass0_load(C2<T>* buf, int nlines, int ls, Begin begin, Fetch fetch, Fix fix) {
   using C = C2<T>;
   using PL = FFTPlan<T, N>;
   constexpr int R = PL::rad(0), E = PL::E, P = PL::P;
@@ -366,7 +368,11 @@ __device__ __forceinline__ void fft_pass0_load(C2<T>* buf, int nlines, int ls, B
 #pragma unroll
       for (int q = 0; q < NB; q++)
 #pragma unroll
-        for (int r = 0; r < R; r++) v[q * R + r] = load(s, t + q * P + r * (N / R));
+        for (int r = 0; r < R; r++) v[q * R + r] = fetch(s, t + q * P + r * (N / R));
+#pragma unroll
+      for (int q = 0; q < NB; q++)
+#pragma unroll
+        for (int r = 0; r < R; r++) v[q * R + r] = fix(s, t + q * P + r * (N / R), v[q * R + r]);
       C* line = buf + (size_t)l * ls;
 #pragma unroll
       for (int q = 0; q < NB; q++) {
@@ -381,11 +387,11 @@ __device__ __forceinline__ void fft_pass0_load(C2<T>* buf, int nlines, int ls, B
 
 // fft_lines with pass 0 fed by fft_pass0_load; waits for the caller's
 // cp.async twiddle copies before the passes that use them.
-template <typename T, int N, int THREADS, typename Begin, typename Load>
+template <typename T, int N, int THREADS, typename Begin, typename Fetch, typename Fix>
 __device__ __forceinline__ void fft_lines_load(C2<T>* buf, int nlines, int ls, const C2<T>* tw, Begin begin,
-                                               Load load) {
+                                               Fetch fetch, Fix fix) {
   static_assert(THREADS % FFTPlan<T, N>::P == 0, "THREADS must be a multiple of threads per line");
-  fft_pass0_load<T, N, THREADS>(buf, nlines, ls, begin, load);
+  fft_pass0_load<T, N, THREADS>(buf, nlines, ls, begin, fetch, fix);
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   fft_passes<T, N, THREADS, 1>(buf, nlines, ls, tw);
@@ -434,16 +440,18 @@ __device__ __forceinline__ void fft_passes_until(C2<T>* buf, int nlines, int ls,
   }
 }
 
-// Whole transform with pass 0 fed by load (fft_pass0_load) and the last pass
+// Whole transform with pass 0 fed by fetch and fix (fft_pass0_load) and the last pass
 // handing its outputs to store: shared memory holds only the exchanges
 // between passes.  Needs a plan of two passes or more.
-template <typename T, int N, int THREADS, typename LBegin, typename Load, typename SBegin, typename Store>
+template <typename T, int N, int THREADS, typename LBegin, typename Fetch, typename Fix, typename SBegin,
+          typename Store>
 __device__ __forceinline__ void fft_lines_load_store(C2<T>* buf, int nlines, int ls, const C2<T>* tw,
-                                                     LBegin lbegin, Load load, SBegin sbegin, Store store) {
+                                                     LBegin lbegin, Fetch fetch, Fix fix, SBegin sbegin,
+                                                     Store store) {
   using PL = FFTPlan<T, N>;
   static_assert(PL::NPASS >= 2, "load and store passes must differ");
   static_assert(THREADS % PL::P == 0, "THREADS must be a multiple of threads per line");
-  fft_pass0_load<T, N, THREADS>(buf, nlines, ls, lbegin, load);
+  fft_pass0_load<T, N, THREADS>(buf, nlines, ls, lbegin, fetch, fix);
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   fft_passes_until<T, N, THREADS, 1, PL::NPASS - 1>(buf, nlines, ls, tw);

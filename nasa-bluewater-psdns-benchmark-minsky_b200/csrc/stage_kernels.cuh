@@ -217,23 +217,28 @@ k_yinv(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ u, C2<T>* __restr
     }
     return s;
   };
-  auto load = [&](const Col& s, int y) {
+  // fetch: the shifted entry (zero where masked); fix: derivative, prefilter
+  // and the conjugation of the backward transform (zero stays zero)
+  auto fetch = [&](const Col& s, int y) {
     const int ky = y > N / 2 ? N - y : y;
     C val = cmk<C>(0, 0);
     if (y != N / 2 && ky <= s.kym) {
       const C sh = cmul(__ldg(st.sy + y), s.sxz);
       val = cmul(__ldg(s.col + y), sh);
-      if constexpr (NC > 0) {
-        if (v == 4) {
-          const T bk = st.b22 * T(kwave<N>(y));
-          val = cmk<C>(-bk * val.y, bk * val.x);
-        }
-      }
-      if constexpr (SPL) val = cscale(s.fx * __ldg(st.spf + (N / 2 + 1) + y) * s.fz, val);
     }
+    return val;
+  };
+  auto fix = [&](const Col& s, int y, C val) {
+    if constexpr (NC > 0) {
+      if (v == 4) {
+        const T bk = st.b22 * T(kwave<N>(y));
+        val = cmk<C>(-bk * val.y, bk * val.x);
+      }
+    }
+    if constexpr (SPL) val = cscale(s.fx * __ldg(st.spf + (N / 2 + 1) + y) * s.fz, val);
     return cconj(val);
   };
-  fft_lines_load<T, N, THREADS>(buf, TB, L, tw, begin, load);
+  fft_lines_load<T, N, THREADS>(buf, TB, L, tw, begin, fetch, fix);
   // columns a0 + l sit at ((a / TBL) n + y) TBL + a % TBL of variable v: a
   // block writes 64-byte halves of the 128-byte runs (a sequential pair of
   // groups per block measured slower than independent blocks)
@@ -289,19 +294,19 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
     const int ac = __ldg(g.colstart + x0 + l);
     return Line{ac, (__ldg(g.colstart + x0 + l + 1) - ac - 1) / 2, x0 + l};
   };
-  auto load = [&](const Line& s, int z) {
-    C val = cmk<C>(0, 0);
-    if (z <= s.kc || z >= N - s.kc) {
-      const int a = s.ac + (z <= s.kc ? z : z - N + 2 * s.kc + 1);
-      val = __ldg(src + ((size_t)((unsigned)a / TBL) * N + y) * TBL + ((unsigned)a % TBL));
-      if constexpr (GRAD) {
-        const T bk = v == 0 ? b11 * T(s.x) : b33 * T(kwave<N>(z));
+  auto fetch = [&](const Line& s, int z) {
+    if (z > s.kc && z < N - s.kc) return cmk<C>(0, 0);
+    const int a = s.ac + (z <= s.kc ? z : z - N + 2 * s.kc + 1);
+    return __ldg(src + ((size_t)((unsigned)a / TBL) * N + y) * TBL + ((unsigned)a % TBL));
+  };
+  auto fix = [&](const Line& s, int z, C val) {
+    if constexpr (GRAD) {
+      const T bk = v == 0 ? b11 * T(s.x) : b33 * T(kwave<N>(z));
+      val = cmk<C>(-bk * val.y, bk * val.x);
+    } else if constexpr (NC > 0) {
+      if (v >= 4) {
+        const T bk = v == 4 ? b11 * T(s.x) : b33 * T(kwave<N>(z));
         val = cmk<C>(-bk * val.y, bk * val.x);
-      } else if constexpr (NC > 0) {
-        if (v >= 4) {
-          const T bk = v == 4 ? b11 * T(s.x) : b33 * T(kwave<N>(z));
-          val = cmk<C>(-bk * val.y, bk * val.x);
-        }
       }
     }
     return cconj(val);
@@ -319,7 +324,7 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
 #pragma unroll
     for (int r = 0; r < R; r++) p[(size_t)(r * (NS / TZ)) * zstride] = cconj(vals[r]);
   };
-  fft_lines_load_store<T, N, THREADS>(buf, nl, L, tw, begin, load, sbegin, store);
+  fft_lines_load_store<T, N, THREADS>(buf, nl, L, tw, begin, fetch, fix, sbegin, store);
 }
 
 // ---------------------------------------------------------------------------
