@@ -347,24 +347,37 @@ def main():
             barrier()
             f0 = torch.cuda.Event(enable_timing=True)
             f1 = torch.cuda.Event(enable_timing=True)
-            f0.record(stream)
             # each step: upload the state from pinned memory, step, download
             # the new state to the same buffer; the asynchronous calls let an
-            # upload overlap the previous download chunk by chunk
-            for _ in range(args.e2e_steps):
-                s.set_state_async_ptr(ptr)
-                s.step()
-                s.get_state_async_ptr(ptr)
-            s.sync()
-            f1.record(stream)
-            f1.synchronize()
-            ems = f0.elapsed_time(f1) / args.e2e_steps
-            if dist is not None:
-                t = torch.tensor([ems], dtype=torch.float64, device="cuda")
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
-                ems = float(t.item())
-            e2e = {"value": world * n ** 3 / (ems * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": nbytes,
-                   "d2h_bytes_per_step": nbytes, "ms_per_step": ems, "steps": args.e2e_steps}
+            # upload overlap the previous download chunk by chunk.  Headline:
+            # the sphere copies (the entries inside the truncation sphere,
+            # which are all the step reads and writes); beside it the copies
+            # of the whole reference-layout array.
+            def timed(up, down):
+                barrier()
+                f0.record(stream)
+                for _ in range(args.e2e_steps):
+                    up(ptr)
+                    s.step()
+                    down(ptr)
+                s.sync()
+                f1.record(stream)
+                f1.synchronize()
+                ems = f0.elapsed_time(f1) / args.e2e_steps
+                if dist is not None:
+                    t = torch.tensor([ems], dtype=torch.float64, device="cuda")
+                    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                    ems = float(t.item())
+                return ems
+            ems_full = timed(s.set_state_async_ptr, s.get_state_async_ptr)
+            ems = timed(s.set_state_sphere_async_ptr, s.get_state_sphere_async_ptr)
+            # entries per variable inside the truncation sphere (masks.f)
+            sphere_bytes = int(P.sphere_mask(n).sum()) * (3 + args.nc) * 16
+            e2e = {"value": world * n ** 3 / (ems * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": sphere_bytes,
+                   "d2h_bytes_per_step": sphere_bytes, "ms_per_step": ems, "steps": args.e2e_steps,
+                   "copies": "entries inside the truncation sphere, pinned host memory read and written by kernels",
+                   "full_array": {"value": world * n ** 3 / (ems_full * 1e-3) / 1e9, "ms_per_step": ems_full,
+                                  "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}}
             del host
         except Exception as ex:  # pinned allocation may exceed host memory
             e2e = {"value": None, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,

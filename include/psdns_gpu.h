@@ -80,6 +80,11 @@ int psdns_gpu_default_params(psdns_params *p);
 int psdns_gpu_geometry(int32_t n, int32_t *kxn, int32_t *xz_tot,
                        int32_t *cut_z, int32_t *colstart);
 
+/* The spherical mask of that geometry (PSDNS/masks.f:46-83) as the largest
+ * kept |ky| per cylinder column: entry y of column a is inside when
+ * y != n/2 and min(y, n-y) <= kymax[a] (array of xz_tot ints). */
+int psdns_gpu_kymax(int32_t n, int32_t *kymax);
+
 /* Create a context: validate parameters, build the cylinder map and the
  * spherical mask (PSDNS/masks.f), allocate the device state and work
  * arrays, and build twiddle tables.  Replaces the set-up calls of
@@ -121,6 +126,19 @@ int psdns_gpu_get_state(void *ctx, double *out, int32_t which, int32_t layout);
  * range of a pending download reads each chunk after it has landed. */
 int psdns_gpu_set_state_async(void *ctx, const double *un, int32_t layout);
 int psdns_gpu_get_state_async(void *ctx, double *out, int32_t which, int32_t layout);
+/* Asynchronous copies of the entries inside the truncation sphere only
+ * (PSDNS_LAYOUT_YCYL; the mask of PSDNS/masks.f:46-83: y != ny/2 and
+ * min(y, ny-y) <= kymax of the column, the entries the path reads and
+ * writes; every other entry of the reference's uy array is zero there).
+ * The host array must be pinned (cudaHostAlloc or cudaHostRegister): kernels
+ * read or write it directly over the bus, 63% of the bytes of the full
+ * array, with no device staging.  Entries outside the sphere are neither
+ * read nor written.  An upload issued right after a download of the same
+ * array overlaps it chunk by chunk; work on the state issued afterwards is
+ * ordered after the upload, and any other call first waits for a pending
+ * download.  The host array must stay untouched until psdns_gpu_sync. */
+int psdns_gpu_set_state_sphere_async(void *ctx, const double *un);
+int psdns_gpu_get_state_sphere_async(void *ctx, double *out, int32_t which);
 /* Wait for every copy and kernel of the context. */
 int psdns_gpu_sync(void *ctx);
 

@@ -180,6 +180,13 @@ struct Ctx {
   const char* pend_out = nullptr;    // host range of the last get_state_async
   size_t pend_out_bytes = 0;
   bool in_pending = false;
+  // sphere-only copies (pinned host memory read and written by kernels):
+  // the downloads run on s_out after ev_ready; an upload that directly
+  // follows a download waits for it chunk by chunk
+  cudaEvent_t ev_ready = nullptr;
+  long long api_calls = 0, sphere_get_call = -1;
+  bool sphere_get_pending = false;
+  bool pend_sphere = false;          // the pending download was a sphere copy
   double prof_ms[6] = {0, 0, 0, 0, 0, 0};
   long long prof_n[6] = {0, 0, 0, 0, 0, 0};
   bool prof_pending[2] = {false, false};
@@ -798,18 +805,35 @@ static int spectra_of(const Geo& g, const void* src, int prec, const psdns_param
 // A chunk of set_state_async whose host range is that of a pending
 // get_state_async waits only for that chunk's download.
 // ---------------------------------------------------------------------------
-static int async_setup(Ctx& c) {
+// Every entry point on a context calls touch first: a sphere download still
+// reading the state on s_out is joined into the context stream before any
+// other work, except by the sphere upload, which waits for it chunk by chunk.
+static void touch(Ctx* c, bool sphere_upload = false) {
+  if (!c) return;
+  c->api_calls++;
+  if (c->sphere_get_pending && !sphere_upload) {
+    for (int k = 0; k < Ctx::kChunks; k++) cudaStreamWaitEvent(c->stream, c->ev_d2h[k], 0);
+    c->sphere_get_pending = false;
+  }
+}
+
+// copy streams and events; with staging, also the complex(8) staging
+// buffers of the full-array copies (the sphere copies need none)
+static int async_setup(Ctx& c, bool staging = true) {
+  if (staging && !c.d_in_stage) {
+    const size_t bytes = sizeof(double2) * c.st_elems;
+    size_t freeb = 0, totb = 0;
+    CK(cudaMemGetInfo(&freeb, &totb));
+    if (2 * bytes + (size_t)256 * 1024 * 1024 > freeb)
+      return set_error("asynchronous state copies need %.2f GB of staging, %.2f GB free", 2 * bytes / 1e9,
+                       freeb / 1e9);
+    CK(cudaMalloc(&c.d_in_stage, bytes));
+    CK(cudaMalloc(&c.d_out_stage, bytes));
+  }
   if (c.s_in) return 0;
-  const size_t bytes = sizeof(double2) * c.st_elems;
-  size_t freeb = 0, totb = 0;
-  CK(cudaMemGetInfo(&freeb, &totb));
-  if (2 * bytes + (size_t)256 * 1024 * 1024 > freeb)
-    return set_error("asynchronous state copies need %.2f GB of staging, %.2f GB free", 2 * bytes / 1e9,
-                     freeb / 1e9);
-  CK(cudaMalloc(&c.d_in_stage, bytes));
-  CK(cudaMalloc(&c.d_out_stage, bytes));
   CK(cudaStreamCreateWithFlags(&c.s_in, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&c.s_out, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&c.ev_ready, cudaEventDisableTiming));
   for (int k = 0; k < Ctx::kChunks; k++) {
     CK(cudaEventCreateWithFlags(&c.ev_h2d[k], cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&c.ev_conv_in[k], cudaEventDisableTiming));
@@ -1045,6 +1069,15 @@ int psdns_gpu_geometry(int32_t n, int32_t* kxn, int32_t* xz_tot, int32_t* cut_z,
   return 0;
 }
 
+int psdns_gpu_kymax(int32_t n, int32_t* kymax) {
+  if (n < 8 || (n & 1)) return set_error("grid size %d not supported", n);
+  if (!kymax) return set_error("null argument");
+  Geometry g;
+  build_geometry(n, g);
+  for (int a = 0; a < g.xz_tot; a++) kymax[a] = g.kymax[a];
+  return 0;
+}
+
 int psdns_gpu_init(const psdns_params* p, void** out) {
   if (!p || !out) return set_error("null argument");
   *out = nullptr;
@@ -1156,6 +1189,7 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
 
 int psdns_gpu_finalize(void* ctx) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return 0;
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->d_colstart, c->d_ax, c->d_az, c->d_kymax, c->d_tw, c->d_tabs, c->d_u, c->d_un,
@@ -1173,6 +1207,7 @@ int psdns_gpu_finalize(void* ctx) {
     for (cudaEvent_t* e : evs)
       if (*e) cudaEventDestroy(*e);
   }
+  if (c->ev_ready) cudaEventDestroy(c->ev_ready);
   if (c->d_in_stage) cudaFree(c->d_in_stage);
   if (c->d_out_stage) cudaFree(c->d_out_stage);
   if (c->s_in) cudaStreamDestroy(c->s_in);
@@ -1187,12 +1222,14 @@ int psdns_gpu_finalize(void* ctx) {
 
 int psdns_gpu_set_state_async(void* ctx, const double* un, int32_t layout) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c || !un) return set_error("null argument");
   if (layout != PSDNS_LAYOUT_YCYL) return set_error("asynchronous state copies use PSDNS_LAYOUT_YCYL");
   if (async_setup(*c)) return 1;
   const char* h = (const char*)un;
   const size_t bytes = sizeof(double2) * c->st_elems;
-  const bool same = c->pend_out == h && c->pend_out_bytes == bytes;
+  // chunks of a pending sphere download do not match these chunks
+  const bool same = c->pend_out == h && c->pend_out_bytes == bytes && !c->pend_sphere;
   const bool overlap = c->pend_out && h < c->pend_out + c->pend_out_bytes && c->pend_out < h + bytes;
   double2* stage = (double2*)c->d_in_stage;
   for (int k = 0; k < Ctx::kChunks; k++) {
@@ -1225,6 +1262,7 @@ int psdns_gpu_set_state_async(void* ctx, const double* un, int32_t layout) {
 
 int psdns_gpu_get_state_async(void* ctx, double* out, int32_t which, int32_t layout) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c || !out) return set_error("null argument");
   if (layout != PSDNS_LAYOUT_YCYL) return set_error("asynchronous state copies use PSDNS_LAYOUT_YCYL");
   if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
@@ -1251,11 +1289,116 @@ int psdns_gpu_get_state_async(void* ctx, double* out, int32_t which, int32_t lay
   }
   c->pend_out = (const char*)out;
   c->pend_out_bytes = sizeof(double2) * c->st_elems;
+  c->pend_sphere = false;
+  return 0;
+}
+
+// device address of pinned (page-locked, mapped) host memory, or an error
+static int mapped_host(const void* p, void** dptr) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error("host array: pointer attributes unavailable");
+  }
+  if (at.type != cudaMemoryTypeHost || !at.devicePointer)
+    return set_error("sphere copies need pinned host memory (cudaHostAlloc or cudaHostRegister)");
+  *dptr = at.devicePointer;
+  return 0;
+}
+
+// columns of chunk k of the sphere copies
+static void sphere_chunk(const Ctx& c, int k, int& a0, int& a1) {
+  const long long tot = c.g.xz_tot;
+  a0 = (int)(tot * k / Ctx::kChunks);
+  a1 = (int)(tot * (k + 1) / Ctx::kChunks);
+}
+
+int psdns_gpu_set_state_sphere_async(void* ctx, const double* un) {
+  Ctx* c = (Ctx*)ctx;
+  touch(c, true);
+  if (!c || !un) return set_error("null argument");
+  if (async_setup(*c, false)) return 1;
+  void* dh = nullptr;
+  if (mapped_host(un, &dh)) return 1;
+  // directly after a sphere download: that download already waited for the
+  // state (ev_ready), and chunk k waits for its chunk k only; otherwise wait
+  // for everything enqueued so far
+  const bool follow = c->sphere_get_pending && c->sphere_get_call == c->api_calls - 1;
+  if (!follow) {
+    if (c->sphere_get_pending)
+      for (int k = 0; k < Ctx::kChunks; k++) CK(cudaStreamWaitEvent(c->s_in, c->ev_d2h[k], 0));
+    CK(cudaEventRecord(c->ev_ready, c->stream));
+  }
+  if (c->pend_out && !c->sphere_get_pending)   // a pending full-array download
+    for (int k = 0; k < Ctx::kChunks; k++) CK(cudaStreamWaitEvent(c->s_in, c->ev_d2h[k], 0));
+  CK(cudaStreamWaitEvent(c->s_in, c->ev_ready, 0));
+  const Geo g = make_geo(*c);
+  for (int k = 0; k < Ctx::kChunks; k++) {
+    int a0, a1;
+    sphere_chunk(*c, k, a0, a1);
+    if (follow) CK(cudaStreamWaitEvent(c->s_in, c->ev_d2h[k], 0));
+    if (a1 > a0) {
+      // two blocks per SM (reads wait on the bus), leaving room for the
+      // download of another chunk beside it
+      const int blocks = std::min(2 * 148, (a1 - a0 + 7) / 8);
+      if (c->prec == PSDNS_PREC_FP64)
+        k_sphere_in<double><<<blocks, 256, 0, c->s_in>>>(g, c->nv, (const double2*)dh, (double2*)c->d_un,
+                                                         (double2*)c->d_u, a0, a1);
+      else
+        k_sphere_in<float><<<blocks, 256, 0, c->s_in>>>(g, c->nv, (const double2*)dh, (float2*)c->d_un,
+                                                        (float2*)c->d_u, a0, a1);
+      CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(c->ev_h2d[k], c->s_in));
+    CK(cudaStreamWaitEvent(c->stream, c->ev_h2d[k], 0));
+  }
+  // the context stream now follows every chunk, and so every download chunk
+  c->sphere_get_pending = false;
+  c->pend_out = nullptr;
+  c->pend_out_bytes = 0;
+  return 0;
+}
+
+int psdns_gpu_get_state_sphere_async(void* ctx, double* out, int32_t which) {
+  Ctx* c = (Ctx*)ctx;
+  touch(c);
+  if (!c || !out) return set_error("null argument");
+  if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
+  if (async_setup(*c, false)) return 1;
+  void* dh = nullptr;
+  if (mapped_host(out, &dh)) return 1;
+  // a pending full-array download of the staging buffers must not be
+  // overtaken; the state is ready when the context stream reaches ev_ready
+  if (c->pend_out)
+    for (int k = 0; k < Ctx::kChunks; k++) CK(cudaStreamWaitEvent(c->s_out, c->ev_d2h[k], 0));
+  CK(cudaEventRecord(c->ev_ready, c->stream));
+  CK(cudaStreamWaitEvent(c->s_out, c->ev_ready, 0));
+  const Geo g = make_geo(*c);
+  const void* src = which == PSDNS_FIELD_U ? c->d_u : c->d_un;
+  for (int k = 0; k < Ctx::kChunks; k++) {
+    int a0, a1;
+    sphere_chunk(*c, k, a0, a1);
+    if (a1 > a0) {
+      const int blocks = std::min(148, (a1 - a0 + 7) / 8);
+      if (c->prec == PSDNS_PREC_FP64)
+        k_sphere_out<double><<<blocks, 256, 0, c->s_out>>>(g, c->nv, (const double2*)src, (double2*)dh, a0, a1);
+      else
+        k_sphere_out<float><<<blocks, 256, 0, c->s_out>>>(g, c->nv, (const float2*)src, (double2*)dh, a0, a1);
+      CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(c->ev_d2h[k], c->s_out));
+  }
+  c->sphere_get_pending = true;
+  c->sphere_get_call = c->api_calls;
+  c->pend_out = (const char*)out;
+  c->pend_out_bytes = sizeof(double2) * c->st_elems;
+  c->pend_sphere = true;
   return 0;
 }
 
 int psdns_gpu_sync(void* ctx) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return set_error("null context");
   if (c->s_in) {
     CK(cudaStreamSynchronize(c->s_in));
@@ -1281,6 +1424,7 @@ int psdns_gpu_sync(void* ctx) {
 // ---------------------------------------------------------------------------
 int psdns_gpu_write_checkpoint(void* ctx, const char* path, int32_t which) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c || !path) return set_error("null argument");
   if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
   const int n = c->n, nxh = n / 2 + 1, xisz = n / 2;
@@ -1328,6 +1472,7 @@ int psdns_gpu_write_checkpoint(void* ctx, const char* path, int32_t which) {
 
 int psdns_gpu_read_checkpoint(void* ctx, const char* path) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c || !path) return set_error("null argument");
   const int n = c->n, nxh = n / 2 + 1, xisz = n / 2;
   const size_t fs = (size_t)nxh * n * n;
@@ -1381,6 +1526,7 @@ int psdns_gpu_read_checkpoint(void* ctx, const char* path) {
 
 int psdns_gpu_set_state(void* ctx, const double* un, int32_t layout) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c || !un) return set_error("null argument");
   if (layout != PSDNS_LAYOUT_YCYL && layout != PSDNS_LAYOUT_FULL) return set_error("unsupported layout %d", layout);
   const size_t vs = (size_t)c->g.xz_tot * c->n;
@@ -1409,6 +1555,7 @@ int psdns_gpu_set_state(void* ctx, const double* un, int32_t layout) {
 
 int psdns_gpu_get_state(void* ctx, double* out, int32_t which, int32_t layout) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c || !out) return set_error("null argument");
   if (layout != PSDNS_LAYOUT_YCYL && layout != PSDNS_LAYOUT_FULL) return set_error("unsupported layout %d", layout);
   if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
@@ -1435,6 +1582,7 @@ int psdns_gpu_get_state(void* ctx, double* out, int32_t which, int32_t layout) {
 
 int psdns_gpu_step(void* ctx, double* info) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return set_error("null context");
   Ops o;
   if (!get_ops(c->prec, c->n, c->nc, o)) return set_error("bad context");
@@ -1468,6 +1616,7 @@ int psdns_gpu_step(void* ctx, double* info) {
 int psdns_gpu_rk_stage(void* ctx, int32_t kstep, const double* gsh, const double* dt, const double* forcing,
                        double* velmax_out) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c || !gsh) return set_error("null argument");
   if (kstep != 1 && kstep != 2) return set_error("kstep must be 1 or 2");
   if (forcing != nullptr && !(c->p.kforce > 0))
@@ -1509,6 +1658,7 @@ int psdns_gpu_rk_stage(void* ctx, int32_t kstep, const double* gsh, const double
 
 int psdns_gpu_field_init(void* ctx, int32_t seed) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return set_error("null context");
   if (seed <= 0) return set_error("seed %d must be positive (ranu.f:33)", seed);
   const Geometry& g = c->g;
@@ -1556,6 +1706,7 @@ int psdns_gpu_field_init(void* ctx, int32_t seed) {
 
 int psdns_gpu_field_sinusoidal(void* ctx, double au, double av) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return set_error("null context");
   const Geometry& g = c->g;
   const int n = c->n;
@@ -1593,6 +1744,7 @@ int psdns_gpu_field_sinusoidal(void* ctx, double au, double av) {
 
 int psdns_gpu_particles_set(void* ctx, int64_t np, const double* pos) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return set_error("null context");
   if (np < 0) return set_error("negative particle count");
   if (np > 0 && !pos) return set_error("null positions");
@@ -1619,6 +1771,7 @@ int psdns_gpu_particles_set(void* ctx, int64_t np, const double* pos) {
 
 int psdns_gpu_particles_init(void* ctx, int64_t nop, int32_t pstart, int32_t kipran) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return set_error("null context");
   if (pstart != 0 && pstart != -1) return set_error("pstart must be 0 (random) or -1 (lattice)");
   if (nop <= 0) return set_error("nop must be positive");
@@ -1634,6 +1787,7 @@ int psdns_gpu_particles_init(void* ctx, int64_t nop, int32_t pstart, int32_t kip
 
 int psdns_gpu_particles_get(void* ctx, double* pos, double* vel) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return set_error("null context");
   if (c->np == 0) return set_error("no particles");
   if (pos) CK(cudaMemcpy(pos, c->d_pos, sizeof(double) * 3 * (size_t)c->np, cudaMemcpyDeviceToHost));
@@ -1643,6 +1797,7 @@ int psdns_gpu_particles_get(void* ctx, double* pos, double* vel) {
 
 int psdns_gpu_spectra(void* ctx, int32_t which, double* ek, double* dk, double* eijk, double* stats) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return set_error("null context");
   if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
   // the ub work array is free between steps: use it for the sums
@@ -1652,6 +1807,7 @@ int psdns_gpu_spectra(void* ctx, int32_t which, double* ek, double* dk, double* 
 
 int psdns_gpu_gradient_moments(void* ctx, int32_t which, const double* gsh, double* out) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c || !out) return set_error("null argument");
   if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
   Ops o;
@@ -1661,6 +1817,7 @@ int psdns_gpu_gradient_moments(void* ctx, int32_t which, const double* gsh, doub
 
 int psdns_gpu_transfer_spectrum(void* ctx, const double* gsh, double* tk) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c || !tk) return set_error("null argument");
   Ops o;
   if (!get_ops(c->prec, c->n, c->nc, o)) return set_error("bad context");
@@ -1669,6 +1826,7 @@ int psdns_gpu_transfer_spectrum(void* ctx, const double* gsh, double* tk) {
 
 int psdns_gpu_spectra_scales(void* ctx, int32_t which, double* xr, double* yr, double* zr, double* stats) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return set_error("null context");
   if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
   return spectra_scales_of(make_geo(*c), which == PSDNS_FIELD_U ? c->d_u : c->d_un, c->prec, c->p, c->stream,
@@ -1677,6 +1835,7 @@ int psdns_gpu_spectra_scales(void* ctx, int32_t which, double* xr, double* yr, d
 
 int psdns_gpu_forcing_stats(void* ctx, double* efk, double* eirate, double* erate) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return set_error("null context");
   if (!(c->p.kforce > 0)) return set_error("context is unforced (kforce = 0)");
   if (efk) for (int k = 0; k < c->kfor; k++) efk[k] = k < (int)c->efk_host.size() ? c->efk_host[k] : 0.0;
@@ -1687,6 +1846,7 @@ int psdns_gpu_forcing_stats(void* ctx, double* efk, double* eirate, double* erat
 
 int psdns_gpu_forcing_table(void* ctx, double* table, int32_t* kfor, int32_t* k2fo) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return set_error("null context");
   if (kfor) *kfor = c->kfor;
   if (k2fo) *k2fo = c->k2fo;
@@ -1696,6 +1856,7 @@ int psdns_gpu_forcing_table(void* ctx, double* table, int32_t* kfor, int32_t* k2
 
 int psdns_gpu_get_stream(void* ctx, void** stream) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c || !stream) return set_error("null argument");
   *stream = (void*)c->stream;
   return 0;
@@ -1703,6 +1864,7 @@ int psdns_gpu_get_stream(void* ctx, void** stream) {
 
 int psdns_gpu_profile(void* ctx, int32_t enable) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return set_error("null context");
   if (enable && !c->ev[0][0][0]) {
     for (int s = 0; s < 2; s++)
@@ -1716,6 +1878,7 @@ int psdns_gpu_profile(void* ctx, int32_t enable) {
 
 int psdns_gpu_kernel_times(void* ctx, double* ms, int64_t* launches) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c) return set_error("null context");
   for (int k = 0; k < 6; k++) {
     if (ms) ms[k] = c->prof_ms[k];
@@ -1726,6 +1889,7 @@ int psdns_gpu_kernel_times(void* ctx, double* ms, int64_t* launches) {
 
 int psdns_gpu_get_time(void* ctx, double* out4) {
   Ctx* c = (Ctx*)ctx;
+  touch(c);
   if (!c || !out4) return set_error("null argument");
   out4[0] = c->time;
   out4[1] = c->dt;

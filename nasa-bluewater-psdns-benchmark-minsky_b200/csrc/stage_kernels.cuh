@@ -1117,6 +1117,76 @@ __global__ void k_to_f64(const C2<T>* __restrict__ src, double2* __restrict__ ds
 // Full half-complex layout u(nxh, ny, nz) (column-major, nxh = n/2 + 1, the
 // FFTW real-to-complex shape of a real (nx, ny, nz) array) <-> cylinder
 // columns: column a = (x, z) holds every y of (x, ., z).
+// Host <-> device copies of the entries inside the truncation sphere only
+// (mask of masks.f: y != n/2 and min(y, n-y) <= kymax(a)), reading or writing
+// pinned host memory directly (a warp per column; each column's entries are
+// the runs y = 0..kym and n-kym..n-1, so a warp moves 512 contiguous bytes per
+// instruction).  Columns a0..a1-1 of every variable; entries outside the
+// sphere are neither read nor written.
+__device__ __forceinline__ int sphere_y(int i, int kym, int n) { return i <= kym ? i : n - 2 * kym - 1 + i; }
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_sphere_in(Geo g, int nv, const double2* __restrict__ h,
+                                                   C2<T>* __restrict__ un, C2<T>* __restrict__ u, int a0, int a1) {
+  const int n = g.n;
+  const size_t vs = (size_t)g.xz_tot * n;
+  const int lane = threadIdx.x & 31;
+  const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int a = a0 + w0; a < a1; a += nw) {
+    const int kym = __ldg(g.kymax + a), cnt = 2 * kym + 1;
+    for (int v = 0; v < nv; v++) {
+      const size_t base = v * vs + (size_t)a * n;
+      // four independent reads in flight per thread (bus latency)
+      for (int i0 = 0; i0 < cnt; i0 += 128) {
+        double2 x[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int i = i0 + j * 32 + lane;
+          if (i < cnt) x[j] = h[base + sphere_y(i, kym, n)];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int i = i0 + j * 32 + lane;
+          if (i < cnt) {
+            const size_t e = base + sphere_y(i, kym, n);
+            const C2<T> c = cmk<C2<T>>((T)x[j].x, (T)x[j].y);
+            un[e] = c;
+            u[e] = c;
+          }
+        }
+      }
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_sphere_out(Geo g, int nv, const C2<T>* __restrict__ src,
+                                                    double2* __restrict__ h, int a0, int a1) {
+  const int n = g.n;
+  const size_t vs = (size_t)g.xz_tot * n;
+  const int lane = threadIdx.x & 31;
+  const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int a = a0 + w0; a < a1; a += nw) {
+    const int kym = __ldg(g.kymax + a), cnt = 2 * kym + 1;
+    for (int v = 0; v < nv; v++) {
+      const size_t base = v * vs + (size_t)a * n;
+      for (int i0 = 0; i0 < cnt; i0 += 128) {
+        C2<T> c[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int i = i0 + j * 32 + lane;
+          if (i < cnt) c[j] = src[base + sphere_y(i, kym, n)];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int i = i0 + j * 32 + lane;
+          if (i < cnt) h[base + sphere_y(i, kym, n)] = make_double2((double)c[j].x, (double)c[j].y);
+        }
+      }
+    }
+  }
+}
+
 template <typename T>
 __global__ void k_full_to_cyl(Geo g, const double2* __restrict__ full, C2<T>* __restrict__ dst,
                               C2<T>* __restrict__ dst2) {

@@ -92,6 +92,20 @@ module psdns_gpu_mod
       type(c_ptr), value :: out
       integer(c_int32_t), value :: which, layout
     end function
+    ! pinned host arrays (c_loc of a cudaHostRegister'ed or cudaHostAlloc'ed uy)
+    integer(c_int) function psdns_gpu_set_state_sphere_async(ctx, un) &
+        bind(c, name='psdns_gpu_set_state_sphere_async')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      type(c_ptr), value :: un
+    end function
+    integer(c_int) function psdns_gpu_get_state_sphere_async(ctx, out, which) &
+        bind(c, name='psdns_gpu_get_state_sphere_async')
+      import :: c_int, c_ptr, c_int32_t
+      type(c_ptr), value :: ctx
+      type(c_ptr), value :: out
+      integer(c_int32_t), value :: which
+    end function
     integer(c_int) function psdns_gpu_sync(ctx) bind(c, name='psdns_gpu_sync')
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx

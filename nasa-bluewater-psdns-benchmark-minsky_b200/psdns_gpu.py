@@ -35,6 +35,9 @@ EXPORTS = (
     "psdns_gpu_read_checkpoint",
     "psdns_gpu_gradient_moments",
     "psdns_gpu_set_state_async",
+    "psdns_gpu_set_state_sphere_async",
+    "psdns_gpu_kymax",
+    "psdns_gpu_get_state_sphere_async",
     "psdns_gpu_get_state_async",
     "psdns_gpu_sync",
     "psdns_gpu_ensemble_create",
@@ -102,6 +105,7 @@ def load():
     vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)
     L.psdns_gpu_default_params.argtypes = [ctypes.POINTER(Params)]
     L.psdns_gpu_geometry.argtypes = [ctypes.c_int32, ip, ip, ip, ip]
+    L.psdns_gpu_kymax.argtypes = [ctypes.c_int32, ip]
     L.psdns_gpu_init.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p)]
     L.psdns_gpu_finalize.argtypes = [vp]
     L.psdns_gpu_set_state.argtypes = [vp, dp, ctypes.c_int32]
@@ -128,6 +132,8 @@ def load():
     L.psdns_gpu_read_checkpoint.argtypes = [vp, ctypes.c_char_p]
     L.psdns_gpu_gradient_moments.argtypes = [vp, ctypes.c_int32, dp, dp]
     L.psdns_gpu_set_state_async.argtypes = [vp, dp, ctypes.c_int32]
+    L.psdns_gpu_set_state_sphere_async.argtypes = [vp, dp]
+    L.psdns_gpu_get_state_sphere_async.argtypes = [vp, dp, ctypes.c_int32]
     L.psdns_gpu_get_state_async.argtypes = [vp, dp, ctypes.c_int32, ctypes.c_int32]
     L.psdns_gpu_sync.argtypes = [vp]
     L.psdns_gpu_ensemble_create.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]
@@ -180,7 +186,16 @@ def geometry(n):
     col = np.zeros(kxn.value + 1, np.int32)
     ip = ctypes.POINTER(ctypes.c_int32)
     _check(load().psdns_gpu_geometry(n, None, None, cut.ctypes.data_as(ip), col.ctypes.data_as(ip)), "geometry")
-    return {"kxn": kxn.value, "xz_tot": tot.value, "cut": cut, "colstart": col}
+    kym = np.zeros(tot.value, np.int32)
+    _check(load().psdns_gpu_kymax(n, kym.ctypes.data_as(ip)), "kymax")
+    return {"kxn": kxn.value, "xz_tot": tot.value, "cut": cut, "colstart": col, "kymax": kym}
+
+
+def sphere_mask(n):
+    """[xz_tot, n] booleans: the entries inside the truncation sphere (masks.f)."""
+    kym = geometry(n)["kymax"].astype(np.int64)
+    y = np.arange(n)
+    return (y[None, :] != n // 2) & (np.minimum(y, n - y)[None, :] <= kym[:, None])
 
 
 NOALLOC_MAX_N = 64
@@ -257,6 +272,16 @@ class Solver:
         """Upload from a pinned host pointer on the copy stream (returns at once)."""
         _check(load().psdns_gpu_set_state_async(self._ctx, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)),
                                                 LAYOUT_YCYL), "set_state_async")
+
+    def set_state_sphere_async_ptr(self, ptr):
+        """Upload the entries inside the truncation sphere from pinned host memory (YCYL)."""
+        _check(load().psdns_gpu_set_state_sphere_async(self._ctx, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double))),
+               "set_state_sphere_async")
+
+    def get_state_sphere_async_ptr(self, ptr, which=FIELD_UN):
+        """Download the entries inside the truncation sphere to pinned host memory (YCYL)."""
+        _check(load().psdns_gpu_get_state_sphere_async(self._ctx, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)),
+                                                       which), "get_state_sphere_async")
 
     def get_state_async_ptr(self, ptr, which=FIELD_UN):
         """Download into a pinned host pointer on the copy stream (returns at once)."""

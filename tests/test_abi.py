@@ -41,6 +41,7 @@ def test_geometry_entry_point(gpu_mod, oracle_mod):
         assert g["kxn"] == o.kxn and g["xz_tot"] == o.xz_tot
         np.testing.assert_array_equal(g["cut"], og["cut"])
         np.testing.assert_array_equal(g["colstart"], og["colstart"])
+        np.testing.assert_array_equal(g["kymax"], og["kymax"])
         o.close()
 
 

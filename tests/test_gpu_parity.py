@@ -440,3 +440,57 @@ def test_transfer_spectrum_matches_oracle(oracle_mod, gpu_mod, prec, tol):
     assert rel_l2(s.get_state(gpu_mod.FIELD_UN), un_o) < (1e-11 if prec == 1 else 2e-5)
     o.close()
     s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [0, 1])
+def test_sphere_copies(gpu_mod, oracle_mod, prec):
+    """psdns_gpu_{set,get}_state_sphere_async: the entries inside the
+    truncation sphere (masks.f) move between pinned host memory and the
+    device; the others are neither read nor written.  A stepping loop that
+    downloads and re-uploads through the same pinned array matches the
+    synchronous path."""
+    import torch
+    n = 32
+    s = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=-1.0, dt=0.005, kshift=1)
+    s.field_init(7)
+    ref = s.get_state(gpu_mod.FIELD_UN)
+    o = oracle_mod.Oracle(n, 0.01, kshift=4)
+    kym = o.geometry()["kymax"].astype(np.int64)
+    o.close()
+    np.testing.assert_array_equal(gpu_mod.geometry(n)["kymax"], kym)
+    y = np.arange(n)
+    ky = np.minimum(y, n - y)
+    inside = (y[None, :] != n // 2) & (ky[None, :] <= kym[:, None])       # [xz_tot, n]
+    np.testing.assert_array_equal(gpu_mod.sphere_mask(n), inside)
+    shape = s.state_shape()
+    host = torch.empty(int(np.prod(shape)) * 2, dtype=torch.float64, pin_memory=True)
+    h = host.numpy().view(np.complex128).reshape(shape)
+    h[...] = 7.0 + 3.0j                                                       # sentinel
+    s.get_state_sphere_async_ptr(host.data_ptr())
+    s.sync()
+    np.testing.assert_array_equal(h[:, inside], ref[:, inside])
+    assert np.all(h[:, ~inside] == 7.0 + 3.0j)
+    # upload a modified field through the sphere path; outside entries of the
+    # host array are ignored
+    h[:, inside] *= 0.5
+    h[:, ~inside] = 1e30
+    s.set_state_sphere_async_ptr(host.data_ptr())
+    s.sync()
+    got = s.get_state(gpu_mod.FIELD_UN)
+    np.testing.assert_allclose(got[:, inside], 0.5 * ref[:, inside], rtol=1e-6 if prec == 0 else 0)
+    # stepping loop through the same array == synchronous stepping
+    t = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=-1.0, dt=0.005, kshift=1)
+    t.set_state(got)
+    h[...] = 0
+    h[:, inside] = got[:, inside]
+    for _ in range(3):
+        s.set_state_sphere_async_ptr(host.data_ptr())
+        s.step()
+        s.get_state_sphere_async_ptr(host.data_ptr())
+        t.step()
+    s.sync()
+    want = t.get_state(gpu_mod.FIELD_UN)
+    np.testing.assert_array_equal(h[:, inside], want[:, inside])
+    s.close()
+    t.close()
