@@ -128,8 +128,9 @@ int psdns_gpu_set_state_async(void *ctx, const double *un, int32_t layout);
 int psdns_gpu_get_state_async(void *ctx, double *out, int32_t which, int32_t layout);
 /* Asynchronous copies of the entries inside the truncation sphere only
  * (PSDNS_LAYOUT_YCYL; the mask of PSDNS/masks.f:46-83: y != ny/2 and
- * min(y, ny-y) <= kymax of the column, the entries the path reads and
- * writes; every other entry of the reference's uy array is zero there).
+ * min(y, ny-y) <= kymax of the column).  These are the entries the step
+ * reads and writes: the reference updates un only inside the mask
+ * (PSDNS/homogeneous/proc4b.f:183-191), so the others keep their values.
  * The host array must be pinned (cudaHostAlloc or cudaHostRegister): kernels
  * read or write it directly over the bus, 63% of the bytes of the full
  * array, with no device staging.  Entries outside the sphere are neither
