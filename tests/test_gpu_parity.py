@@ -443,8 +443,8 @@ def test_transfer_spectrum_matches_oracle(oracle_mod, gpu_mod, prec, tol):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("prec", [0, 1])
-def test_sphere_copies(gpu_mod, oracle_mod, prec):
+@pytest.mark.parametrize("prec,nc", [(0, 0), (1, 0), (0, 1)])
+def test_sphere_copies(gpu_mod, oracle_mod, prec, nc):
     """psdns_gpu_{set,get}_state_sphere_async: the entries inside the
     truncation sphere (masks.f) move between pinned host memory and the
     device; the others are neither read nor written.  A stepping loop that
@@ -452,9 +452,13 @@ def test_sphere_copies(gpu_mod, oracle_mod, prec):
     synchronous path."""
     import torch
     n = 32
-    s = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=-1.0, dt=0.005, kshift=1)
+    kw = dict(nc=1, pr=1.0, grad=(0.0, 1.0, 0.0)) if nc else {}
+    s = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=-1.0, dt=0.005, kshift=1, **kw)
     s.field_init(7)
     ref = s.get_state(gpu_mod.FIELD_UN)
+    if nc:   # give the scalar a field of its own
+        ref[3] = 0.1 * ref[0]
+        s.set_state(ref)
     o = oracle_mod.Oracle(n, 0.01, kshift=4)
     kym = o.geometry()["kymax"].astype(np.int64)
     o.close()
@@ -480,7 +484,7 @@ def test_sphere_copies(gpu_mod, oracle_mod, prec):
     got = s.get_state(gpu_mod.FIELD_UN)
     np.testing.assert_allclose(got[:, inside], 0.5 * ref[:, inside], rtol=1e-6 if prec == 0 else 0)
     # stepping loop through the same array == synchronous stepping
-    t = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=-1.0, dt=0.005, kshift=1)
+    t = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=-1.0, dt=0.005, kshift=1, **kw)
     t.set_state(got)
     h[...] = 0
     h[:, inside] = got[:, inside]
