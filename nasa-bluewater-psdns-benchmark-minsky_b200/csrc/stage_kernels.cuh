@@ -575,8 +575,12 @@ __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const 
       out = cmk<C>(-bk1 * p5.y - kz * p3.y, bk1 * p5.x + kz * p3.x);
     } else if constexpr (MODE == 2) {
       out = s0[i];
-    } else {
+    } else if constexpr (MODE == 3) {
       out = s1[i];
+    } else {                            // MODE 4: s0 to this slot and s1 to slot + 2
+      out = s0[i];
+      dst[2 * ubf_var_elems<T>(g.nab_f, N) + ((size_t)((unsigned)a / TB) * N + y0 + yy) * TB + ((unsigned)a % TB)] =
+          s1[i];
     }
     dst[((size_t)((unsigned)a / TB) * N + y0 + yy) * TB + ((unsigned)a % TB)] = out;
   }
@@ -636,8 +640,8 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
     fft_lines<T, N, THREADS>(s0, nt, L, tw);
     fft_lines<T, N, THREADS>(s1, nt, L, tw);
   }
-  zfwd_store<T, N, 2>(g, s0, s1, L, ub, 1, y0, YT, x0, x1, b11, b33);
-  zfwd_store<T, N, 3>(g, s0, s1, L, ub, 3, y0, YT, x0, x1, b11, b33);
+  // P2 -> ub slot 1 and P4 -> ub slot 3 in one pass over the cylinder indices
+  zfwd_store<T, N, 4>(g, s0, s1, L, ub, 1, y0, YT, x0, x1, b11, b33);
   if constexpr (NC > 0) {
     __syncthreads();
     zfwd_load<T, N>(g, uz, 5, y0, YT, x0, nl, s1, L);

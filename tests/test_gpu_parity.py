@@ -456,9 +456,10 @@ def test_sphere_copies(gpu_mod, oracle_mod, prec, nc):
     s = gpu_mod.Solver(n=n, precision=prec, viscos=0.01, cfl=-1.0, dt=0.005, kshift=1, **kw)
     s.field_init(7)
     ref = s.get_state(gpu_mod.FIELD_UN)
-    if nc:   # give the scalar a field of its own
+    if nc:   # give the scalar a field of its own (stored in the device precision)
         ref[3] = 0.1 * ref[0]
         s.set_state(ref)
+        ref = s.get_state(gpu_mod.FIELD_UN)
     o = oracle_mod.Oracle(n, 0.01, kshift=4)
     kym = o.geometry()["kymax"].astype(np.int64)
     o.close()
