@@ -220,6 +220,36 @@ def test_particles_match_oracle(oracle_mod, gpu_mod, prec, tol_p, tol_v):
     o.close(); s.close()
 
 
+@pytest.mark.parametrize("prec,tol_p,tol_v", [(1, 1e-11, 1e-9), (0, 1e-6, 2e-4)])
+def test_particles_edge_positions(oracle_mod, gpu_mod, prec, tol_p, tol_v):
+    """Positions the cell search must fold: far outside the box on both sides
+    (partsp.f keeps unwrapped coordinates; spcal_local.f folds ipx mod n with
+    a 1000 n offset for negatives), exactly on grid planes, and on the
+    periodic seam."""
+    n, nu = 32, 0.01
+    o = oracle_mod.Oracle(n, nu, cfl=-1, dt=0.01, kshift=1)
+    un0 = o.field_init(11)
+    o.set_state(un0)
+    rng = np.random.default_rng(8)
+    far = rng.uniform(-3 * n, 4 * n, size=(200, 3))
+    planes = rng.integers(-2 * n, 3 * n, size=(100, 3)).astype(np.float64)
+    seam = np.array([[0.0, 1.0, float(n)], [float(n + 1), 1.0 - 1e-12, 0.5], [1.0, 1.0, 1.0],
+                     [-1.0, -float(n), 2.0 * n + 1.0]])
+    pos = np.concatenate([far, planes, seam])
+    o.particles_set(pos)
+    s = gpu_mod.Solver(n=n, precision=prec, viscos=nu, cfl=-1, dt=0.01, kshift=1)
+    s.set_state(un0)
+    s.particles_set(pos)
+    for _ in range(3):
+        o.step()
+        s.step()
+    po, vo = o.particles_get()
+    pg, vg = s.particles_get()
+    assert np.abs(pg - po).max() < tol_p * n
+    assert np.abs(vg - vo).max() < tol_v * np.abs(vo).max()
+    o.close(); s.close()
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_full_layout_round_trip(oracle_mod, gpu_mod, prec):
     """PSDNS_LAYOUT_FULL: u(nxh,ny,nz,nv) <-> cylinder columns (x, ., z)."""
