@@ -173,6 +173,16 @@ int psdns_gpu_particles_set(void *ctx, int64_t np, const double *pos);
  * (either may be NULL). */
 int psdns_gpu_particles_get(void *ctx, double *pos, double *vel);
 
+/* The particle phase of psdns_gpu_step for a driver that runs the stages
+ * itself with psdns_gpu_rk_stage: call it before rk_stage(kstep = 1) of each
+ * step (partsp.f is called at the start of rksubstep(1),
+ * PSDNS/timestep_module.f:168-186), with that stage's shifts gsh(1:3,1) and
+ * the previous step's dt (rk_advpos.f:31-37; ignored by the first call, which
+ * only interpolates).  Builds the spline of the current un on the shifted
+ * grid and advances the particles (partin.f positions from
+ * psdns_gpu_particles_init are made here too). */
+int psdns_gpu_particles_advance(void *ctx, const double *gsh1, double dt_prev);
+
 /* Shell spectra in FP64 (replaces PSDNS/homogeneous/sptr.f:139-400 for the
  * velocity): shells ik = int(|k| + 1.5), n of them (mxyz, comsp_set.f:14).
  * which = PSDNS_FIELD_UN (as sptr(un,...)) or PSDNS_FIELD_U.  Outputs (each

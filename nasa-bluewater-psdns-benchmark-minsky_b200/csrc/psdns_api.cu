@@ -1785,6 +1785,26 @@ int psdns_gpu_particles_init(void* ctx, int64_t nop, int32_t pstart, int32_t kip
   return 0;
 }
 
+int psdns_gpu_particles_advance(void* ctx, const double* gsh1, double dt_prev) {
+  Ctx* c = (Ctx*)ctx;
+  touch(c);
+  if (!c || !gsh1) return set_error("null argument");
+  if (c->np == 0 && c->pin_nop == 0) return set_error("no particles");
+  if (!c->part_first && !(dt_prev > 0)) return set_error("the particle step needs a positive dt");
+  Ops o;
+  if (!get_ops(c->prec, c->n, c->nc, o)) return set_error("bad context");
+  // the stage-1 shifts and dt that psdns_gpu_step would hold at this point;
+  // rk_stage(1) sets both again for its own use
+  for (int i = 0; i < 3; i++) c->gsh[i][0] = gsh1[i];
+  c->dt = dt_prev;
+  if (c->prec == PSDNS_PREC_FP64) fill_shift_tables<double>(*c); else fill_shift_tables<float>(*c);
+  if (upload_tables(*c)) return 1;
+  if (c->pin_nop > 0 && make_partin(*c)) return 1;
+  if (c->np > 0 && o.particles(*c)) return 1;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
 int psdns_gpu_particles_get(void* ctx, double* pos, double* vel) {
   Ctx* c = (Ctx*)ctx;
   touch(c);

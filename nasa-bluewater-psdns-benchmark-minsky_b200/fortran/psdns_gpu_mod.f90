@@ -106,6 +106,13 @@ module psdns_gpu_mod
       type(c_ptr), value :: out
       integer(c_int32_t), value :: which
     end function
+    integer(c_int) function psdns_gpu_particles_advance(ctx, gsh1, dt_prev) &
+        bind(c, name='psdns_gpu_particles_advance')
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: gsh1(3)
+      real(c_double), value :: dt_prev
+    end function
     integer(c_int) function psdns_gpu_sync(ctx) bind(c, name='psdns_gpu_sync')
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx

@@ -37,6 +37,7 @@ EXPORTS = (
     "psdns_gpu_set_state_async",
     "psdns_gpu_set_state_sphere_async",
     "psdns_gpu_kymax",
+    "psdns_gpu_particles_advance",
     "psdns_gpu_get_state_sphere_async",
     "psdns_gpu_get_state_async",
     "psdns_gpu_sync",
@@ -106,6 +107,7 @@ def load():
     L.psdns_gpu_default_params.argtypes = [ctypes.POINTER(Params)]
     L.psdns_gpu_geometry.argtypes = [ctypes.c_int32, ip, ip, ip, ip]
     L.psdns_gpu_kymax.argtypes = [ctypes.c_int32, ip]
+    L.psdns_gpu_particles_advance.argtypes = [vp, dp, ctypes.c_double]
     L.psdns_gpu_init.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p)]
     L.psdns_gpu_finalize.argtypes = [vp]
     L.psdns_gpu_set_state.argtypes = [vp, dp, ctypes.c_int32]
@@ -346,6 +348,12 @@ class Solver:
         """partin.f positions, made at the next step's particle phase."""
         _check(load().psdns_gpu_particles_init(self._ctx, int(nop), int(pstart), int(kipran)), "particles_init")
         self._np = int(nop) if pstart == 0 else int(nop) ** 3
+
+    def particles_advance(self, gsh1, dt_prev):
+        """The particle phase of a step for drivers that call rk_stage themselves:
+        before rk_stage(1), with that stage's shifts gsh(1:3,1) and the previous dt."""
+        g = np.ascontiguousarray(gsh1, dtype=np.float64)
+        _check(load().psdns_gpu_particles_advance(self._ctx, _dp(g), float(dt_prev)), "particles_advance")
 
     def particles_get(self):
         pos = np.zeros((3, self._np)); vel = np.zeros((3, self._np))

@@ -251,6 +251,38 @@ def test_particles_edge_positions(oracle_mod, gpu_mod, prec, tol_p, tol_v):
 
 
 @pytest.mark.parametrize("prec", [0, 1])
+def test_particles_advance_with_rk_stage(gpu_mod, prec):
+    """A driver that runs the stages itself (rk_stage with its own shifts and
+    dt) and calls particles_advance before stage 1 moves the particles exactly
+    as psdns_gpu_step does (zero shifts, kshift = 4, so both paths use the
+    same grid)."""
+    n, nu, dt = 32, 0.01, 0.01
+    kw = dict(n=n, precision=prec, viscos=nu, cfl=-1, dt=dt, kshift=4, kforce=0.0)
+    a = gpu_mod.Solver(**kw)
+    b = gpu_mod.Solver(**kw)
+    a.field_init(5)
+    b.set_state(a.get_state(gpu_mod.FIELD_UN))
+    pos = 1.0 + np.random.default_rng(4).random((300, 3)) * n
+    a.particles_set(pos)
+    b.particles_set(pos)
+    gsh = np.zeros((3, 2))
+    dt_prev = 0.0
+    for _ in range(3):
+        assert a.step()["status"] == 0
+        b.particles_advance(gsh[:, 0], dt_prev)
+        b.rk_stage(1, gsh, dt)
+        b.rk_stage(2, gsh)
+        dt_prev = dt
+    pa, va = a.particles_get()
+    pb, vb = b.particles_get()
+    np.testing.assert_array_equal(pb, pa)
+    np.testing.assert_array_equal(vb, va)
+    np.testing.assert_array_equal(b.get_state(gpu_mod.FIELD_UN), a.get_state(gpu_mod.FIELD_UN))
+    assert np.abs(pa - pos).max() > 0.05
+    a.close(); b.close()
+
+
+@pytest.mark.parametrize("prec", [0, 1])
 def test_full_layout_round_trip(oracle_mod, gpu_mod, prec):
     """PSDNS_LAYOUT_FULL: u(nxh,ny,nz,nv) <-> cylinder columns (x, ., z)."""
     n = 32
