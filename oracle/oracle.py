@@ -5,9 +5,12 @@ CPU-baseline leg of bench.py, as the checker.  The product library never
 imports this module.
 
 The oracle restates the PSDNS RK2 time step (timestep_module.f:70-481 and the
-routines it calls) in FP64 C.  Parity status: unpinned at the FFT boundary
-(the reference's FFTW is not vendored, and the reference ships no golden
-vectors); the oracle FFT is cross-checked against numpy.fft by the tests.
+routines it calls) in FP64 C.  Parity status: pinned only by the reference's
+own shipped checks (README.spp:101-105 eulstat criteria and pcheck.f's exact
+grid values for the pfield.f sinusoidal field, tests/test_reference_criteria.py),
+otherwise unpinned at the FFT boundary (the reference's FFTW is not vendored,
+and the reference ships no golden vectors); the oracle FFT is cross-checked
+against numpy.fft by the tests.
 """
 import ctypes
 import os

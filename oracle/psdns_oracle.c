@@ -5,14 +5,18 @@
  * calls this file; only tests/, __graft_entry__.smoke() and bench.py's CPU
  * baseline leg use it, as the checker.
  *
- * Parity status: UNPINNED at the FFT boundary.  The reference (a Fortran/MPI
- * code, PSDNS) builds against FFTW 3, which is neither vendored nor pinned in
- * the reference tree, and the reference ships no golden vectors or known-answer
- * tests.  The reference cannot be compiled in this container (no Fortran
- * compiler, MPI or FFTW).  This restatement therefore follows the reference's
- * arithmetic statement by statement (citations below, paths relative to the
- * PSDNS project) and uses its own FP64 FFT, which tests cross-check against
- * numpy.fft.
+ * Parity status: pinned only by the reference's own shipped checks, otherwise
+ * UNPINNED at the FFT boundary.  The reference (a Fortran/MPI code, PSDNS)
+ * builds against FFTW 3, which is neither vendored nor pinned in the reference
+ * tree, and it ships no golden vectors; its only correctness checks are the
+ * eulstat criteria of its example runs (README.spp:101-105, the sinusoidal
+ * field of hooks/initial_conditions/pfield.f) and pcheck.f's exact values of
+ * that field on the grid, which tests/test_reference_criteria.py applies to
+ * this restatement.  The reference cannot be compiled in this container (no
+ * Fortran compiler, MPI or FFTW).  This restatement therefore follows the
+ * reference's arithmetic statement by statement (citations below, paths
+ * relative to the PSDNS project) and uses its own FP64 FFT, which tests
+ * cross-check against numpy.fft.
  *
  * Storage follows the reference's own single-rank layout:
  *   y-cylinders  uy(ny, num_al, nv)   -> here u[v][a][y]   (complex)
