@@ -561,3 +561,26 @@ def test_sphere_copies(gpu_mod, oracle_mod, prec, nc):
     np.testing.assert_array_equal(h[:, inside], want[:, inside])
     s.close()
     t.close()
+
+
+def test_error_paths_leave_context_usable(gpu_mod):
+    """Refused calls return an error status with a message and change
+    nothing: sphere copies from pageable memory, a particle step without
+    particles, a stage-1 call without dt."""
+    n = 32
+    s = gpu_mod.Solver(n=n, precision=0, viscos=0.01, cfl=-1.0, dt=0.005, kshift=1)
+    s.field_init(3)
+    before = s.get_state(gpu_mod.FIELD_UN)
+    pageable = np.zeros(int(np.prod(s.state_shape())) * 2)
+    with pytest.raises(RuntimeError, match="pinned"):
+        s.set_state_sphere_async_ptr(pageable.ctypes.data)
+    with pytest.raises(RuntimeError, match="pinned"):
+        s.get_state_sphere_async_ptr(pageable.ctypes.data)
+    with pytest.raises(RuntimeError, match="no particles"):
+        s.particles_advance(np.zeros(3), 0.005)
+    with pytest.raises(RuntimeError, match="dt"):
+        s.rk_stage(1, np.zeros((3, 2)), dt=0.0)
+    s.sync()
+    np.testing.assert_array_equal(s.get_state(gpu_mod.FIELD_UN), before)
+    assert s.step()["status"] == 0
+    s.close()
