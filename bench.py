@@ -144,6 +144,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": n}
 
 
+def reduce_max_ms(ms, dist, device):
+    """Max over ranks of a per-rank time (the slowest replica sets the pace);
+    device is "cuda" under NCCL, "cpu" under gloo."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world, n, ms_step):
+    """Whole-job Gpts/s: every replica advances its own n^3 box per step."""
+    return world * n ** 3 / (ms_step * 1e-3) / 1e9
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -290,12 +306,9 @@ def main():
     s.profile(False)
     ck = clocks.stop()
     barrier()
-    if dist is not None:
-        t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = reduce_max_ms(ms_total, dist, "cuda")
     ms_step = ms_total / args.steps
-    value = world * n ** 3 / (ms_step * 1e-3) / 1e9
+    value = aggregate_rate(world, n, ms_step)
 
     names = ["k_yinv", "k_zinv", "k_xchain", "k_zfwd", "k_yfwd", "particles"]
     per_launch, step_bytes = algorithmic_bytes(n, s.kxn, s.xz_tot, csz)
@@ -363,20 +376,15 @@ def main():
                 s.sync()
                 f1.record(stream)
                 f1.synchronize()
-                ems = f0.elapsed_time(f1) / args.e2e_steps
-                if dist is not None:
-                    t = torch.tensor([ems], dtype=torch.float64, device="cuda")
-                    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-                    ems = float(t.item())
-                return ems
+                return reduce_max_ms(f0.elapsed_time(f1) / args.e2e_steps, dist, "cuda")
             ems_full = timed(s.set_state_async_ptr, s.get_state_async_ptr)
             ems = timed(s.set_state_sphere_async_ptr, s.get_state_sphere_async_ptr)
             # entries per variable inside the truncation sphere (masks.f)
             sphere_bytes = int(P.sphere_mask(n).sum()) * (3 + args.nc) * 16
-            e2e = {"value": world * n ** 3 / (ems * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": sphere_bytes,
+            e2e = {"value": aggregate_rate(world, n, ems), "unit": UNIT, "h2d_bytes_per_step": sphere_bytes,
                    "d2h_bytes_per_step": sphere_bytes, "ms_per_step": ems, "steps": args.e2e_steps,
                    "copies": "entries inside the truncation sphere, pinned host memory read and written by kernels",
-                   "full_array": {"value": world * n ** 3 / (ems_full * 1e-3) / 1e9, "ms_per_step": ems_full,
+                   "full_array": {"value": aggregate_rate(world, n, ems_full), "ms_per_step": ems_full,
                                   "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}}
             del host
         except Exception as ex:  # pinned allocation may exceed host memory
