@@ -584,3 +584,32 @@ def test_error_paths_leave_context_usable(gpu_mod):
     np.testing.assert_array_equal(s.get_state(gpu_mod.FIELD_UN), before)
     assert s.step()["status"] == 0
     s.close()
+
+
+def test_sphere_download_then_step_keeps_the_old_state(gpu_mod):
+    """A step issued right after a sphere download must not overwrite the
+    state while the download still reads it: the host array holds the
+    state before the step, and an upload issued later is ordered after it."""
+    import torch
+    n = 32
+    s = gpu_mod.Solver(n=n, precision=1, viscos=0.01, cfl=-1.0, dt=0.005, kshift=1)
+    s.field_init(21)
+    before = s.get_state(gpu_mod.FIELD_UN)
+    inside = gpu_mod.sphere_mask(n)
+    shape = s.state_shape()
+    host = torch.zeros(int(np.prod(shape)) * 2, dtype=torch.float64, pin_memory=True)
+    h = host.numpy().view(np.complex128).reshape(shape)
+    for _ in range(3):
+        s.get_state_sphere_async_ptr(host.data_ptr())
+        s.step()
+    s.sync()
+    after = s.get_state(gpu_mod.FIELD_UN)
+    # the last download read the state of the step before the last one
+    s2 = gpu_mod.Solver(n=n, precision=1, viscos=0.01, cfl=-1.0, dt=0.005, kshift=1)
+    s2.set_state(before)
+    s2.step()
+    s2.step()
+    want = s2.get_state(gpu_mod.FIELD_UN)
+    np.testing.assert_array_equal(h[:, inside], want[:, inside])
+    assert not np.array_equal(want[:, inside], after[:, inside])
+    s.close(); s2.close()
