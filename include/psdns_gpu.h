@@ -23,6 +23,7 @@
 #ifndef PSDNS_GPU_H
 #define PSDNS_GPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -139,6 +140,12 @@ int psdns_gpu_get_state_async(void *ctx, double *out, int32_t which, int32_t lay
  * ordered after the upload, and any other call first waits for a pending
  * download.  The host array must stay untouched until psdns_gpu_sync. */
 int psdns_gpu_set_state_sphere_async(void *ctx, const double *un);
+/* Pin (page-lock and map) an existing host array for the sphere copies, and
+ * undo it: a Fortran driver's uy array can then be passed as it is, without
+ * calling the CUDA runtime itself.  Pinning is slow (do it once) and the
+ * array must stay allocated until it is unpinned. */
+int psdns_gpu_host_register(void *ptr, size_t bytes);
+int psdns_gpu_host_unregister(void *ptr);
 int psdns_gpu_get_state_sphere_async(void *ctx, double *out, int32_t which);
 /* Wait for every copy and kernel of the context. */
 int psdns_gpu_sync(void *ctx);

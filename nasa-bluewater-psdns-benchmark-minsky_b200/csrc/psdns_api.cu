@@ -1313,6 +1313,26 @@ static void sphere_chunk(const Ctx& c, int k, int& a0, int& a1) {
   a1 = (int)(tot * (k + 1) / Ctx::kChunks);
 }
 
+int psdns_gpu_host_register(void* ptr, size_t bytes) {
+  if (!ptr || bytes == 0) return set_error("null or empty host array");
+  const cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterMapped | cudaHostRegisterPortable);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error("cudaHostRegister: %s", cudaGetErrorString(e));
+  }
+  return 0;
+}
+
+int psdns_gpu_host_unregister(void* ptr) {
+  if (!ptr) return set_error("null host array");
+  const cudaError_t e = cudaHostUnregister(ptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error("cudaHostUnregister: %s", cudaGetErrorString(e));
+  }
+  return 0;
+}
+
 int psdns_gpu_set_state_sphere_async(void* ctx, const double* un) {
   Ctx* c = (Ctx*)ctx;
   touch(c, true);

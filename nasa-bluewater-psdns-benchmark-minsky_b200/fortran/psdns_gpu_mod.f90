@@ -113,6 +113,15 @@ module psdns_gpu_mod
       real(c_double), intent(in) :: gsh1(3)
       real(c_double), value :: dt_prev
     end function
+    integer(c_int) function psdns_gpu_host_register(ptr, bytes) bind(c, name='psdns_gpu_host_register')
+      import :: c_int, c_ptr, c_size_t
+      type(c_ptr), value :: ptr
+      integer(c_size_t), value :: bytes
+    end function
+    integer(c_int) function psdns_gpu_host_unregister(ptr) bind(c, name='psdns_gpu_host_unregister')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ptr
+    end function
     integer(c_int) function psdns_gpu_sync(ctx) bind(c, name='psdns_gpu_sync')
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx

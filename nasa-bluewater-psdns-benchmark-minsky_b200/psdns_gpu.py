@@ -38,6 +38,8 @@ EXPORTS = (
     "psdns_gpu_set_state_sphere_async",
     "psdns_gpu_kymax",
     "psdns_gpu_particles_advance",
+    "psdns_gpu_host_register",
+    "psdns_gpu_host_unregister",
     "psdns_gpu_get_state_sphere_async",
     "psdns_gpu_get_state_async",
     "psdns_gpu_sync",
@@ -108,6 +110,8 @@ def load():
     L.psdns_gpu_geometry.argtypes = [ctypes.c_int32, ip, ip, ip, ip]
     L.psdns_gpu_kymax.argtypes = [ctypes.c_int32, ip]
     L.psdns_gpu_particles_advance.argtypes = [vp, dp, ctypes.c_double]
+    L.psdns_gpu_host_register.argtypes = [vp, ctypes.c_size_t]
+    L.psdns_gpu_host_unregister.argtypes = [vp]
     L.psdns_gpu_init.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p)]
     L.psdns_gpu_finalize.argtypes = [vp]
     L.psdns_gpu_set_state.argtypes = [vp, dp, ctypes.c_int32]
@@ -191,6 +195,17 @@ def geometry(n):
     kym = np.zeros(tot.value, np.int32)
     _check(load().psdns_gpu_kymax(n, kym.ctypes.data_as(ip)), "kymax")
     return {"kxn": kxn.value, "xz_tot": tot.value, "cut": cut, "colstart": col, "kymax": kym}
+
+
+def host_register(arr):
+    """Pin a host numpy array in place (for the sphere copies); returns its address."""
+    ptr = arr.ctypes.data
+    _check(load().psdns_gpu_host_register(ctypes.c_void_p(ptr), arr.nbytes), "host_register")
+    return ptr
+
+
+def host_unregister(arr):
+    _check(load().psdns_gpu_host_unregister(ctypes.c_void_p(arr.ctypes.data)), "host_unregister")
 
 
 def sphere_mask(n):

@@ -613,3 +613,29 @@ def test_sphere_download_then_step_keeps_the_old_state(gpu_mod):
     np.testing.assert_array_equal(h[:, inside], want[:, inside])
     assert not np.array_equal(want[:, inside], after[:, inside])
     s.close(); s2.close()
+
+
+def test_host_register_for_sphere_copies(gpu_mod):
+    """psdns_gpu_host_register pins an ordinary host array in place (what a
+    Fortran driver would do with its uy array) so that the sphere copies can
+    use it; after psdns_gpu_host_unregister they refuse it again."""
+    n = 32
+    s = gpu_mod.Solver(n=n, precision=1, viscos=0.01, cfl=-1.0, dt=0.005, kshift=1)
+    s.field_init(2)
+    ref = s.get_state(gpu_mod.FIELD_UN)
+    inside = gpu_mod.sphere_mask(n)
+    h = np.zeros(s.state_shape(), np.complex128)
+    gpu_mod.host_register(h)
+    try:
+        s.get_state_sphere_async_ptr(h.ctypes.data)
+        s.sync()
+        np.testing.assert_array_equal(h[:, inside], ref[:, inside])
+        h[:, inside] *= 2.0
+        s.set_state_sphere_async_ptr(h.ctypes.data)
+        s.sync()
+        np.testing.assert_array_equal(s.get_state(gpu_mod.FIELD_UN)[:, inside], 2.0 * ref[:, inside])
+    finally:
+        gpu_mod.host_unregister(h)
+    with pytest.raises(RuntimeError, match="pinned"):
+        s.get_state_sphere_async_ptr(h.ctypes.data)
+    s.close()
