@@ -217,5 +217,63 @@ module psdns_gpu_mod
       character(kind=c_char), intent(out) :: buf(*)
       integer(c_int32_t), value :: len
     end function
+    integer(c_int) function psdns_gpu_geometry(n, kxn, xz_tot, cut_z, colstart) bind(c, name='psdns_gpu_geometry')
+      import :: c_int, c_int32_t
+      integer(c_int32_t), value :: n
+      integer(c_int32_t) :: kxn, xz_tot
+      integer(c_int32_t) :: cut_z(*), colstart(*)
+    end function
+    integer(c_int) function psdns_gpu_kymax(n, kymax) bind(c, name='psdns_gpu_kymax')
+      import :: c_int, c_int32_t
+      integer(c_int32_t), value :: n
+      integer(c_int32_t) :: kymax(*)
+    end function
+    integer(c_int) function psdns_gpu_field_init(ctx, seed) bind(c, name='psdns_gpu_field_init')
+      import :: c_int, c_ptr, c_int32_t
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: seed
+    end function
+    integer(c_int) function psdns_gpu_forcing_stats(ctx, efk, eirate, erate) bind(c, name='psdns_gpu_forcing_stats')
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double) :: efk(*), eirate(3), erate
+    end function
+    integer(c_int) function psdns_gpu_forcing_table(ctx, table, kfor, k2fo) bind(c, name='psdns_gpu_forcing_table')
+      import :: c_int, c_ptr, c_double, c_int32_t
+      type(c_ptr), value :: ctx
+      real(c_double) :: table(*)
+      integer(c_int32_t) :: kfor, k2fo
+    end function
+    integer(c_int) function psdns_gpu_get_time(ctx, out4) bind(c, name='psdns_gpu_get_time')
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double) :: out4(4)
+    end function
+    integer(c_int) function psdns_gpu_get_stream(ctx, stream) bind(c, name='psdns_gpu_get_stream')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      type(c_ptr) :: stream
+    end function
+    integer(c_int) function psdns_gpu_profile(ctx, enable) bind(c, name='psdns_gpu_profile')
+      import :: c_int, c_ptr, c_int32_t
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: enable
+    end function
+    integer(c_int) function psdns_gpu_kernel_times(ctx, ms, launches) bind(c, name='psdns_gpu_kernel_times')
+      import :: c_int, c_ptr, c_double, c_int64_t
+      type(c_ptr), value :: ctx
+      real(c_double) :: ms(6)
+      integer(c_int64_t) :: launches(6)
+    end function
+    ! device arrays u_dev, un_dev and the stream are device/CUDA handles
+    integer(c_int) function psdns_gpu_rk_stage_noalloc(p, kstep, gsh, dt, u_dev, un_dev, velmax_out, stream) &
+        bind(c, name='psdns_gpu_rk_stage_noalloc')
+      import :: c_int, c_ptr, c_double, c_int32_t, psdns_params
+      type(psdns_params), intent(in) :: p
+      integer(c_int32_t), value :: kstep
+      real(c_double), intent(in) :: gsh(6), dt(*)
+      type(c_ptr), value :: u_dev, un_dev, stream
+      real(c_double) :: velmax_out
+    end function
   end interface
 end module psdns_gpu_mod
