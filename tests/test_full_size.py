@@ -30,23 +30,23 @@ def exact_moments(n, a):
     return np.array([a ** m * np.mean(c ** m) ** 3 for m in range(1, 9)])
 
 
-def test_sinusoidal_1024_reference_checks(gpu_mod):
+@pytest.mark.parametrize("prec,rtol,vtol", [(0, 1e-5, 2e-6), (1, 1e-11, 1e-12)])
+def test_sinusoidal_1024_reference_checks(gpu_mod, prec, rtol, vtol):
     n, nu, dt = 1024, 1e-3, 2e-3
-    s = gpu_mod.Solver(n=n, precision=gpu_mod.PREC_FP32, viscos=nu, cfl=-1.0, dt=dt, kshift=4, kforce=0.0)
+    s = gpu_mod.Solver(n=n, precision=prec, viscos=nu, cfl=-1.0, dt=dt, kshift=4, kforce=0.0)
     s.field_sinusoidal(1.0, 1.0)
     mx, mz = s.gradient_moments()
-    rtol = 1e-5
     for got, want in ((mx, exact_moments(n, 1.0)), (mz, exact_moments(n, -2.0))):
         scale = abs(want[1])
         np.testing.assert_allclose(got, want, rtol=rtol, atol=rtol * scale * 16)
     tke = [s.spectra()[3]["tke"]]
     # tke = <u^2 + v^2 + w^2>/2 = (1 + 1 + 4)/8/2 on the grid
-    np.testing.assert_allclose(tke[0], 0.375, rtol=1e-6)
+    np.testing.assert_allclose(tke[0], 0.375, rtol=max(rtol, 1e-12))
     for i in range(3):
         info = s.step()
         assert info["status"] == 0
         if i == 0:
-            np.testing.assert_allclose(info["velmax"], exact_velmax(n), rtol=2e-6)
+            np.testing.assert_allclose(info["velmax"], exact_velmax(n), rtol=vtol)
         tke.append(s.spectra()[3]["tke"])
     assert np.all(np.diff(tke) <= 1e-7 * tke[0])
     assert tke[-1] < tke[0]
