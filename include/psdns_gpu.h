@@ -228,19 +228,20 @@ int psdns_gpu_kernel_times(void *ctx, double *ms, int64_t *launches);
 
 /* One RK stage that allocates no device memory.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc, such as a
- * Fortran/OpenACC driver whose device arrays belong to another runtime, a
- * process with a fixed device-memory budget, or code that must not allocate
- * while its stream is captured.  The caller passes its own device arrays u and
- * un (YCYL layout, 3 variables, complex float for PSDNS_PREC_FP32 or complex
- * double for PSDNS_PREC_FP64); all other device memory comes from one static
- * array of PSDNS_NOALLOC_BYTES per GPU, held until the process exits.  Boxes
- * up to PSDNS_NOALLOC_MAX_N^3 (16, 32 or 64), unforced, nc = 0; larger sizes
- * are rejected.  gsh = gsh(3,2) column-major; dt = the step's dt, passed at
- * both stages; velmax_out (stage 1) as in psdns_gpu_rk_stage; stream = a
- * cudaStream_t or NULL.  The first call on a device looks up the array's
- * device address: make it before any stream capture.  Calls share the array,
- * so calls that overlap on the GPU race; the call returns after its work on
- * the stream has completed. */
+ * Fortran/OpenACC driver whose device arrays belong to another runtime, or a
+ * process with a fixed device-memory budget.  The caller passes its own device
+ * arrays u and un (YCYL layout, 3 variables, complex float for
+ * PSDNS_PREC_FP32 or complex double for PSDNS_PREC_FP64) on the current
+ * device; all other device memory comes from one static array of
+ * PSDNS_NOALLOC_BYTES per GPU, held until the process exits.  Boxes up to
+ * PSDNS_NOALLOC_MAX_N^3 (16, 32 or 64), unforced, nc = 0; larger sizes are
+ * rejected.  gsh = gsh(3,2) column-major; dt = the step's dt, passed at both
+ * stages; velmax_out (stage 1) as in psdns_gpu_rk_stage; stream = a
+ * cudaStream_t or NULL.  Each call looks up the array's device address,
+ * copies its tables from host memory and synchronises the stream before it
+ * returns; a stream that is being captured is refused with an error.  Calls
+ * share the array, so calls that overlap on the GPU race.  Host pointers and
+ * other devices' memory are rejected. */
 #define PSDNS_NOALLOC_MAX_N 64
 #define PSDNS_NOALLOC_BYTES (16u * 1024u * 1024u)
 int psdns_gpu_rk_stage_noalloc(const psdns_params *p, int32_t kstep, const double *gsh, const double *dt,

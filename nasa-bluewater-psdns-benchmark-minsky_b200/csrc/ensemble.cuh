@@ -1,147 +1,13 @@
 // ensemble.cuh -- many independent boxes advanced together (included at the
-// end of psdns_api.cu, which defines Ctx, Impl and the host helpers).
-//
-// Boxes of the same grid size n form a class: their states, work arrays and
-// stage tables are stored back to back, and every stage kernel runs once per
-// class with the box as an extra grid dimension (Geo::sbox/bbox/zbox,
-// StageTables::tbox/normv).  A step therefore costs ten kernel launches per
-// distinct n, whatever the number of boxes.  Each box keeps the host state
-// of a single-box run (its own shift RNG stream, dt, time), so box b of an
-// ensemble follows exactly the run of a single context with the same
-// parameters.  Classes whose boxes all use a fixed dt (cfl <= 0) replay each
-// step from a captured CUDA graph; with cfl > 0 the host reads the classes'
-// velmax once per step, between stage-1 parts A and B, to set every box's dt.
+// end of psdns_api.cu, which defines Ctx, Impl and the host helpers; the
+// ensemble types and kernel sequences are in ensemble_impl.cuh).
 
 namespace psdns {
-
-struct EnsClass {
-  int n = 0, nb = 0, prec = 0;
-  std::vector<Ctx*> box;          // host state per box (no device arrays of its own)
-  std::vector<int> index;         // ensemble index of each box
-  Geometry g;
-  int nzt = 0, nab_i = 0, nab_f = 0;
-  size_t st_elems = 0, ub_elems = 0, uz_elems = 0, tab_bytes = 0;
-  int *d_colstart = nullptr, *d_ax = nullptr, *d_az = nullptr, *d_kymax = nullptr;
-  void *d_u = nullptr, *d_un = nullptr, *d_ub = nullptr, *d_uz = nullptr, *d_tabs = nullptr, *d_tw = nullptr;
-  void* d_normv = nullptr;
-  unsigned long long* d_velmax = nullptr;
-  void *h_tabs = nullptr, *h_normv = nullptr;
-  unsigned long long* h_velmax = nullptr;
-  cudaStream_t stream = nullptr;
-  bool fixed_dt = true;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  int (*stage_a)(EnsClass&, int, int, int) = nullptr;
-  int (*stage_b)(EnsClass&, int, int, int) = nullptr;
-  // boxes per launch of the fixed-dt step (0: all).  A sub-batch runs its
-  // whole step (both stages) before the next starts, so that its work
-  // arrays can stay in the 126 MB L2; the first steps try candidate sizes
-  // (they are real steps: the batching does not change any result) and the
-  // fastest is kept for the captured graph.
-  int sub = 0;
-  bool tuned = false;
-  int trial = -1;
-  std::vector<int> cands;
-  std::vector<float> cand_ms;
-};
-
-struct Ensemble {
-  int count = 0, prec = 0;
-  std::vector<EnsClass*> cls;
-  std::vector<std::pair<int, int>> where;   // box -> (class, slot)
-};
-
-static Geo ens_geo(const EnsClass& e) {
-  Geo g;
-  g.n = e.n; g.kxn = e.g.kxn; g.xz_tot = e.g.xz_tot; g.nzt = e.nzt;
-  g.nab_i = e.nab_i; g.nab_f = e.nab_f;
-  g.colstart = e.d_colstart; g.ax = e.d_ax; g.az = e.d_az; g.kymax = e.d_kymax;
-  g.sbox = e.st_elems; g.bbox = e.ub_elems; g.zbox = e.uz_elems;
-  return g;
-}
-
-template <typename T>
-static StageTables<T> ens_tables(const EnsClass& e, int ks, int b0) {
-  TabLayout<T> L(e.n);
-  const char* b = (const char*)e.d_tabs + (size_t)b0 * e.tab_bytes;
-  const psdns_params& p = e.box[0]->p;
-  StageTables<T> st;
-  st.sx = (const C2<T>*)(b + L.sx[ks]);
-  st.sy = (const C2<T>*)(b + L.sy[ks]);
-  st.sz = (const C2<T>*)(b + L.sz[ks]);
-  st.xfac = (const T*)(b + L.xf);
-  st.yfac = (const T*)(b + L.yf);
-  st.zfac = (const T*)(b + L.zf);
-  st.xdif = (const T*)(b + L.xd);
-  st.ydif = (const T*)(b + L.yd);
-  st.zdif = (const T*)(b + L.zd);
-  st.forc = nullptr;
-  st.kfor = 0; st.k2fo = 0; st.kforce2 = 0;
-  st.b11 = (T)(p.beta1 * p.beta1);
-  st.b22 = (T)(p.beta2 * p.beta2);
-  st.b33 = (T)(p.beta3 * p.beta3);
-  st.norm = T(0);
-  st.spf = nullptr;
-  st.tbox = e.tab_bytes;
-  st.normv = (const T*)e.d_normv + b0;
-  return st;
-}
-
-template <typename T, int N> struct EnsImpl {
-  using C = C2<T>;
-  using TL = Tiles<T>;
-  using I = Impl<T, N, 0>;
-
-  // boxes b0 .. b0 + nb - 1
-  static int stage_a(EnsClass& e, int kstep, int b0, int nb) {
-    const Geo g = ens_geo(e);
-    const StageTables<T> st = ens_tables<T>(e, kstep - 1, b0);
-    const C* tw = (const C*)e.d_tw;
-    C* u = (C*)e.d_u + (size_t)b0 * e.st_elems;
-    C* ub = (C*)e.d_ub + (size_t)b0 * e.ub_elems;
-    C* uz = (C*)e.d_uz + (size_t)b0 * e.uz_elems;
-    const int kxn = e.g.kxn;
-    k_yinv<T, N><<<dim3(k1_blocks<T>(e.nab_i), 3, nb), K1Launch<T, N>::THREADS, I::sm1(), e.stream>>>(g, st, u, ub, tw);
-    k_zinv<T, N><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3 * nb), Launch<T, N, TL::XT2>::THREADS, I::sm2(),
-                   e.stream>>>(g, ub, uz, tw, st.b11, st.b33);
-    k_xchain<T, N><<<dim3(e.nzt, N, nb), K3Launch<T, N, 0>::THREADS, I::sm3(), e.stream>>>(
-        g, uz, tw, st.b11, st.b22, st.b33, e.d_velmax + b0, kstep == 1 ? 1 : 0);
-    k_zfwd<T, N><<<dim3(N / TL::YT4, (kxn + TL::XT4 - 1) / TL::XT4, nb), K4Launch<T, N>::THREADS, I::sm4(),
-                   e.stream>>>(g, uz, ub, tw, st.b11, st.b33);
-    CK(cudaGetLastError());
-    return 0;
-  }
-
-  static int stage_b(EnsClass& e, int kstep, int b0, int nb) {
-    const Geo g = ens_geo(e);
-    const StageTables<T> st = ens_tables<T>(e, kstep - 1, b0);
-    constexpr int TH = K5Launch<T, N, 0>::THREADS;
-    const C* ub = (const C*)e.d_ub + (size_t)b0 * e.ub_elems;
-    C* u = (C*)e.d_u + (size_t)b0 * e.st_elems;
-    C* un = (C*)e.d_un + (size_t)b0 * e.st_elems;
-    if (kstep == 1)
-      k_yfwd<T, N, 1><<<dim3(e.nab_f, nb), TH, I::sm5(), e.stream>>>(g, st, ub, u, un, (const C*)e.d_tw, nullptr);
-    else
-      k_yfwd<T, N, 2><<<dim3(e.nab_f, nb), TH, I::sm5(), e.stream>>>(g, st, ub, u, un, (const C*)e.d_tw, nullptr);
-    CK(cudaGetLastError());
-    return 0;
-  }
-
-  static int setup(EnsClass& e) {
-    if (I::setup()) return 1;
-    Ctx tmp;
-    if (I::twiddles(tmp)) return 1;
-    e.d_tw = tmp.d_tw;
-    e.stage_a = &EnsImpl::stage_a;
-    e.stage_b = &EnsImpl::stage_b;
-    return 0;
-  }
-};
 
 static int ens_setup(EnsClass& e) {
 #define PSDNS_ECASE(NN)                                                                           \
   case NN:                                                                                        \
-    return e.prec == PSDNS_PREC_FP64 ? EnsImpl<double, NN>::setup(e) : EnsImpl<float, NN>::setup(e);
+    return ens_setup_n<NN>(e);
   switch (e.n) {
     PSDNS_ECASE(16)
     PSDNS_ECASE(32)

@@ -25,6 +25,7 @@
 
 namespace psdns {
 
+#ifndef PSDNS_INST_N
 static thread_local std::string g_last_error;
 
 int set_error(const char* fmt, ...) {
@@ -37,11 +38,15 @@ int set_error(const char* fmt, ...) {
   return 1;
 }
 
+#endif
+
 #define CK(call)                                                                         \
   do {                                                                                   \
     cudaError_t e_ = (call);                                                             \
     if (e_ != cudaSuccess) return set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
   } while (0)
+
+#ifndef PSDNS_INST_N
 
 // ---------------------------------------------------------------------------
 // geometry (PSDNS/mpisetup.f:307-357, next_xz :710-732, masks.f:46-83)
@@ -131,6 +136,8 @@ double Rng::ranu() {
   iseed = is;
   return (double)is * 0.46566127e-9;
 }
+
+#endif  // PSDNS_INST_N
 
 // ---------------------------------------------------------------------------
 // context
@@ -263,9 +270,41 @@ static StageTables<T> make_tables(const Ctx& c, int ks) {
   return st;
 }
 
+// stage tables of both stages for the shifts in c.gsh (shifts.f:146-178)
 template <typename T>
-static void fill_shift_tables(Ctx& c);
-static int upload_tables(Ctx& c);
+static void fill_shift_tables(Ctx& c) {
+  TabLayout<T> L(c.n);
+  char* b = (char*)c.h_tabs;
+  const int n = c.n;
+  const double pi = 4. * std::atan(1.);
+  const double ph = 2. * pi / n;
+  for (int k = 0; k < 2; k++) {
+    C2<T>* sx = (C2<T>*)(b + L.sx[k]);
+    C2<T>* sy = (C2<T>*)(b + L.sy[k]);
+    C2<T>* sz = (C2<T>*)(b + L.sz[k]);
+    for (int x = 0; x <= n / 2; x++) {
+      const double th = (ph * c.g.kx[x]) * c.gsh[0][k];
+      sx[x] = cmk<C2<T>>((T)std::cos(th), (T)std::sin(th));
+    }
+    for (int y = 0; y < n; y++) {
+      const double th = (ph * c.g.ky[y]) * c.gsh[1][k];
+      sy[y] = cmk<C2<T>>((T)std::cos(th), (T)std::sin(th));
+    }
+    for (int z = 0; z < n; z++) {
+      const double th = (ph * c.g.kz[z]) * c.gsh[2][k];
+      sz[z] = cmk<C2<T>>((T)std::cos(th), (T)std::sin(th));
+    }
+  }
+}
+
+static int upload_tables(Ctx& c) {
+  const size_t tot = c.prec == PSDNS_PREC_FP64 ? TabLayout<double>(c.n).total : TabLayout<float>(c.n).total;
+  CK(cudaMemcpyAsync(c.d_tabs, c.h_tabs, tot, cudaMemcpyHostToDevice, c.stream));
+  // the staging buffer is reused by the next fill: wait for the copy
+  CK(cudaStreamSynchronize(c.stream));
+  return 0;
+}
+
 
 // ---------------------------------------------------------------------------
 // per-(precision, n, nc) kernel launch sequence
@@ -486,15 +525,32 @@ struct Ops {
   int (*transfer)(Ctx&, const double*, double*);
 };
 
-template <typename T, int N, int NC> static Ops ops_for() {
+template <typename T, int N, int NC> Ops ops_for() {
   using I = Impl<T, N, NC>;
   return Ops{&I::setup, &I::twiddles, &I::stage_a, &I::stage_b, &I::particles, &I::moments, &I::transfer};
 }
 
-template <int N> static Ops ops_n(int prec, int nc) {
+template <int N> Ops ops_n(int prec, int nc) {
   if (prec == PSDNS_PREC_FP64) return nc ? ops_for<double, N, 1>() : ops_for<double, N, 0>();
   return nc ? ops_for<float, N, 1>() : ops_for<float, N, 0>();
 }
+
+}  // namespace psdns
+#include "ensemble_impl.cuh"
+namespace psdns {
+
+// The kernels of each grid size are instantiated in a unit of their own
+// (this file compiled with -DPSDNS_INST_N=n), so that the library builds in
+// parallel; the main unit (no PSDNS_INST_N) holds the host code.
+#define PSDNS_FOR_EACH_N(X) X(16) X(32) X(48) X(64) X(96) X(128) X(256) X(512) X(1024)
+#ifdef PSDNS_INST_N
+template Ops ops_n<PSDNS_INST_N>(int, int);
+template int ens_setup_n<PSDNS_INST_N>(EnsClass&);
+}  // namespace psdns
+#else
+#define PSDNS_EXTERN_N(NN) extern template Ops ops_n<NN>(int, int); extern template int ens_setup_n<NN>(EnsClass&);
+PSDNS_FOR_EACH_N(PSDNS_EXTERN_N)
+#undef PSDNS_EXTERN_N
 
 static bool get_ops(int prec, int n, int nc, Ops& o) {
 #define PSDNS_CASE(NN)    \
@@ -543,32 +599,6 @@ static void draw_shifts(Ctx& c) {
 }
 
 template <typename T>
-static void fill_shift_tables(Ctx& c) {
-  TabLayout<T> L(c.n);
-  char* b = (char*)c.h_tabs;
-  const int n = c.n;
-  const double pi = 4. * std::atan(1.);
-  const double ph = 2. * pi / n;
-  for (int k = 0; k < 2; k++) {
-    C2<T>* sx = (C2<T>*)(b + L.sx[k]);
-    C2<T>* sy = (C2<T>*)(b + L.sy[k]);
-    C2<T>* sz = (C2<T>*)(b + L.sz[k]);
-    for (int x = 0; x <= n / 2; x++) {
-      const double th = (ph * c.g.kx[x]) * c.gsh[0][k];
-      sx[x] = cmk<C2<T>>((T)std::cos(th), (T)std::sin(th));
-    }
-    for (int y = 0; y < n; y++) {
-      const double th = (ph * c.g.ky[y]) * c.gsh[1][k];
-      sy[y] = cmk<C2<T>>((T)std::cos(th), (T)std::sin(th));
-    }
-    for (int z = 0; z < n; z++) {
-      const double th = (ph * c.g.kz[z]) * c.gsh[2][k];
-      sz[z] = cmk<C2<T>>((T)std::cos(th), (T)std::sin(th));
-    }
-  }
-}
-
-template <typename T>
 static void fill_factor_tables(Ctx& c) {
   TabLayout<T> L(c.n);
   char* b = (char*)c.h_tabs;
@@ -597,14 +627,6 @@ static void fill_factor_tables(Ctx& c) {
     term = b33 * c.dt;
     for (int z = 0; z < n; z++) zd[z] = (T)std::pow(std::exp(-(nu * (c.g.kz[z] * c.g.kz[z]) * term)), ipr);
   }
-}
-
-static int upload_tables(Ctx& c) {
-  const size_t tot = c.prec == PSDNS_PREC_FP64 ? TabLayout<double>(c.n).total : TabLayout<float>(c.n).total;
-  CK(cudaMemcpyAsync(c.d_tabs, c.h_tabs, tot, cudaMemcpyHostToDevice, c.stream));
-  // the staging buffer is reused by the next fill: wait for the copy
-  CK(cudaStreamSynchronize(c.stream));
-  return 0;
 }
 
 // step.f:49-99, :247-262, :280-295.  Returns nonzero on the reference's abort
@@ -1942,3 +1964,4 @@ int psdns_gpu_get_time(void* ctx, double* out4) {
 
 // ensembles of boxes (batched stage kernels, CUDA graphs)
 #include "ensemble.cuh"
+#endif  // PSDNS_INST_N

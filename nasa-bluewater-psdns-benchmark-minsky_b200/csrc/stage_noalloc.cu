@@ -2,29 +2,29 @@
 //
 // Some callers cannot call cudaMalloc: a Fortran or OpenACC driver whose
 // device arrays are owned by another runtime and that hands us only their
-// addresses; a process started with a fixed device-memory budget handed out
-// once at start-up; code that must not allocate while it runs (for example
-// while its stream is being captured).  psdns_gpu_rk_stage_noalloc serves
-// them: the caller passes its own device arrays u and un, and every other
-// piece of device memory the stage needs (the transposed cylinder and
-// z-pencil work arrays, shift and integrating-factor tables, geometry,
-// twiddles, the velmax accumulator) lives in one file-scope static device
-// array of PSDNS_NOALLOC_BYTES bytes.  Every GPU that loads the library keeps
-// that array until the process exits.
+// addresses, or a process started with a fixed device-memory budget handed
+// out once at start-up.  psdns_gpu_rk_stage_noalloc serves them: the caller
+// passes its own device arrays u and un, and every other piece of device
+// memory the stage needs (the transposed cylinder and z-pencil work arrays,
+// shift and integrating-factor tables, geometry, twiddles, the velmax
+// accumulator) lives in one file-scope static device array of
+// PSDNS_NOALLOC_BYTES bytes.  Every GPU that loads the library keeps that
+// array until the process exits.
 //
 // The array's name is only a host-side stand-in for the device address, so
-// the first call on each device (with that device current) looks the address
-// up with cudaGetSymbolAddress and caches it; make that first call before any
-// stream capture begins.  All calls share the array and it keeps the last
-// call's contents; what must start at zero (the velmax accumulator) is
-// cleared by each call.  Calls whose work overlaps on the GPU (two streams,
-// or two host threads) race on the array and must be serialised by the
-// caller.
+// every call looks the address up with cudaGetSymbolAddress on the current
+// device (cheap, and never stale, e.g. after a cudaDeviceReset reloads the
+// module).  The call copies its tables from host memory and synchronises the
+// caller's stream before it returns, so it refuses a stream that is being
+// captured rather than breaking the capture.  All calls share the array and
+// it keeps the last call's contents; what must start at zero (the velmax
+// accumulator) is cleared by each call.  Calls whose work overlaps on the GPU
+// (two streams, or two host threads) race on the array and must be
+// serialised by the caller.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <vector>
 
 #include "psdns_gpu.h"
@@ -40,26 +40,33 @@ constexpr size_t kBytes = PSDNS_NOALLOC_BYTES;
 
 static __device__ __align__(256) unsigned char g_scratch[kBytes];
 
-constexpr int kMaxDevices = 64;
-static std::mutex g_mu;
-static unsigned char* g_base[kMaxDevices] = {};
-
 static size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
 
-// device address of g_scratch on the current device (looked up once per device)
+// device address of g_scratch on the current device
 static int scratch_base(unsigned char** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+  if (e != cudaSuccess) return set_error("cudaGetSymbolAddress(g_scratch) failed: %s", cudaGetErrorString(e));
+  *out = (unsigned char*)p;
+  return 0;
+}
+
+// u and un must be device (or managed) memory of the current device: a host
+// pointer or another GPU's memory would reach the kernels otherwise
+static int check_device_array(const void* ptr, const char* name) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return set_error("cudaGetDevice failed: %s", cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return set_error("device index %d out of range", dev);
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_base[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_scratch);
-    if (e != cudaSuccess) return set_error("cudaGetSymbolAddress(g_scratch) failed: %s", cudaGetErrorString(e));
-    g_base[dev] = (unsigned char*)p;
+  if (e != cudaSuccess) return set_error("noalloc: cudaGetDevice failed: %s", cudaGetErrorString(e));
+  cudaPointerAttributes at;
+  e = cudaPointerGetAttributes(&at, ptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error("noalloc: %s is not a device pointer (%s)", name, cudaGetErrorString(e));
   }
-  *out = g_base[dev];
+  if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+    return set_error("noalloc: %s must point to device or managed memory", name);
+  if (at.type == cudaMemoryTypeDevice && at.device != dev)
+    return set_error("noalloc: %s lives on device %d, the current device is %d", name, at.device, dev);
   return 0;
 }
 
@@ -237,6 +244,15 @@ extern "C" int psdns_gpu_rk_stage_noalloc(const psdns_params* p, int32_t kstep, 
     return set_error("noalloc: grid %d^3 exceeds the largest box the static scratch holds (%d^3)", n,
                      noalloc::kMaxN);
   cudaStream_t st = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error("noalloc: the stream is not valid on the current device");
+  }
+  if (cap != cudaStreamCaptureStatusNone)
+    return set_error("noalloc: the stream is being captured; this call copies host tables and synchronises the "
+                     "stream, so it cannot be captured");
+  if (noalloc::check_device_array(u_dev, "u") || noalloc::check_device_array(un_dev, "un")) return 1;
   const bool dbl = p->precision == PSDNS_PREC_FP64;
   if (!dbl && p->precision != PSDNS_PREC_FP32) return set_error("noalloc: bad precision");
 #define NA_CASE(NN)                                                                                             \
