@@ -26,6 +26,7 @@ oracle, C/OpenMP on all host cores) on a bounded sample: one RK2 step of a
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -57,6 +58,8 @@ def parse():
     ap.add_argument("--unforced", action="store_true")
     ap.add_argument("--nc", type=int, default=0, choices=[0, 1],
                     help="1: also advance a passive scalar (Sc = 1, mean gradient (0, 1, 0))")
+    ap.add_argument("--accuracy-steps", type=int, default=3,
+                    help="steps of the same-seed FP64 run that judges the error of the timed arm (0: skip)")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="instead: B boxes of n in {32,48,64,96}, log-uniform viscosity, fixed dt")
     return ap.parse_args()
@@ -158,6 +161,52 @@ def reduce_max_ms(ms, dist, device):
 def aggregate_rate(world, n, ms_step):
     """Whole-job Gpts/s: every replica advances its own n^3 box per step."""
     return world * n ** 3 / (ms_step * 1e-3) / 1e9
+
+
+def accuracy_leg(P, n, make_solver, npart, steps, arms):
+    """Error of each arm against the FP64 device run of the same seed and
+    configuration after `steps` steps (run one after the other, outside the
+    timed region; the FP64 device step matches the FP64 oracle to 1e-11 up
+    to 256^3).  Returns, per arm: relative L2 of the velocity un, the largest
+    relative E(k) error over shells holding at least 1e-6 of the peak (and,
+    as the tail figure, 1e-10 of the peak; sptr.f:161-165 shells, FP64 sums
+    on the device), and the largest
+    particle position difference in grid units."""
+    import numpy as np
+
+    def run(prec, mode):
+        s = make_solver(prec, mode)
+        for _ in range(steps):
+            s.step()
+        out = {"un": s.get_state(P.FIELD_UN), "ek": s.spectra(P.FIELD_UN)[0]}
+        if npart > 0:
+            out["pos"] = s.particles_get()[0]
+        s.close()
+        return out
+
+    ref = run(P.PREC_FP64, 0)
+    nrm = np.sqrt(sum(float(np.vdot(ref["un"][v], ref["un"][v]).real) for v in range(ref["un"].shape[0])))
+    res = {}
+    for name, prec, mode in arms:
+        got = run(prec, mode)
+        d2 = 0.0
+        for v in range(3):
+            d = got["un"][v] - ref["un"][v]
+            d2 += float(np.vdot(d, d).real)
+            del d
+        m = ref["ek"] > 1e-6 * ref["ek"].max()
+        t = ref["ek"] > 1e-10 * ref["ek"].max()
+        ent = {"velocity_rel_l2": math.sqrt(d2) / nrm,
+               "ek_max_rel": float(np.max(np.abs(got["ek"][m] - ref["ek"][m]) / ref["ek"][m])),
+               "ek_shells": int(m.sum()),
+               "ek_max_rel_tail": float(np.max(np.abs(got["ek"][t] - ref["ek"][t]) / ref["ek"][t])),
+               "ek_shells_tail": int(t.sum())}
+        if npart > 0:
+            ent["particle_pos_max"] = float(np.abs(got["pos"] - ref["pos"]).max())
+        res[name] = ent
+        del got
+    return {"against": f"FP64 device run of the same seed and configuration, {steps} steps", "steps": steps,
+            "arms": res}
 
 
 def run_reference(args):
@@ -400,6 +449,19 @@ def main():
                "sample": f"one RK2 step of a {args.cpu_n}^3 box (FP64 C/OpenMP restatement of the reference, "
                          f"{cores} threads, {t:.2f} s); Gpts/s = {args.cpu_n}^3/t"}
     s.close()
+    accuracy = None
+    if rank == 0 and world == 1 and args.accuracy_steps > 0 and prec == P.PREC_FP32:
+        def make_solver(p_, mode):
+            t = P.Solver(n=n, precision=p_, viscos=nu, cfl=math.pi, dt=0.0, kshift=1, kforce=kforce, tforce=0.5,
+                         epsfor=epsfor, tfiuo=0.0, nc=args.nc, pr=1.0, grad=(0.0, 1.0, 0.0))
+            t.field_init(1234 + rank)
+            if npart > 0:
+                t.particles_set(1.0 + np.random.default_rng(4321 + rank).random((npart, 3)) * n)
+            return t
+        try:
+            accuracy = accuracy_leg(P, n, make_solver, npart, args.accuracy_steps, [("fp32", P.PREC_FP32, 0)])
+        except Exception as ex:
+            accuracy = {"error": str(ex)[:300]}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -417,6 +479,7 @@ def main():
                          "step_achieved": step_bytes / (ms_step * 1e-3) / 1e9,
                          "step_frac": step_bytes / (ms_step * 1e-3) / 1e9 / peak},
             "kernels": kernel_table,
+            "accuracy": accuracy,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(sum(kcnt[:5]) + 4 * kcnt[5]),
