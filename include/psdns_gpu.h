@@ -226,6 +226,23 @@ int psdns_gpu_get_stream(void *ctx, void **stream);
 int psdns_gpu_profile(void *ctx, int32_t enable);
 int psdns_gpu_kernel_times(void *ctx, double *ms, int64_t *launches);
 
+/* Batched forward 1-D DFT of nlines lines of n = 1024 complex points,
+ * X_k = sum_j x_j exp(-2 pi i jk/n): the transform the stage kernels run
+ * along every axis (the reference's FFTW 1-D transforms planned in
+ * PSDNS/epfftw.f, e.g. PSDNS/transform.f:134).  mode 0: FP32 Stockham
+ * radix-32 passes; mode 1: tensor cores (tcgen05.mma), split-BF16 operands
+ * (hi + lo, three products) with FP32 accumulation.  in/out: host complex(8)
+ * arrays of nlines*n values (computed in FP32).  A standalone check and
+ * comparison of the two DFT forms; it allocates its own device buffers. */
+int psdns_gpu_dft_lines(int32_t n, int64_t nlines, int32_t mode, const double *in, double *out);
+
+/* Diagnostic of the tensor-core operand layouts: d = a b^T for a (128 x 64,
+ * row-major) and b (64 x 64, row-major: row n holds column n of b^T),
+ * both rounded to BF16, with one tcgen05.mma tile accumulated in FP32;
+ * a_mn_major selects the layout of a in shared memory (1: MN-major, as the
+ * DFT uses, 0: K-major).  No counterpart in the reference. */
+int psdns_gpu_tc_gemm_check(int32_t a_mn_major, const float *a, const float *b, float *d);
+
 /* One RK stage that allocates no device memory.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc, such as a
  * Fortran/OpenACC driver whose device arrays belong to another runtime, or a

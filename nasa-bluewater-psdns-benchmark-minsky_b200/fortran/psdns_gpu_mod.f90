@@ -266,6 +266,20 @@ module psdns_gpu_mod
       integer(c_int64_t) :: launches(6)
     end function
     ! device arrays u_dev, un_dev and the stream are device/CUDA handles
+    ! batched 1024-point DFT of lines (mode 0: FP32, 1: split-BF16 tensor cores)
+    integer(c_int) function psdns_gpu_dft_lines(n, nlines, mode, in, out) bind(c, name='psdns_gpu_dft_lines')
+      import :: c_int, c_int32_t, c_int64_t, c_double_complex
+      integer(c_int32_t), value :: n
+      integer(c_int64_t), value :: nlines
+      integer(c_int32_t), value :: mode
+      complex(c_double_complex), intent(in) :: in(*)
+      complex(c_double_complex), intent(out) :: out(*)
+    end function
+    integer(c_int) function psdns_gpu_tc_gemm_check(a_mn_major, a, b, d) bind(c, name='psdns_gpu_tc_gemm_check')
+      import :: c_int, c_int32_t, c_ptr
+      integer(c_int32_t), value :: a_mn_major
+      type(c_ptr), value :: a, b, d
+    end function
     integer(c_int) function psdns_gpu_rk_stage_noalloc(p, kstep, gsh, dt, u_dev, un_dev, velmax_out, stream) &
         bind(c, name='psdns_gpu_rk_stage_noalloc')
       import :: c_int, c_ptr, c_double, c_int32_t, psdns_params

@@ -65,6 +65,8 @@ EXPORTS = (
     "psdns_gpu_profile",
     "psdns_gpu_kernel_times",
     "psdns_gpu_rk_stage_noalloc",
+    "psdns_gpu_dft_lines",
+    "psdns_gpu_tc_gemm_check",
     "psdns_gpu_forcing_stats",
     "psdns_gpu_spectra",
     "psdns_gpu_particles_set",
@@ -130,6 +132,9 @@ def load():
     L.psdns_gpu_spectra.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
+    L.psdns_gpu_dft_lines.argtypes = [ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, dp, dp]
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.psdns_gpu_tc_gemm_check.argtypes = [ctypes.c_int32, fp, fp, fp]
     L.psdns_gpu_field_sinusoidal.argtypes = [vp, ctypes.c_double, ctypes.c_double]
     L.psdns_gpu_transfer_spectrum.argtypes = [vp, dp, dp]
     L.psdns_gpu_spectra_scales.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
@@ -213,6 +218,33 @@ def sphere_mask(n):
     kym = geometry(n)["kymax"].astype(np.int64)
     y = np.arange(n)
     return (y[None, :] != n // 2) & (np.minimum(y, n - y)[None, :] <= kym[:, None])
+
+
+DFT_FP32 = 0
+DFT_TC_BF16X3 = 1
+
+
+def dft_lines(x, mode=DFT_TC_BF16X3):
+    """Forward DFT along the last axis (1024 points) of a complex array on the
+    device (psdns_gpu_dft_lines): mode DFT_FP32 (Stockham radix-32 passes)
+    or DFT_TC_BF16X3 (tensor cores, split-BF16 operands, FP32 accumulation)."""
+    a = np.ascontiguousarray(x, dtype=np.complex128)
+    n = a.shape[-1]
+    out = np.empty_like(a)
+    _check(load().psdns_gpu_dft_lines(n, a.size // n, int(mode), _dp(a.view(np.float64)),
+                                      _dp(out.view(np.float64))), "psdns_gpu_dft_lines")
+    return out
+
+
+def tc_gemm_check(a, b, a_mn_major=1):
+    """d = a b^T on one tensor-core tile (a: 128 x 64, b: 64 x 64, rounded to BF16)."""
+    fa = np.ascontiguousarray(a, dtype=np.float32)
+    fb = np.ascontiguousarray(b, dtype=np.float32)
+    d = np.zeros((128, 64), np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    _check(load().psdns_gpu_tc_gemm_check(int(a_mn_major), fa.ctypes.data_as(fp), fb.ctypes.data_as(fp),
+                                          d.ctypes.data_as(fp)), "psdns_gpu_tc_gemm_check")
+    return d
 
 
 NOALLOC_MAX_N = 64
