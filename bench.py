@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--unforced", action="store_true")
     ap.add_argument("--nc", type=int, default=0, choices=[0, 1],
                     help="1: also advance a passive scalar (Sc = 1, mean gradient (0, 1, 0))")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-precision arm (1-D transforms on the tensor cores, split BF16)")
     ap.add_argument("--accuracy-steps", type=int, default=3,
                     help="steps of the same-seed FP64 run that judges the error of the timed arm (0: skip)")
     ap.add_argument("--ensemble", type=int, default=0,
@@ -449,17 +451,52 @@ def main():
                "sample": f"one RK2 step of a {args.cpu_n}^3 box (FP64 C/OpenMP restatement of the reference, "
                          f"{cores} threads, {t:.2f} s); Gpts/s = {args.cpu_n}^3/t"}
     s.close()
+
+    def make_solver(p_, mode):
+        t = P.Solver(n=n, precision=p_, viscos=nu, cfl=math.pi, dt=0.0, kshift=1, kforce=kforce, tforce=0.5,
+                     epsfor=epsfor, tfiuo=0.0, nc=args.nc, pr=1.0, grad=(0.0, 1.0, 0.0), dft=mode)
+        t.field_init(1234 + rank)
+        if npart > 0:
+            t.particles_set(1.0 + np.random.default_rng(4321 + rank).random((npart, 3)) * n)
+        return t
+
+    # mixed-precision arm: the same workload with every 1-D transform of the
+    # five stage kernels on the tensor cores (split BF16, FP32 accumulation);
+    # the particle spline chain keeps its FP32 transforms
+    mixed = None
+    use_mixed = n == 1024 and prec == P.PREC_FP32 and not args.no_mixed
+    if use_mixed:
+        try:
+            t = make_solver(P.PREC_FP32, P.DFT_TC_BF16X3)
+            tstream = torch.cuda.ExternalStream(t.stream())
+            for _ in range(args.warmup):
+                t.step()
+            barrier()
+            t.profile(True)
+            e0.record(tstream)
+            for _ in range(args.steps):
+                t.step()
+            e1.record(tstream)
+            e1.synchronize()
+            mms = reduce_max_ms(e0.elapsed_time(e1), dist, "cuda") / args.steps
+            mk, mc = t.kernel_times()
+            t.profile(False)
+            t.close()
+            mixed = {"ms_per_step": mms, "value": aggregate_rate(world, n, mms), "unit": UNIT,
+                     "dft": "tensor cores (tcgen05.mma), split BF16 hi+lo, 3 products, FP32 accumulation",
+                     "kernels": {names[i]: {"ms_per_launch": mk[i] / max(1, mc[i]), "launches": int(mc[i]),
+                                            "achieved_gbs": per_launch[names[i]] / (mk[i] / max(1, mc[i]) * 1e-3) / 1e9}
+                                 for i in range(6) if mc[i] > 0},
+                     "gpu_launches": int(sum(mc[:5]) + 4 * mc[5])}
+        except Exception as ex:
+            mixed = {"error": str(ex)[:300]}
     accuracy = None
     if rank == 0 and world == 1 and args.accuracy_steps > 0 and prec == P.PREC_FP32:
-        def make_solver(p_, mode):
-            t = P.Solver(n=n, precision=p_, viscos=nu, cfl=math.pi, dt=0.0, kshift=1, kforce=kforce, tforce=0.5,
-                         epsfor=epsfor, tfiuo=0.0, nc=args.nc, pr=1.0, grad=(0.0, 1.0, 0.0))
-            t.field_init(1234 + rank)
-            if npart > 0:
-                t.particles_set(1.0 + np.random.default_rng(4321 + rank).random((npart, 3)) * n)
-            return t
+        arms = [("fp32", P.PREC_FP32, P.DFT_FP32)]
+        if use_mixed:
+            arms.append(("mixed_bf16x3", P.PREC_FP32, P.DFT_TC_BF16X3))
         try:
-            accuracy = accuracy_leg(P, n, make_solver, npart, args.accuracy_steps, [("fp32", P.PREC_FP32, 0)])
+            accuracy = accuracy_leg(P, n, make_solver, npart, args.accuracy_steps, arms)
         except Exception as ex:
             accuracy = {"error": str(ex)[:300]}
     if rank == 0:
@@ -479,6 +516,7 @@ def main():
                          "step_achieved": step_bytes / (ms_step * 1e-3) / 1e9,
                          "step_frac": step_bytes / (ms_step * 1e-3) / 1e9 / peak},
             "kernels": kernel_table,
+            "arms": {"plain_fp32": {"ms_per_step": ms_step, "value": value, "unit": UNIT}, "mixed_bf16x3": mixed},
             "accuracy": accuracy,
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -34,6 +34,10 @@ extern "C" {
 #define PSDNS_PREC_FP32 0
 #define PSDNS_PREC_FP64 1
 
+/* 1-D transform arithmetic of the stage kernels (psdns_params.dft). */
+#define PSDNS_DFT_FP32 0
+#define PSDNS_DFT_TC_BF16X3 1
+
 /* State layouts for set/get.
  * PSDNS_LAYOUT_YCYL: the reference's y-cylinder array uy(ny,num_al,nv) of a
  *   single rank (jproc = 1), column-major: element (y, a, v) at
@@ -60,7 +64,11 @@ typedef struct psdns_params {
     int32_t ksran;           /* RNG sequence for shifts (PSDNS/input.f:269)  */
     int32_t seed_input;      /* iseed record of the input file               */
     int32_t kranf1, kranf2;  /* RNG sequences for forcing (PSDNS/input.f:268)*/
-    int32_t reserved_i[6];
+    int32_t dft;             /* 1-D transforms: PSDNS_DFT_FP32 (Stockham
+                                passes in the state precision) or
+                                PSDNS_DFT_TC_BF16X3 (tensor cores, split BF16,
+                                FP32 state at n = 1024 only)                */
+    int32_t reserved_i[5];
     double viscos;           /* kinematic viscosity                          */
     double beta1, beta2, beta3; /* box scaling; 1 for a 2*pi box             */
     double cfl;              /* > 0: dt = cfl/velmax (PSDNS/step.f:77-78)    */

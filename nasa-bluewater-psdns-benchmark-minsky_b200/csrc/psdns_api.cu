@@ -152,6 +152,12 @@ struct Ctx {
   void *d_tw = nullptr, *d_tabs = nullptr, *d_u = nullptr, *d_un = nullptr, *d_ub = nullptr, *d_uz = nullptr;
   void *d_forc = nullptr;
   double* d_efkz = nullptr;
+  // tensor-core transforms (dft = PSDNS_DFT_TC_BF16X3): B operands,
+  // twiddles and the error word of the bounded MMA waits
+  int dft = PSDNS_DFT_FP32;
+  void* d_tcb = nullptr;
+  float2* d_tw2 = nullptr;
+  unsigned* d_tcerr = nullptr;
   unsigned long long* d_velmax = nullptr;
   void* h_tabs = nullptr;          // pinned staging of the stage tables
   unsigned long long* h_velmax = nullptr;
@@ -320,7 +326,26 @@ template <typename T, int N, int NC> struct Impl {
   static size_t sm4() { return TWB + sizeof(C) * 2 * TL::XT4 * TL::YT4 * L; }
   static size_t sm5() { return TWB + sizeof(C) * (4 + NC) * TL::TB_F * L; }
 
+  // the tensor-core form (FP32 state at n = 1024): the same kernels with
+  // their 1-D transforms on the tensor cores, and a shared-memory tail
+  static constexpr bool kTc = std::is_same<T, float>::value && N == 1024;
+  static TcArgs tc_args(const Ctx& c) { return TcArgs{(const uint4*)c.d_tcb, c.d_tw2, c.d_tcerr}; }
+
   static int setup() {
+    if constexpr (kTc) {
+      CK(cudaFuncSetAttribute(k_yinv<T, N, false, NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(sm1() + kTcTail)));
+      CK(cudaFuncSetAttribute(k_zinv<T, N, NC, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(sm2() + kTcTail)));
+      CK(cudaFuncSetAttribute(k_xchain<T, N, NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)K3Launch<T, N, NC>::SMEM_TC));
+      CK(cudaFuncSetAttribute(k_zfwd<T, N, NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(sm4() + kTcTail)));
+      CK(cudaFuncSetAttribute(k_yfwd<T, N, 1, NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(sm5() + kTcTail)));
+      CK(cudaFuncSetAttribute(k_yfwd<T, N, 2, NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(sm5() + kTcTail)));
+    }
     CK(cudaFuncSetAttribute(k_yinv<T, N, false, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1()));
     CK(cudaFuncSetAttribute(k_zinv<T, N, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2()));
     CK(cudaFuncSetAttribute(k_xchain<T, N, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3()));
@@ -455,6 +480,8 @@ template <typename T, int N, int NC> struct Impl {
 
   // stage part A: K1..K4 (through the forward z transform)
   static int stage_a(Ctx& c, int kstep) {
+    if constexpr (kTc)
+      if (c.dft == PSDNS_DFT_TC_BF16X3) return stage_a_tc(c, kstep);
     Geo g = make_geo(c);
     StageTables<T> st = make_tables<T>(c, kstep - 1);
     const C* tw = (const C*)c.d_tw;
@@ -497,8 +524,63 @@ template <typename T, int N, int NC> struct Impl {
     return 0;
   }
 
+  // stage part A with the 1-D transforms on the tensor cores (same launch
+  // grids as stage_a)
+  static int stage_a_tc(Ctx& c, int kstep) {
+    Geo g = make_geo(c);
+    StageTables<T> st = make_tables<T>(c, kstep - 1);
+    const TcArgs ta = tc_args(c);
+    const C* tw = (const C*)c.d_tw;
+    C* u = (C*)c.d_u;
+    C* ub = (C*)c.d_ub;
+    C* uz = (C*)c.d_uz;
+    const int kxn = c.g.kxn;
+    const int s = kstep - 1;
+    prof_mark(c, s, 0, 0);
+    k_yinv<T, N, false, NC, true><<<dim3(k1_blocks<T>(c.nab_i), 3 + 2 * NC), K1Launch<T, N>::THREADS,
+                                    sm1() + kTcTail, c.stream>>>(g, st, u, ub, tw, ta);
+    prof_mark(c, s, 0, 1);
+    prof_mark(c, s, 1, 0);
+    k_zinv<T, N, NC, false, true><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3 + 3 * NC),
+                                    Launch<T, N, TL::XT2>::THREADS, sm2() + kTcTail, c.stream>>>(
+        g, ub, uz, tw, st.b11, st.b33, ta);
+    prof_mark(c, s, 1, 1);
+    prof_mark(c, s, 2, 0);
+    const T cb1 = (T)(c.p.beta1 * c.p.grad[0]), cb2 = (T)(c.p.beta2 * c.p.grad[1]),
+            cb3 = (T)(c.p.beta3 * c.p.grad[2]);
+    k_xchain<T, N, NC, true><<<dim3(c.nzt, N), K3Launch<T, N, NC>::THREADS, K3Launch<T, N, NC>::SMEM_TC,
+                               c.stream>>>(g, uz, tw, st.b11, st.b22, st.b33, c.d_velmax, kstep == 1 ? 1 : 0, cb1,
+                                           cb2, cb3, ta);
+    prof_mark(c, s, 2, 1);
+    prof_mark(c, s, 3, 0);
+    k_zfwd<T, N, NC, true><<<dim3(N / TL::YT4, (kxn + TL::XT4 - 1) / TL::XT4), K4Launch<T, N>::THREADS,
+                             sm4() + kTcTail, c.stream>>>(g, uz, ub, tw, st.b11, st.b33, ta);
+    prof_mark(c, s, 3, 1);
+    CK(cudaGetLastError());
+    return 0;
+  }
+
+  static int stage_b_tc(Ctx& c, int kstep) {
+    Geo g = make_geo(c);
+    StageTables<T> st = make_tables<T>(c, kstep - 1);
+    const TcArgs ta = tc_args(c);
+    constexpr int TH = K5Launch<T, N, NC>::THREADS;
+    prof_mark(c, kstep - 1, 4, 0);
+    if (kstep == 1)
+      k_yfwd<T, N, 1, NC, true><<<c.nab_f, TH, sm5() + kTcTail, c.stream>>>(
+          g, st, (const C*)c.d_ub, (C*)c.d_u, (C*)c.d_un, (const C*)c.d_tw, c.d_efkz, ta);
+    else
+      k_yfwd<T, N, 2, NC, true><<<c.nab_f, TH, sm5() + kTcTail, c.stream>>>(
+          g, st, (const C*)c.d_ub, (C*)c.d_u, (C*)c.d_un, (const C*)c.d_tw, c.d_efkz, ta);
+    prof_mark(c, kstep - 1, 4, 1);
+    CK(cudaGetLastError());
+    return 0;
+  }
+
   // stage part B: K5
   static int stage_b(Ctx& c, int kstep) {
+    if constexpr (kTc)
+      if (c.dft == PSDNS_DFT_TC_BF16X3) return stage_b_tc(c, kstep);
     Geo g = make_geo(c);
     StageTables<T> st = make_tables<T>(c, kstep - 1);
     constexpr int TH = K5Launch<T, N, NC>::THREADS;
@@ -751,6 +833,11 @@ static int run_stage(Ctx& c, const Ops& o, int kstep, int* ctl_err) {
     double vm;
     std::memcpy(&vm, c.h_velmax, sizeof vm);
     c.velmax = vm;
+    if (c.d_tcerr) {
+      unsigned e = 0;
+      CK(cudaMemcpy(&e, c.d_tcerr, sizeof e, cudaMemcpyDeviceToHost));
+      if (e) return set_error("a tensor-core transform gave up waiting for its MMAs (error word %u)", e);
+    }
     *ctl_err = step_control(c);
     if (c.prec == PSDNS_PREC_FP64) fill_factor_tables<double>(c); else fill_factor_tables<float>(c);
     if (upload_tables(c)) return 1;
@@ -1113,6 +1200,10 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
     return set_error("RNG sequence numbers must be 1..20 (ranseq.f:131)");
   if (p->seed_input <= 0) return set_error("seed iseed=%d must be positive (ranu.f:33)", p->seed_input);
   if (p->cfl <= 0. && !(p->dt > 0.)) return set_error("fixed dt must be positive when cfl <= 0");
+  if (p->dft != PSDNS_DFT_FP32 && p->dft != PSDNS_DFT_TC_BF16X3)
+    return set_error("dft must be PSDNS_DFT_FP32 or PSDNS_DFT_TC_BF16X3");
+  if (p->dft == PSDNS_DFT_TC_BF16X3 && (p->precision != PSDNS_PREC_FP32 || p->nx != 1024))
+    return set_error("the tensor-core transforms (PSDNS_DFT_TC_BF16X3) need an FP32 state at n = 1024");
   Ops o;
   if (!get_ops(p->precision, p->nx, p->nc, o))
     return set_error("grid size %d not supported (16..1024 powers of 2, 48, 96)", p->nx);
@@ -1184,6 +1275,19 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
       cudaMemcpy(c->d_kymax, g.kymax.data(), sizeof(int) * g.xz_tot, cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(set_error("geometry upload failed"));
   if (o.twiddles(*c)) return fail(1);
+  c->dft = p->dft;
+  if (c->dft == PSDNS_DFT_TC_BF16X3) {
+    std::vector<uint16_t> bt(tc::kBBytes / 2);
+    std::vector<float2> tw2(1024);
+    tc::build_tables(bt.data(), tw2.data());
+    ALLOC2(c->d_tcb, tc::kBBytes);
+    ALLOC2(c->d_tw2, sizeof(float2) * 1024);
+    ALLOC2(c->d_tcerr, sizeof(unsigned));
+    if (cudaMemcpy(c->d_tcb, bt.data(), tc::kBBytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->d_tw2, tw2.data(), sizeof(float2) * 1024, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(c->d_tcerr, 0, sizeof(unsigned)) != cudaSuccess)
+      return fail(set_error("tensor-core table upload failed"));
+  }
   {
     // cubic B-spline symbol per axis: 6 / (4 + 2 cos(2 pi k / n))
     const size_t ns = (size_t)(n / 2 + 1) + 2 * n;
@@ -1215,7 +1319,8 @@ int psdns_gpu_finalize(void* ctx) {
   if (!c) return 0;
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->d_colstart, c->d_ax, c->d_az, c->d_kymax, c->d_tw, c->d_tabs, c->d_u, c->d_un,
-                  c->d_ub, c->d_uz, c->d_forc, c->d_efkz, c->d_velmax, c->d_pos, c->d_vel, c->d_bs, c->d_spf};
+                  c->d_ub, c->d_uz, c->d_forc, c->d_efkz, c->d_velmax, c->d_pos, c->d_vel, c->d_bs, c->d_spf,
+                  c->d_tcb, c->d_tw2, c->d_tcerr};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (int s = 0; s < 2; s++)

@@ -23,6 +23,7 @@
 #include <type_traits>
 
 #include "fft_core.cuh"
+#include "tc_dft.cuh"
 
 namespace psdns {
 
@@ -170,14 +171,46 @@ struct K5Launch : Launch<T, N, (4 + NC) * Tiles<T>::TB_F, 1024> {};
 
 template <int N> struct LS { static constexpr int value = N + N / 32 + 4; };
 
+// Mixed-precision form of the stage kernels (template flag TCM, FP32 state
+// at n = 1024): every 1024-point transform runs on the tensor cores
+// (tc_dft.cuh, split-BF16 operands, FP32 accumulation) instead of the FP32
+// Stockham passes.  TcArgs: the B operands and twiddles of tc_dft.cuh and
+// the error word its bounded waits report to.  The shared-memory tail (B
+// operands, barrier, TMEM address) follows the kernel's own lines.
+struct TcArgs {
+  const uint4* btab = nullptr;
+  const float2* tw2 = nullptr;
+  unsigned* err = nullptr;
+};
+constexpr size_t kTcTail = tc::kBBytes + 16;
+// TMEM columns for nlines lines: 64 per tile of four, as a power of two
+__host__ __device__ constexpr int tc_cols(int nlines) {
+  int c = 64 * ((nlines + 3) / 4), p = 32;
+  while (p < c) p *= 2;
+  return p;
+}
+template <int NCOLS>
+__device__ __forceinline__ void tc_begin(tc::Work& w, unsigned char* tail, const TcArgs& a) {
+  tc::setup<NCOLS>(w, tail, reinterpret_cast<uint64_t*>(tail + tc::kBBytes),
+                   reinterpret_cast<uint32_t*>(tail + tc::kBBytes + 8), a.btab, a.tw2, a.err);
+}
+// in-place forward transform of lines in shared memory, FP32 or tensor cores
+template <typename T, int N, int THREADS, bool TCM>
+__device__ __forceinline__ void lines_fft(C2<T>* buf, int nlines, int ls, const C2<T>* tw, tc::Work& w) {
+  if constexpr (TCM)
+    tc::fft1024_lines<THREADS>(buf, nlines, ls, w);
+  else
+    fft_lines<T, N, THREADS>(buf, nlines, ls, tw);
+}
+
 // ---------------------------------------------------------------------------
 // K1: phase shift + mask + y backward FFT, transposed store to ub (TB_I block)
 // grid (ceil(xz_tot/TB_I), 3); one block = one ub block of TB_I columns
 // ---------------------------------------------------------------------------
-template <typename T, int N, bool SPL = false, int NC = 0>
-__global__ void __launch_bounds__(K1Launch<T, N>::THREADS, 3)
+template <typename T, int N, bool SPL = false, int NC = 0, bool TCM = false>
+__global__ void __launch_bounds__(K1Launch<T, N>::THREADS, TCM ? 2 : 3)
 k_yinv(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ u, C2<T>* __restrict__ ub,
-       const C2<T>* __restrict__ tw_g) {
+       const C2<T>* __restrict__ tw_g, TcArgs tca = TcArgs()) {
   // grid (nab_i, 3 + 2 nc, boxes)
   const int box = blockIdx.z;
   const StageTables<T> st = st_all.at_box(box);
@@ -238,7 +271,19 @@ k_yinv(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ u, C2<T>* __restr
     if constexpr (SPL) val = cscale(s.fx * __ldg(st.spf + (N / 2 + 1) + y) * s.fz, val);
     return cconj(val);
   };
-  fft_lines_load<T, N, THREADS>(buf, TB, L, tw, begin, fetch, fix);
+  if constexpr (TCM) {
+    tc::Work w;
+    constexpr int NCOL = tc_cols(TB);
+    tc_begin<NCOL>(w, reinterpret_cast<unsigned char*>(buf + TB * L), tca);
+    auto line = [&](int l) { return buf + (size_t)l * L; };
+    tc::fft1024<THREADS>(
+        TB, w, reinterpret_cast<unsigned char*>(buf), (uint32_t)(4 * L * sizeof(C)), begin,
+        [&](const Col& s, int y) { return fix(s, y, fetch(s, y)); }, line,
+        [](C* p, int k, C v) { p[pad32(k)] = v; });
+    tc::teardown<NCOL>(w);
+  } else {
+    fft_lines_load<T, N, THREADS>(buf, TB, L, tw, begin, fetch, fix);
+  }
   // columns a0 + l sit at ((a / TBL) n + y) TBL + a % TBL of variable v: a
   // block writes 64-byte halves of the 128-byte runs (a sequential pair of
   // groups per block measured slower than independent blocks)
@@ -258,10 +303,10 @@ __host__ __device__ __forceinline__ int k1_blocks(int nab_i) { return nab_i; }
 // K2: cylinder unpack (zero fill) + z backward FFT, store to uz
 // grid (n, ceil(kxn/XT2), 3)
 // ---------------------------------------------------------------------------
-template <typename T, int N, int NC = 0, bool GRAD = false>
-__global__ void __launch_bounds__(Launch<T, N, Tiles<T>::XT2>::THREADS, 3)
+template <typename T, int N, int NC = 0, bool GRAD = false, bool TCM = false>
+__global__ void __launch_bounds__(Launch<T, N, Tiles<T>::XT2>::THREADS, TCM ? 2 : 3)
 k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11 = T(1),
-       T b33 = T(1)) {
+       T b33 = T(1), TcArgs tca = TcArgs()) {
   // GRAD (grid.z = 2): uz slot 0 = i b11 kx u, slot 1 = i b33 kz w, the
   // gradients whose moments vgmomt.f takes (itransform.f:222-230)
   // NC = 1 (grid.z = 6): uz slot 3 = y gradient of the scalar (ub 4), slot
@@ -324,7 +369,18 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
 #pragma unroll
     for (int r = 0; r < R; r++) p[(size_t)(r * (NS / TZ)) * zstride] = cconj(vals[r]);
   };
-  fft_lines_load_store<T, N, THREADS>(buf, nl, L, tw, begin, fetch, fix, sbegin, store);
+  if constexpr (TCM) {
+    tc::Work w;
+    constexpr int NCOL = tc_cols(XT);
+    tc_begin<NCOL>(w, reinterpret_cast<unsigned char*>(buf + XT * L), tca);
+    tc::fft1024<THREADS>(
+        nl, w, reinterpret_cast<unsigned char*>(buf), (uint32_t)(4 * L * sizeof(C)), begin,
+        [&](const Line& s, int z) { return fix(s, z, fetch(s, z)); }, sbegin,
+        [&](C* d, int z, C v) { d[((unsigned)z / TZ) * zstride + (unsigned)z % TZ] = cconj(v); });
+    tc::teardown<NCOL>(w);
+  } else {
+    fft_lines_load_store<T, N, THREADS>(buf, nl, L, tw, begin, fetch, fix, sbegin, store);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -422,12 +478,18 @@ struct K3Launch {
   // twiddles + 5 product buffers (6 input buffers with a scalar) of TZ/2 lines
   static constexpr size_t SMEM =
       sizeof(C2<T>) * (FFTPlan<T, N>::TWSIZE + (size_t)(NC ? 6 : 5) * NPAIR * LS<N>::value);
+  // tensor-core form: the line buffers rounded up to whole tiles of four
+  // lines (the operands overlay them), then the tail
+  static constexpr int LINES_TC = ((NC ? 6 : 5) * NPAIR + 3) / 4 * 4;
+  static constexpr size_t SMEM_TC =
+      sizeof(C2<T>) * (FFTPlan<T, N>::TWSIZE + (size_t)LINES_TC * LS<N>::value) + kTcTail;
 };
 
-template <typename T, int N, int NC = 0>
+template <typename T, int N, int NC = 0, bool TCM = false>
 __global__ void __launch_bounds__(K3Launch<T, N, NC>::THREADS)
 k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T b22, T b33,
-         unsigned long long* velmax_bits, int want_velmax, T cb1 = T(0), T cb2 = T(0), T cb3 = T(0)) {
+         unsigned long long* velmax_bits, int want_velmax, T cb1 = T(0), T cb2 = T(0), T cb3 = T(0),
+         TcArgs tca = TcArgs()) {
   // NC = 1: inputs also hold the scalar gradient (slots 3 = d/dy, 4 = d/dx,
   // 5 = d/dz); the advection term u.(G + grad theta) (itransform.f:522-530,
   // G = cb, init.f:42-45) is formed in physical space and goes to slot 5.
@@ -445,6 +507,10 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
   C* bufE = bufW + NPAIR * L;
   C* bufF = bufE + NPAIR * L;
   load_twiddles<T, N>(tw, tw_g);
+  constexpr int NCOL = tc_cols(K3Launch<T, N, NC>::LINES_TC);
+  tc::Work w;
+  if constexpr (TCM)
+    tc_begin<NCOL>(w, reinterpret_cast<unsigned char*>(bufU + K3Launch<T, N, NC>::LINES_TC * L), tca);
   // grid (nzt, n, boxes)
   const int zt = blockIdx.x, y = blockIdx.y, box = blockIdx.z;
   uz += box * g.zbox;
@@ -459,7 +525,7 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
   if constexpr (NC > 0) xchain_pack<T, N, 3, THREADS>(g, uz, 3, y, zt, bufU + 3 * NPAIR * L, L);
   cp_async_wait_all();
   __syncthreads();
-  fft_lines<T, N, THREADS>(bufU, NVIN * NPAIR, L, tw);
+  lines_fft<T, N, THREADS, TCM>(bufU, NVIN * NPAIR, L, tw, w);
   // buffers now hold conj(a + i b): a = re, b = -im
   const T hf = T(0.5) / T(N);
   // realspace_vel.f:105-114, in place: slot 0 = b11 u^2 - bv2, 1 = uv,
@@ -497,7 +563,8 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
     if ((threadIdx.x & 31) == 0) atomic_max_pos<T>(velmax_bits, vm);
   }
   __syncthreads();
-  fft_lines<T, N, THREADS>(bufU, (5 + NC) * NPAIR, L, tw);
+  lines_fft<T, N, THREADS, TCM>(bufU, (5 + NC) * NPAIR, L, tw, w);
+  if constexpr (TCM) tc::teardown<NCOL>(w);
   xchain_store<T, N>(g, bufU, 5 + NC, L, uz, 0, y, zt, hf);
 }
 
@@ -586,10 +653,10 @@ __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const 
   }
 }
 
-template <typename T, int N, int NC = 0>
-__global__ void __launch_bounds__(K4Launch<T, N>::THREADS, 3)
+template <typename T, int N, int NC = 0, bool TCM = false>
+__global__ void __launch_bounds__(K4Launch<T, N>::THREADS, TCM ? 2 : 3)
 k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>* __restrict__ tw_g,
-       T b11, T b33) {
+       T b11, T b33, TcArgs tca = TcArgs()) {
   // NC = 1: the scalar advection term (uz slot 5) goes to ub slot 4 without
   // derivatives (transform.f: i2f = 4+nc)
   // grid (n / YT4, ceil(kxn / XT4)): YT4 adjacent y rows x XT4 x lines
@@ -602,6 +669,9 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
   C* s0 = tw + FFTPlan<T, N>::TWSIZE;
   C* s1 = s0 + NLT * L;
   load_twiddles<T, N>(tw, tw_g);
+  constexpr int NCOL = tc_cols(2 * NLT);
+  tc::Work w;
+  if constexpr (TCM) tc_begin<NCOL>(w, reinterpret_cast<unsigned char*>(s1 + NLT * L), tca);
   // grid (n / YT4, ceil(kxn / XT4), boxes)
   const int y0 = blockIdx.x * YT, x0 = blockIdx.y * XT, box = blockIdx.z;
   uz += box * g.zbox;
@@ -615,10 +685,10 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
   cp_async_wait_all();
   __syncthreads();
   if (nl == XT) {
-    fft_lines<T, N, THREADS>(s0, 2 * NLT, L, tw);
+    lines_fft<T, N, THREADS, TCM>(s0, 2 * NLT, L, tw, w);
   } else {
-    fft_lines<T, N, THREADS>(s0, nt, L, tw);
-    fft_lines<T, N, THREADS>(s1, nt, L, tw);
+    lines_fft<T, N, THREADS, TCM>(s0, nt, L, tw, w);
+    lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
   }
   zfwd_store<T, N, 0>(g, s0, s1, L, ub, 0, y0, YT, x0, x1, b11, b33);
   __syncthreads();
@@ -626,7 +696,7 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
   zfwd_load<T, N>(g, uz, 2, y0, YT, x0, nl, s1, L);
   cp_async_wait_all();
   __syncthreads();
-  fft_lines<T, N, THREADS>(s1, nt, L, tw);
+  lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
   zfwd_store<T, N, 1>(g, s0, s1, L, ub, 2, y0, YT, x0, x1, b11, b33);
   __syncthreads();
   // round 3: P2 -> s0, P4 -> s1
@@ -635,10 +705,10 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
   cp_async_wait_all();
   __syncthreads();
   if (nl == XT) {
-    fft_lines<T, N, THREADS>(s0, 2 * NLT, L, tw);
+    lines_fft<T, N, THREADS, TCM>(s0, 2 * NLT, L, tw, w);
   } else {
-    fft_lines<T, N, THREADS>(s0, nt, L, tw);
-    fft_lines<T, N, THREADS>(s1, nt, L, tw);
+    lines_fft<T, N, THREADS, TCM>(s0, nt, L, tw, w);
+    lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
   }
   // P2 -> ub slot 1 and P4 -> ub slot 3 in one pass over the cylinder indices
   zfwd_store<T, N, 4>(g, s0, s1, L, ub, 1, y0, YT, x0, x1, b11, b33);
@@ -647,9 +717,10 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
     zfwd_load<T, N>(g, uz, 5, y0, YT, x0, nl, s1, L);
     cp_async_wait_all();
     __syncthreads();
-    fft_lines<T, N, THREADS>(s1, nt, L, tw);
+    lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
     zfwd_store<T, N, 3>(g, s0, s1, L, ub, 4, y0, YT, x0, x1, b11, b33);
   }
+  if constexpr (TCM) tc::teardown<NCOL>(w);
 }
 
 // ---------------------------------------------------------------------------
@@ -672,10 +743,10 @@ __device__ __forceinline__ void project3(C2<T>& u1, C2<T>& u2, C2<T>& u3, T kx, 
   u3 = cmk<C>(u3.x + kz * psi.x, u3.y + kz * psi.y);
 }
 
-template <typename T, int N, int KSTEP, int NC = 0>
+template <typename T, int N, int KSTEP, int NC = 0, bool TCM = false>
 __global__ void __launch_bounds__(K5Launch<T, N, NC>::THREADS)
 k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __restrict__ u,
-       C2<T>* __restrict__ un, const C2<T>* __restrict__ tw_g, double* __restrict__ efkz) {
+       C2<T>* __restrict__ un, const C2<T>* __restrict__ tw_g, double* __restrict__ efkz, TcArgs tca = TcArgs()) {
   // grid (nab_f, boxes); forcing (efkz) is for single boxes only.
   // KSTEP = 0: transfer spectrum only (trfsp.f:62-83): the shell sums of
   // tfact Re(conj(un) . w) go to efkz[n/2] (shell ik = int(|k|/st.tdk + 1.5));
@@ -725,9 +796,14 @@ k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __rest
       }
     }
   };
+  static_assert(!TCM || KSTEP != 0, "the transfer spectrum keeps the FP32 transform");
+  constexpr int NCOL = tc_cols(NVF * TB);
+  tc::Work w;
+  if constexpr (TCM) tc_begin<NCOL>(w, reinterpret_cast<unsigned char*>(buf + NVF * TB * L), tca);
   cp_async_wait_all();
   __syncthreads();
-  fft_lines<T, N, THREADS>(buf, NVF * TB, L, tw);
+  lines_fft<T, N, THREADS, TCM>(buf, NVF * TB, L, tw, w);
+  if constexpr (TCM) tc::teardown<NCOL>(w);
   // issued together after the transform (registers are free again), so each
   // thread waits once for all of its points
   load_un();

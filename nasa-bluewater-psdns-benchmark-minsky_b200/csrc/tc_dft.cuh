@@ -254,39 +254,48 @@ __device__ __forceinline__ void run_mmas(Work& w, uint32_t tile0, uint32_t tile_
 }
 
 // Forward DFT (natural order in and out) of nlines <= THREADS/32 lines of
-// 1024 complex FP32 values in shared memory, line l at buf + l ls, element i
-// at pad32(i) (the layout of fft_lines).  The operands of tile t overlay
-// lines 4t .. 4t + 3 (ls * 8 * 4 >= 32 KB bytes, 16-byte aligned): the
-// storage of every line up to the next multiple of four is overwritten.
-// Called by every thread of the block; ends with a barrier.
-template <int THREADS>
-__device__ __forceinline__ void fft1024_lines(float2* buf, int nlines, int ls, Work& w) {
+// 1024 complex FP32 values, warp l transforming line l.  The caller supplies
+// the operands and takes the results through callbacks: s = lbegin(l), then
+// load(s, i) returns element i of line l (i = 8 g + e for the thread's
+// groups g = lane + 32 j); t = sbegin(l), then store(t, k, v) receives
+// output k = lane + 32 k2.  tiles: shared memory for ceil(nlines/4) operand
+// tiles of 32 KB, tstride bytes apart (16-byte aligned); every thread's
+// loads complete before the first tile is written, so the tiles may overlay
+// the input.  Called by every thread of the block; the stores are issued
+// after the last block-wide barrier.
+template <int THREADS, typename LBegin, typename Load, typename SBegin, typename Store>
+__device__ __forceinline__ void fft1024(int nlines, Work& w, unsigned char* tiles, uint32_t tstride,
+                                        LBegin lbegin, Load load, SBegin sbegin, Store store) {
   static_assert(THREADS % 32 == 0, "whole warps");
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int q = warp & 3;
   const int ntiles = (nlines + 3) >> 2;
   const bool in_tile = warp < 4 * ntiles;
   const bool act = warp < nlines;
-  unsigned char* tile = reinterpret_cast<unsigned char*>(buf + (size_t)(warp & ~3) * ls);
-  const uint32_t tile0 = smem_u32(buf), tstride = (uint32_t)(4 * ls * sizeof(float2));
+  unsigned char* tile = tiles + (size_t)(warp >> 2) * tstride;
+  const uint32_t tile0 = smem_u32(tiles);
   const uint32_t trow = w.tmem + ((uint32_t)(32 * q) << 16) + 64u * (warp >> 2);
 
   // stage 1 operand: thread holds groups g = lane + 32 j of 8 consecutive
   // elements 8 g .. 8 g + 7 (n1 = g / 4, n2 = 8 (g % 4) + e)
   float re[32], im[32];
-  {
-    const float2* line = buf + (size_t)warp * ls;
+  if (act) {
+    const auto s = lbegin(warp);
+    float2 v[32];
 #pragma unroll
     for (int j = 0; j < 4; j++)
 #pragma unroll
-      for (int e = 0; e < 8; e++) {
-        float2 v = make_float2(0.f, 0.f);
-        if (act) v = line[pad32(8 * (lane + 32 * j) + e)];
-        re[8 * j + e] = v.x;
-        im[8 * j + e] = v.y;
-      }
+      for (int e = 0; e < 8; e++) v[8 * j + e] = load(s, 8 * (lane + 32 * j) + e);
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+      re[i] = v[i].x;
+      im[i] = v[i].y;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 32; i++) re[i] = im[i] = 0.f;
   }
-  __syncthreads();   // every line is read before the tiles overwrite them
+  __syncthreads();   // every input is read before the tiles are written
   if (in_tile) {
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -338,12 +347,25 @@ __device__ __forceinline__ void fft1024_lines(float2* buf, int nlines, int ls, W
     tmem_ld32(trow + 32, im);
   }
   fence_before();
-  __syncthreads();   // the tiles are free: write the lines back
+  __syncthreads();   // the tiles are free
   if (act) {
-    float2* line = buf + (size_t)warp * ls;
+    const auto t = sbegin(warp);
 #pragma unroll
-    for (int k2 = 0; k2 < 32; k2++) line[pad32(lane + 32 * k2)] = make_float2(re[k2], im[k2]);
+    for (int k2 = 0; k2 < 32; k2++) store(t, lane + 32 * k2, make_float2(re[k2], im[k2]));
   }
+}
+
+// fft1024 on lines held in shared memory, line l at buf + l ls, element i
+// at pad32(i) (the layout of fft_lines), in place.  The operand tiles
+// overlay lines 4t .. 4t + 3 (ls * 8 * 4 >= 32 KB bytes, 16-byte aligned):
+// the storage of every line up to the next multiple of four is
+// overwritten.  Ends with a barrier.
+template <int THREADS>
+__device__ __forceinline__ void fft1024_lines(float2* buf, int nlines, int ls, Work& w) {
+  auto line = [&](int l) { return buf + (size_t)l * ls; };
+  fft1024<THREADS>(
+      nlines, w, reinterpret_cast<unsigned char*>(buf), (uint32_t)(4 * ls * sizeof(float2)), line,
+      [](const float2* p, int i) { return p[pad32(i)]; }, line, [](float2* p, int k, float2 v) { p[pad32(k)] = v; });
   __syncthreads();
 }
 

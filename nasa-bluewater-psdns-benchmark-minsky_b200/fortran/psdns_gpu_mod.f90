@@ -8,6 +8,7 @@ module psdns_gpu_mod
   implicit none
 
   integer(c_int32_t), parameter :: PSDNS_PREC_FP32 = 0, PSDNS_PREC_FP64 = 1
+  integer(c_int32_t), parameter :: PSDNS_DFT_FP32 = 0, PSDNS_DFT_TC_BF16X3 = 1
   integer(c_int32_t), parameter :: PSDNS_LAYOUT_YCYL = 0
   integer(c_int32_t), parameter :: PSDNS_LAYOUT_FULL = 1
   integer(c_int32_t), parameter :: PSDNS_FIELD_U = 0, PSDNS_FIELD_UN = 1
@@ -15,7 +16,8 @@ module psdns_gpu_mod
   type, bind(c) :: psdns_params
     integer(c_int32_t) :: nx, ny, nz, nc, precision, kshift, ksran, seed_input
     integer(c_int32_t) :: kranf1, kranf2
-    integer(c_int32_t) :: reserved_i(6)
+    integer(c_int32_t) :: dft
+    integer(c_int32_t) :: reserved_i(5)
     real(c_double) :: viscos, beta1, beta2, beta3, cfl, dt
     real(c_double) :: kforce, tforce, epsfor, tfiuo, pr
     real(c_double) :: grad(3)

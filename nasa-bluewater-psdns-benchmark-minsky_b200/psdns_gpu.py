@@ -20,6 +20,8 @@ _LIB = None
 
 PREC_FP32 = 0
 PREC_FP64 = 1
+DFT_FP32 = 0          # psdns_params.dft: Stockham passes in the state precision
+DFT_TC_BF16X3 = 1     # tensor cores, split-BF16 operands, FP32 accumulation (FP32 state, n = 1024)
 LAYOUT_YCYL = 0
 LAYOUT_FULL = 1
 FIELD_U = 0
@@ -82,7 +84,7 @@ class Params(ctypes.Structure):
         ("nc", ctypes.c_int32), ("precision", ctypes.c_int32), ("kshift", ctypes.c_int32),
         ("ksran", ctypes.c_int32), ("seed_input", ctypes.c_int32),
         ("kranf1", ctypes.c_int32), ("kranf2", ctypes.c_int32),
-        ("reserved_i", ctypes.c_int32 * 6),
+        ("dft", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 5),
         ("viscos", ctypes.c_double), ("beta1", ctypes.c_double), ("beta2", ctypes.c_double),
         ("beta3", ctypes.c_double), ("cfl", ctypes.c_double), ("dt", ctypes.c_double),
         ("kforce", ctypes.c_double), ("tforce", ctypes.c_double), ("epsfor", ctypes.c_double),
@@ -218,10 +220,6 @@ def sphere_mask(n):
     kym = geometry(n)["kymax"].astype(np.int64)
     y = np.arange(n)
     return (y[None, :] != n // 2) & (np.minimum(y, n - y)[None, :] <= kym[:, None])
-
-
-DFT_FP32 = 0
-DFT_TC_BF16X3 = 1
 
 
 def dft_lines(x, mode=DFT_TC_BF16X3):
