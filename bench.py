@@ -60,6 +60,8 @@ def parse():
                     help="1: also advance a passive scalar (Sc = 1, mean gradient (0, 1, 0))")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision arm (1-D transforms on the tensor cores, split BF16)")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned arm (128^3 + spectral-correction network against 512^3 DNS)")
     ap.add_argument("--accuracy-steps", type=int, default=3,
                     help="steps of the same-seed FP64 run that judges the error of the timed arm (0: skip)")
     ap.add_argument("--ensemble", type=int, default=0,
@@ -490,6 +492,23 @@ def main():
                      "gpu_launches": int(sum(mc[:5]) + 4 * mc[5])}
         except Exception as ex:
             mixed = {"error": str(ex)[:300]}
+    # learned arm: 512^3 forced DNS (kmax eta = 1.5) against a 128^3 box with
+    # the spectral-correction network, trained on the device on filtered
+    # 512^3 data made in the same run (learned.py); wall time per step of
+    # each and the corrected box's error against the filtered DNS
+    learned_arm = None
+    if rank == 0 and world == 1 and n == 1024 and not args.no_learned:
+        try:
+            import learned
+            rep, net = learned.run(n_fine=512, n_coarse=128, dt=5e-4, spin=1200, pairs=60, m=10, iters=2000,
+                                   steps=800, every=40)
+            net.close()
+            learned_arm = dict(rep)
+            learned_arm["ms_per_step_plain_512"] = rep["ms_per_step_fine"]
+            learned_arm["speedup_wall_time"] = rep["ms_per_step_fine"] / rep["ms_per_step_coarse_corrected"]
+            learned_arm["timing"] = "host clock around each synchronised step (corrected: step + correction)"
+        except Exception as ex:
+            learned_arm = {"error": str(ex)[:300]}
     accuracy = None
     if rank == 0 and world == 1 and args.accuracy_steps > 0 and prec == P.PREC_FP32:
         arms = [("fp32", P.PREC_FP32, P.DFT_FP32)]
@@ -516,7 +535,8 @@ def main():
                          "step_achieved": step_bytes / (ms_step * 1e-3) / 1e9,
                          "step_frac": step_bytes / (ms_step * 1e-3) / 1e9 / peak},
             "kernels": kernel_table,
-            "arms": {"plain_fp32": {"ms_per_step": ms_step, "value": value, "unit": UNIT}, "mixed_bf16x3": mixed},
+            "arms": {"plain_fp32": {"ms_per_step": ms_step, "value": value, "unit": UNIT}, "mixed_bf16x3": mixed,
+                     "learned_128_vs_512": learned_arm},
             "accuracy": accuracy,
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -234,6 +234,51 @@ int psdns_gpu_get_stream(void *ctx, void **stream);
 int psdns_gpu_profile(void *ctx, int32_t enable);
 int psdns_gpu_kernel_times(void *ctx, double *ms, int64_t *launches);
 
+/* Learned coarse solver.  No counterpart in the reference, which runs the
+ * resolved DNS only; judged on the reference's statistics (E(k), epsilon
+ * and skewness of PSDNS/homogeneous/sptr.f:354-365, du/dx moments of
+ * PSDNS/vgmomt.f).  A coarse box advanced by psdns_gpu_step is corrected
+ * after each step by a per-shell eddy viscosity nu_t(k) = nu g(k), g the
+ * output of a spectral-correction network (4 layers: features -> width ->
+ * width -> width -> 1, tanh, softplus output; BF16 weights, FP32
+ * accumulation) from per-shell features of the box's spectrum.
+ *
+ * psdns_gpu_filter_state: the coarse box's u and un become the fine box's
+ *   un restricted to the coarse truncation sphere (sharp filter in
+ *   wavenumber space), both boxes in the same precision on this device.
+ * psdns_gpu_shell_factor: multiply u and un of every mode of shell
+ *   int(|k| + 0.5) = i, 1 <= i <= nshell, by f[i] (f[0..nshell]).
+ * psdns_gpu_corrector_features: features of shells 1..nshell of u or un:
+ *   x[3 (i-1) + 0..2] = i / kmax, log10(E(i) i^(5/3) / eps^(2/3)) (clamped
+ *   to +-10), log10(kmax eta) with eps the resolved dissipation.
+ * psdns_gpu_corrector_apply: features of un for the resolved shells, network
+ *   forward pass, damping exp(-nu g(i) i^2 dt) with the last step's dt;
+ *   info[0] = 1 if applied, 0 if the plain step was kept (non-finite,
+ *   negative or runaway output: the fallback); info[1] = max g.
+ * psdns_gpu_corrector_create/destroy: a network with Glorot-uniform weights
+ *   from seed.  _params: get (get != 0) or set the PSDNS_CORRECTOR_PARAMS
+ *   FP32 master weights (W0[H][F] b0 W1[H][H] b1 W2[H][H] b2 W3[H] b3).
+ *   _forward: g for nb feature rows.  _grad: for the loss
+ *   L = sum w (a g - tau)^2 / sum w over nb samples, its value and its
+ *   gradient with respect to the master weights (forward with the BF16
+ *   weights).  _train: iters full-batch Adam steps (learning rate lr) on the
+ *   device; loss_hist[iters] (may be NULL) gets the loss before each step. */
+#define PSDNS_CORRECTOR_FEATURES 3
+#define PSDNS_CORRECTOR_WIDTH 32
+#define PSDNS_CORRECTOR_PARAMS 2273
+int psdns_gpu_filter_state(const void *fine, void *coarse);
+int psdns_gpu_shell_factor(void *ctx, int32_t nshell, const double *f);
+int psdns_gpu_corrector_features(void *ctx, int32_t which, int32_t nshell, float *x);
+int psdns_gpu_corrector_apply(void *corr, void *ctx, double *info);
+int psdns_gpu_corrector_create(int32_t seed, void **corr);
+int psdns_gpu_corrector_destroy(void *corr);
+int psdns_gpu_corrector_params(void *corr, int32_t get, float *w);
+int psdns_gpu_corrector_forward(void *corr, int64_t nb, const float *x, float *g);
+int psdns_gpu_corrector_grad(void *corr, int64_t nb, const float *x, const float *a, const float *tau,
+                             const float *wt, float *grad, double *loss);
+int psdns_gpu_corrector_train(void *corr, int64_t nb, const float *x, const float *a, const float *tau,
+                              const float *wt, int32_t iters, double lr, double *loss_hist);
+
 /* Batched forward 1-D DFT of nlines lines of n = 1024 complex points,
  * X_k = sum_j x_j exp(-2 pi i jk/n): the transform the stage kernels run
  * along every axis (the reference's FFTW 1-D transforms planned in

@@ -13,7 +13,7 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
-UNITS = ("psdns_api.cu", "stage_noalloc.cu", "forcing.cpp", "tc_dft.cu")
+UNITS = ("psdns_api.cu", "stage_noalloc.cu", "forcing.cpp", "tc_dft.cu", "learned.cu")
 SRC = [os.path.join(CSRC, f) for f in UNITS if os.path.exists(os.path.join(CSRC, f))]
 # psdns_api.cu is compiled once for the host code and once per grid size for
 # that size's kernels (-DPSDNS_INST_N), so that the units build in parallel

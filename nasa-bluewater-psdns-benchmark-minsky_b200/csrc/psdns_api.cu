@@ -22,6 +22,7 @@
 #include "stage_kernels.cuh"
 #include "field_init.cuh"
 #include "spectra.cuh"
+#include "learned.cuh"
 
 namespace psdns {
 
@@ -158,6 +159,7 @@ struct Ctx {
   void* d_tcb = nullptr;
   float2* d_tw2 = nullptr;
   unsigned* d_tcerr = nullptr;
+  double* d_shf = nullptr;   // per-shell factors of the learned correction
   unsigned long long* d_velmax = nullptr;
   void* h_tabs = nullptr;          // pinned staging of the stage tables
   unsigned long long* h_velmax = nullptr;
@@ -1320,7 +1322,7 @@ int psdns_gpu_finalize(void* ctx) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->d_colstart, c->d_ax, c->d_az, c->d_kymax, c->d_tw, c->d_tabs, c->d_u, c->d_un,
                   c->d_ub, c->d_uz, c->d_forc, c->d_efkz, c->d_velmax, c->d_pos, c->d_vel, c->d_bs, c->d_spf,
-                  c->d_tcb, c->d_tw2, c->d_tcerr};
+                  c->d_tcb, c->d_tw2, c->d_tcerr, c->d_shf};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (int s = 0; s < 2; s++)
@@ -2052,6 +2054,109 @@ int psdns_gpu_kernel_times(void* ctx, double* ms, int64_t* launches) {
     if (launches) launches[k] = c->prof_n[k];
   }
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// learned coarse solver: filter, shell damping, features, correction
+// ---------------------------------------------------------------------------
+int psdns_gpu_filter_state(const void* fine, void* coarse) {
+  const Ctx* f = (const Ctx*)fine;
+  Ctx* c = (Ctx*)coarse;
+  touch(c);
+  if (!f || !c) return set_error("filter_state: null context");
+  if (f->prec != c->prec) return set_error("filter_state: both boxes must have the same precision");
+  if (!(f->n > c->n)) return set_error("filter_state: the fine box (n = %d) must be larger than the coarse (n = %d)",
+                                       f->n, c->n);
+  if (f->p.beta1 != c->p.beta1 || f->p.beta2 != c->p.beta2 || f->p.beta3 != c->p.beta3)
+    return set_error("filter_state: the boxes must have the same shape (beta)");
+  CK(cudaStreamSynchronize(f->stream));
+  const size_t tot = 3 * (size_t)c->g.xz_tot * c->n;
+  const int blocks = (int)std::min<size_t>((tot + 255) / 256, 148 * 16);
+  if (c->prec == PSDNS_PREC_FP64)
+    k_filter_state<double><<<blocks, 256, 0, c->stream>>>(make_geo(*f), (const double2*)f->d_un, make_geo(*c),
+                                                          (double2*)c->d_u, (double2*)c->d_un);
+  else
+    k_filter_state<float><<<blocks, 256, 0, c->stream>>>(make_geo(*f), (const float2*)f->d_un, make_geo(*c),
+                                                         (float2*)c->d_u, (float2*)c->d_un);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int psdns_gpu_shell_factor(void* ctx, int32_t nshell, const double* f) {
+  Ctx* c = (Ctx*)ctx;
+  touch(c);
+  if (!c || !f) return set_error("shell_factor: null argument");
+  if (nshell < 1 || nshell >= c->n) return set_error("shell_factor: nshell must be in 1 .. n-1");
+  if (!c->d_shf) CK(cudaMalloc((void**)&c->d_shf, sizeof(double) * c->n));
+  CK(cudaMemcpyAsync(c->d_shf, f, sizeof(double) * (nshell + 1), cudaMemcpyHostToDevice, c->stream));
+  const size_t tot = 3 * (size_t)c->g.xz_tot * c->n;
+  const int blocks = (int)std::min<size_t>((tot + 255) / 256, 148 * 16);
+  const double b11 = c->p.beta1 * c->p.beta1, b22 = c->p.beta2 * c->p.beta2, b33 = c->p.beta3 * c->p.beta3;
+  if (c->prec == PSDNS_PREC_FP64)
+    k_shell_factor<double><<<blocks, 256, 0, c->stream>>>(make_geo(*c), (double2*)c->d_u, (double2*)c->d_un,
+                                                          c->d_shf, nshell, b11, b22, b33);
+  else
+    k_shell_factor<float><<<blocks, 256, 0, c->stream>>>(make_geo(*c), (float2*)c->d_u, (float2*)c->d_un, c->d_shf,
+                                                         nshell, b11, b22, b33);
+  CK(cudaGetLastError());
+  // f is borrowed for the call only
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+// shells 1 .. K of the coarse box: K = int(kmax + 0.5), kmax = sqrt(2) n / 3
+static int resolved_shells(int n) { return (int)(std::sqrt(2.0) * n / 3.0 + 0.5); }
+
+int psdns_gpu_corrector_features(void* ctx, int32_t which, int32_t nshell, float* x) {
+  Ctx* c = (Ctx*)ctx;
+  touch(c);
+  if (!c || !x) return set_error("corrector_features: null argument");
+  if (nshell < 1 || nshell > resolved_shells(c->n))
+    return set_error("corrector_features: nshell must be in 1 .. %d", resolved_shells(c->n));
+  std::vector<double> ek(c->n);
+  double st[7];
+  if (psdns_gpu_spectra(c, which, ek.data(), nullptr, nullptr, st)) return 1;
+  // per shell i: i / kmax; the compensated spectrum log10(E(i) i^(5/3) /
+  // eps^(2/3)) (clamped to [-10, 10]); the resolution log10(kmax eta),
+  // eta = (nu^3 / eps)^(1/4), eps the resolved dissipation (sptr.f:354-365)
+  const double kmax = std::sqrt(2.0) * c->n / 3.0, nu = c->p.viscos;
+  const double eps = st[1] > 0 ? st[1] : 1e-300;
+  const double res = std::log10(kmax * std::pow(nu * nu * nu / eps, 0.25));
+  for (int i = 1; i <= nshell; i++) {
+    double comp = std::log10(std::max(ek[i], 1e-300) * std::pow((double)i, 5.0 / 3.0) / std::pow(eps, 2.0 / 3.0));
+    comp = std::min(10.0, std::max(-10.0, comp));
+    x[3 * (i - 1) + 0] = (float)(i / kmax);
+    x[3 * (i - 1) + 1] = (float)comp;
+    x[3 * (i - 1) + 2] = (float)res;
+  }
+  return 0;
+}
+
+int psdns_gpu_corrector_apply(void* corr, void* ctx, double* info) {
+  Ctx* c = (Ctx*)ctx;
+  touch(c);
+  if (!corr || !c) return set_error("corrector_apply: null argument");
+  const int K = resolved_shells(c->n);
+  std::vector<float> x(3 * K), g(K);
+  if (psdns_gpu_corrector_features(c, PSDNS_FIELD_UN, K, x.data())) return 1;
+  if (mlp::forward_host(corr, K, x.data(), g.data())) return 1;
+  // eddy viscosity nu_t(i) = nu g(i); damping over the last step's dt
+  std::vector<double> f(K + 1, 1.0);
+  double gmax = 0;
+  bool ok = c->dt > 0;
+  for (int i = 1; i <= K && ok; i++) {
+    const double gi = g[i - 1];
+    if (!(gi >= 0) || !(gi < 1e4)) ok = false;   // NaN, negative or runaway: fall back
+    gmax = std::max(gmax, gi);
+    f[i] = std::exp(-c->p.viscos * gi * (double)i * i * c->dt);
+  }
+  if (info) {
+    info[0] = ok ? 1.0 : 0.0;
+    info[1] = gmax;
+  }
+  if (!ok) return 0;   // the plain solver's step stands
+  return psdns_gpu_shell_factor(c, K, f.data());
 }
 
 int psdns_gpu_get_time(void* ctx, double* out4) {

@@ -58,4 +58,9 @@ struct EPForcing {
 
 int set_error(const char* fmt, ...);
 
+// spectral-correction network (learned.cu): forward pass of nb feature rows
+namespace mlp {
+int forward_host(void* corr, long long nb, const float* x, float* g);
+}
+
 }  // namespace psdns

@@ -268,6 +268,70 @@ module psdns_gpu_mod
       integer(c_int64_t) :: launches(6)
     end function
     ! device arrays u_dev, un_dev and the stream are device/CUDA handles
+    ! learned coarse solver: filter, shell damping, features and the correction network
+    integer(c_int) function psdns_gpu_filter_state(fine, coarse) bind(c, name='psdns_gpu_filter_state')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: fine, coarse
+    end function
+    integer(c_int) function psdns_gpu_shell_factor(ctx, nshell, f) bind(c, name='psdns_gpu_shell_factor')
+      import :: c_int, c_ptr, c_int32_t, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: nshell
+      real(c_double), intent(in) :: f(0:*)
+    end function
+    integer(c_int) function psdns_gpu_corrector_features(ctx, which, nshell, x) &
+        bind(c, name='psdns_gpu_corrector_features')
+      import :: c_int, c_ptr, c_int32_t, c_float
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: which, nshell
+      real(c_float), intent(out) :: x(*)
+    end function
+    integer(c_int) function psdns_gpu_corrector_apply(corr, ctx, info) bind(c, name='psdns_gpu_corrector_apply')
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: corr, ctx
+      real(c_double), intent(out) :: info(2)
+    end function
+    integer(c_int) function psdns_gpu_corrector_create(seed, corr) bind(c, name='psdns_gpu_corrector_create')
+      import :: c_int, c_ptr, c_int32_t
+      integer(c_int32_t), value :: seed
+      type(c_ptr), intent(out) :: corr
+    end function
+    integer(c_int) function psdns_gpu_corrector_destroy(corr) bind(c, name='psdns_gpu_corrector_destroy')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: corr
+    end function
+    integer(c_int) function psdns_gpu_corrector_params(corr, get, w) bind(c, name='psdns_gpu_corrector_params')
+      import :: c_int, c_ptr, c_int32_t, c_float
+      type(c_ptr), value :: corr
+      integer(c_int32_t), value :: get
+      real(c_float), intent(inout) :: w(*)
+    end function
+    integer(c_int) function psdns_gpu_corrector_forward(corr, nb, x, g) bind(c, name='psdns_gpu_corrector_forward')
+      import :: c_int, c_ptr, c_int64_t, c_float
+      type(c_ptr), value :: corr
+      integer(c_int64_t), value :: nb
+      real(c_float), intent(in) :: x(*)
+      real(c_float), intent(out) :: g(*)
+    end function
+    integer(c_int) function psdns_gpu_corrector_grad(corr, nb, x, a, tau, wt, grad, loss) &
+        bind(c, name='psdns_gpu_corrector_grad')
+      import :: c_int, c_ptr, c_int64_t, c_float, c_double
+      type(c_ptr), value :: corr
+      integer(c_int64_t), value :: nb
+      real(c_float), intent(in) :: x(*), a(*), tau(*), wt(*)
+      real(c_float), intent(out) :: grad(*)
+      real(c_double), intent(out) :: loss
+    end function
+    integer(c_int) function psdns_gpu_corrector_train(corr, nb, x, a, tau, wt, iters, lr, loss_hist) &
+        bind(c, name='psdns_gpu_corrector_train')
+      import :: c_int, c_ptr, c_int64_t, c_int32_t, c_float, c_double
+      type(c_ptr), value :: corr
+      integer(c_int64_t), value :: nb
+      real(c_float), intent(in) :: x(*), a(*), tau(*), wt(*)
+      integer(c_int32_t), value :: iters
+      real(c_double), value :: lr
+      real(c_double), intent(out) :: loss_hist(*)
+    end function
     ! batched 1024-point DFT of lines (mode 0: FP32, 1: split-BF16 tensor cores)
     integer(c_int) function psdns_gpu_dft_lines(n, nlines, mode, in, out) bind(c, name='psdns_gpu_dft_lines')
       import :: c_int, c_int32_t, c_int64_t, c_double_complex

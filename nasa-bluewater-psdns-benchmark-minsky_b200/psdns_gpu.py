@@ -68,6 +68,16 @@ EXPORTS = (
     "psdns_gpu_kernel_times",
     "psdns_gpu_rk_stage_noalloc",
     "psdns_gpu_dft_lines",
+    "psdns_gpu_filter_state",
+    "psdns_gpu_shell_factor",
+    "psdns_gpu_corrector_features",
+    "psdns_gpu_corrector_apply",
+    "psdns_gpu_corrector_create",
+    "psdns_gpu_corrector_destroy",
+    "psdns_gpu_corrector_params",
+    "psdns_gpu_corrector_forward",
+    "psdns_gpu_corrector_grad",
+    "psdns_gpu_corrector_train",
     "psdns_gpu_tc_gemm_check",
     "psdns_gpu_forcing_stats",
     "psdns_gpu_spectra",
@@ -134,6 +144,17 @@ def load():
     L.psdns_gpu_spectra.argtypes = [vp, ctypes.c_int32, dp, dp, dp, dp]
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
+    L.psdns_gpu_filter_state.argtypes = [vp, vp]
+    L.psdns_gpu_shell_factor.argtypes = [vp, ctypes.c_int32, dp]
+    fq = ctypes.POINTER(ctypes.c_float)
+    L.psdns_gpu_corrector_features.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, fq]
+    L.psdns_gpu_corrector_apply.argtypes = [vp, vp, dp]
+    L.psdns_gpu_corrector_create.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]
+    L.psdns_gpu_corrector_destroy.argtypes = [vp]
+    L.psdns_gpu_corrector_params.argtypes = [vp, ctypes.c_int32, fq]
+    L.psdns_gpu_corrector_forward.argtypes = [vp, ctypes.c_int64, fq, fq]
+    L.psdns_gpu_corrector_grad.argtypes = [vp, ctypes.c_int64, fq, fq, fq, fq, fq, dp]
+    L.psdns_gpu_corrector_train.argtypes = [vp, ctypes.c_int64, fq, fq, fq, fq, ctypes.c_int32, ctypes.c_double, dp]
     L.psdns_gpu_dft_lines.argtypes = [ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, dp, dp]
     fp = ctypes.POINTER(ctypes.c_float)
     L.psdns_gpu_tc_gemm_check.argtypes = [ctypes.c_int32, fp, fp, fp]
@@ -243,6 +264,82 @@ def tc_gemm_check(a, b, a_mn_major=1):
     _check(load().psdns_gpu_tc_gemm_check(int(a_mn_major), fa.ctypes.data_as(fp), fb.ctypes.data_as(fp),
                                           d.ctypes.data_as(fp)), "psdns_gpu_tc_gemm_check")
     return d
+
+
+CORRECTOR_FEATURES = 3
+CORRECTOR_WIDTH = 32
+CORRECTOR_PARAMS = 2273
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def resolved_shells(n):
+    """Shells 1..K of an n^3 box's truncation sphere: K = int(sqrt(2) n / 3 + 0.5)."""
+    return int(np.sqrt(2.0) * n / 3.0 + 0.5)
+
+
+class Corrector:
+    """The spectral-correction network of the learned coarse solver
+    (psdns_gpu_corrector_*): per-shell features -> eddy viscosity / nu."""
+
+    def __init__(self, seed=1):
+        h = ctypes.c_void_p()
+        _check(load().psdns_gpu_corrector_create(int(seed), ctypes.byref(h)), "psdns_gpu_corrector_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            load().psdns_gpu_corrector_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def get_params(self):
+        w = np.zeros(CORRECTOR_PARAMS, np.float32)
+        _check(load().psdns_gpu_corrector_params(self._h, 1, _fp(w)), "corrector_params")
+        return w
+
+    def set_params(self, w):
+        w = _f32(w)
+        assert w.size == CORRECTOR_PARAMS
+        _check(load().psdns_gpu_corrector_params(self._h, 0, _fp(w)), "corrector_params")
+
+    def forward(self, x):
+        x = _f32(x).reshape(-1, CORRECTOR_FEATURES)
+        g = np.zeros(len(x), np.float32)
+        _check(load().psdns_gpu_corrector_forward(self._h, len(x), _fp(x), _fp(g)), "corrector_forward")
+        return g
+
+    def grad(self, x, a, tau, wt):
+        x = _f32(x).reshape(-1, CORRECTOR_FEATURES)
+        a, tau, wt = _f32(a), _f32(tau), _f32(wt)
+        g = np.zeros(CORRECTOR_PARAMS, np.float32)
+        loss = np.zeros(1)
+        _check(load().psdns_gpu_corrector_grad(self._h, len(x), _fp(x), _fp(a), _fp(tau), _fp(wt), _fp(g), _dp(loss)),
+               "corrector_grad")
+        return g, float(loss[0])
+
+    def train(self, x, a, tau, wt, iters=2000, lr=3e-3):
+        x = _f32(x).reshape(-1, CORRECTOR_FEATURES)
+        a, tau, wt = _f32(a), _f32(tau), _f32(wt)
+        hist = np.zeros(int(iters))
+        _check(load().psdns_gpu_corrector_train(self._h, len(x), _fp(x), _fp(a), _fp(tau), _fp(wt), int(iters),
+                                                float(lr), _dp(hist)), "corrector_train")
+        return hist
 
 
 NOALLOC_MAX_N = 64
@@ -411,6 +508,29 @@ class Solver:
         ek = np.zeros(n); dk = np.zeros(n); e6 = np.zeros(n * 6); st = np.zeros(7)
         _check(load().psdns_gpu_spectra(self._ctx, int(which), _dp(ek), _dp(dk), _dp(e6), _dp(st)), "spectra")
         return ek, dk, e6.reshape(n, 6), dict(zip(["tke", "eps", "skew", "klen", "kvel", "ktime", "ekl"], st))
+
+    def filter_from(self, fine):
+        """This (coarse) box's u and un := fine box's un inside this box's
+        truncation sphere (psdns_gpu_filter_state)."""
+        _check(load().psdns_gpu_filter_state(fine._ctx, self._ctx), "psdns_gpu_filter_state")
+
+    def shell_factor(self, f):
+        """Multiply the modes of shell i (1..len(f)-1) by f[i]."""
+        f = np.ascontiguousarray(f, np.float64)
+        _check(load().psdns_gpu_shell_factor(self._ctx, len(f) - 1, _dp(f)), "psdns_gpu_shell_factor")
+
+    def corrector_features(self, which=FIELD_UN, nshell=None):
+        k = resolved_shells(self.n) if nshell is None else int(nshell)
+        x = np.zeros((k, CORRECTOR_FEATURES), np.float32)
+        _check(load().psdns_gpu_corrector_features(self._ctx, int(which), k, _fp(x)), "corrector_features")
+        return x
+
+    def corrector_apply(self, corr):
+        """Damp the resolved shells by the network's eddy viscosity over the
+        last step's dt; returns (applied, max g)."""
+        info = np.zeros(2)
+        _check(load().psdns_gpu_corrector_apply(corr.handle, self._ctx, _dp(info)), "corrector_apply")
+        return bool(info[0]), float(info[1])
 
     def write_checkpoint(self, path, which=FIELD_UN):
         """One-task pencil file in the reference's format (outpen_write_r.f)."""

@@ -82,7 +82,8 @@ def _f_args():
 # C scalar passed by value -> Fortran kind; C pointee -> Fortran kinds that may bind it
 _BY_VALUE = {"int32_t": "integer(c_int32_t)", "int64_t": "integer(c_int64_t)", "size_t": "integer(c_size_t)",
              "double": "real(c_double)"}
-_BY_REF = {"double": ("real(c_double)", "complex(c_double_complex)"), "int32_t": ("integer(c_int32_t)",),
+_BY_REF = {"double": ("real(c_double)", "complex(c_double_complex)"), "float": ("real(c_float)",),
+           "int32_t": ("integer(c_int32_t)",),
            "int64_t": ("integer(c_int64_t)",), "char": ("character(kind=c_char)",),
            "psdns_params": ("type(psdns_params)",), "void": ("type(c_ptr)",)}
 
