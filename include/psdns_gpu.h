@@ -68,7 +68,9 @@ typedef struct psdns_params {
                                 passes in the state precision) or
                                 PSDNS_DFT_TC_BF16X3 (tensor cores, split BF16,
                                 FP32 state at n = 1024 only)                */
-    int32_t reserved_i[5];
+    int32_t rkmethod;        /* 2 (proc4a/proc4b) or 4 (advanc_1..4, nc = 0,
+                                no particles); 0 means 2 (PSDNS/input.f:222) */
+    int32_t reserved_i[4];
     double viscos;           /* kinematic viscosity                          */
     double beta1, beta2, beta3; /* box scaling; 1 for a 2*pi box             */
     double cfl;              /* > 0: dt = cfl/velmax (PSDNS/step.f:77-78)    */

@@ -230,6 +230,8 @@ int psdns_gpu_ensemble_create(const psdns_params* p, int32_t count, void** out) 
     if (q.precision != PSDNS_PREC_FP32 && q.precision != PSDNS_PREC_FP64) return set_error("box %d: precision", i);
     if (q.nc != 0) return set_error("box %d: ensembles carry no passive scalar (nc = 0)", i);
     if (q.kforce > 0) return set_error("box %d: ensembles are unforced (kforce = 0)", i);
+    if (q.rkmethod == 4 || q.dft != PSDNS_DFT_FP32)
+      return set_error("box %d: ensembles run the RK2 step with the FP32 transforms", i);
     if (q.kshift < 1 || q.kshift > 4) return set_error("box %d: kshift must be 1..4", i);
     if (q.ksran < 1 || q.ksran > 20) return set_error("box %d: RNG sequence must be 1..20", i);
     if (q.seed_input <= 0) return set_error("box %d: seed must be positive", i);

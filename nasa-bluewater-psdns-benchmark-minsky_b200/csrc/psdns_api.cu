@@ -160,6 +160,10 @@ struct Ctx {
   float2* d_tw2 = nullptr;
   unsigned* d_tcerr = nullptr;
   double* d_shf = nullptr;   // per-shell factors of the learned correction
+  // RK scheme (timestep_module.f:295-308): 2 (proc4a/proc4b) or 4
+  // (advanc_1..4, accumulator u1 of comp_set.f:72 in d_u1)
+  int rk = 2;
+  void* d_u1 = nullptr;
   unsigned long long* d_velmax = nullptr;
   void* h_tabs = nullptr;          // pinned staging of the stage tables
   unsigned long long* h_velmax = nullptr;
@@ -185,7 +189,7 @@ struct Ctx {
   double erate = 0, eirate[3] = {0, 0, 0};
   // per-kernel CUDA-event timing: [stage][kernel][begin/end]
   bool prof = false;
-  cudaEvent_t ev[2][6][2] = {};
+  cudaEvent_t ev[4][6][2] = {};   // RK4 has four stages
   // asynchronous state copies: copy streams, complex(8) staging of the whole
   // state in each direction, per-chunk events (allocated on first use)
   static constexpr int kChunks = 12;
@@ -204,7 +208,7 @@ struct Ctx {
   bool pend_sphere = false;          // the pending download was a sphere copy
   double prof_ms[6] = {0, 0, 0, 0, 0, 0};
   long long prof_n[6] = {0, 0, 0, 0, 0, 0};
-  bool prof_pending[2] = {false, false};
+  bool prof_pending[4] = {false, false, false, false};
 };
 
 static void prof_mark(Ctx& c, int stage, int k, int end) {
@@ -353,6 +357,12 @@ template <typename T, int N, int NC> struct Impl {
     CK(cudaFuncSetAttribute(k_xchain<T, N, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3()));
     CK(cudaFuncSetAttribute(k_zfwd<T, N, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm4()));
     CK(cudaFuncSetAttribute(k_yfwd<T, N, 1, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
+    if constexpr (NC == 0) {
+      CK(cudaFuncSetAttribute(k_yfwd<T, N, 11>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
+      CK(cudaFuncSetAttribute(k_yfwd<T, N, 12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
+      CK(cudaFuncSetAttribute(k_yfwd<T, N, 13>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
+      CK(cudaFuncSetAttribute(k_yfwd<T, N, 14>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
+    }
     CK(cudaFuncSetAttribute(k_yfwd<T, N, 2, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm5()));
     CK(cudaFuncSetAttribute(k_zinv<T, N, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2()));
     CK(cudaFuncSetAttribute(k_yfwd<T, N, 0, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -485,7 +495,7 @@ template <typename T, int N, int NC> struct Impl {
     if constexpr (kTc)
       if (c.dft == PSDNS_DFT_TC_BF16X3) return stage_a_tc(c, kstep);
     Geo g = make_geo(c);
-    StageTables<T> st = make_tables<T>(c, kstep - 1);
+    StageTables<T> st = make_tables<T>(c, (kstep - 1) & 1);
     const C* tw = (const C*)c.d_tw;
     C* u = (C*)c.d_u;
     C* ub = (C*)c.d_ub;
@@ -530,7 +540,7 @@ template <typename T, int N, int NC> struct Impl {
   // grids as stage_a)
   static int stage_a_tc(Ctx& c, int kstep) {
     Geo g = make_geo(c);
-    StageTables<T> st = make_tables<T>(c, kstep - 1);
+    StageTables<T> st = make_tables<T>(c, (kstep - 1) & 1);
     const TcArgs ta = tc_args(c);
     const C* tw = (const C*)c.d_tw;
     C* u = (C*)c.d_u;
@@ -564,7 +574,7 @@ template <typename T, int N, int NC> struct Impl {
 
   static int stage_b_tc(Ctx& c, int kstep) {
     Geo g = make_geo(c);
-    StageTables<T> st = make_tables<T>(c, kstep - 1);
+    StageTables<T> st = make_tables<T>(c, (kstep - 1) & 1);
     const TcArgs ta = tc_args(c);
     constexpr int TH = K5Launch<T, N, NC>::THREADS;
     prof_mark(c, kstep - 1, 4, 0);
@@ -580,11 +590,36 @@ template <typename T, int N, int NC> struct Impl {
   }
 
   // stage part B: K5
+  // K5 of the RK4 sub-stages (velocity only)
+  static int stage_b_rk4(Ctx& c, int kstep) {
+    if constexpr (NC == 0) {
+      Geo g = make_geo(c);
+      StageTables<T> st = make_tables<T>(c, (kstep - 1) & 1);
+      constexpr int TH = K5Launch<T, N, NC>::THREADS;
+      const C* ub = (const C*)c.d_ub;
+      C *u = (C*)c.d_u, *un = (C*)c.d_un, *r = (C*)c.d_u1;
+      const C* tw = (const C*)c.d_tw;
+      prof_mark(c, kstep - 1, 4, 0);
+      switch (kstep) {
+        case 1: k_yfwd<T, N, 11><<<c.nab_f, TH, sm5(), c.stream>>>(g, st, ub, u, un, tw, c.d_efkz, TcArgs(), r); break;
+        case 2: k_yfwd<T, N, 12><<<c.nab_f, TH, sm5(), c.stream>>>(g, st, ub, u, un, tw, c.d_efkz, TcArgs(), r); break;
+        case 3: k_yfwd<T, N, 13><<<c.nab_f, TH, sm5(), c.stream>>>(g, st, ub, u, un, tw, c.d_efkz, TcArgs(), r); break;
+        default: k_yfwd<T, N, 14><<<c.nab_f, TH, sm5(), c.stream>>>(g, st, ub, u, un, tw, c.d_efkz, TcArgs(), r);
+      }
+      prof_mark(c, kstep - 1, 4, 1);
+      CK(cudaGetLastError());
+      return 0;
+    } else {
+      return set_error("RK4 advances the velocity only (nc = 0)");
+    }
+  }
+
   static int stage_b(Ctx& c, int kstep) {
+    if (c.rk == 4) return stage_b_rk4(c, kstep);
     if constexpr (kTc)
       if (c.dft == PSDNS_DFT_TC_BF16X3) return stage_b_tc(c, kstep);
     Geo g = make_geo(c);
-    StageTables<T> st = make_tables<T>(c, kstep - 1);
+    StageTables<T> st = make_tables<T>(c, (kstep - 1) & 1);
     constexpr int TH = K5Launch<T, N, NC>::THREADS;
     prof_mark(c, kstep - 1, 4, 0);
     if (kstep == 1)
@@ -1202,6 +1237,10 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
     return set_error("RNG sequence numbers must be 1..20 (ranseq.f:131)");
   if (p->seed_input <= 0) return set_error("seed iseed=%d must be positive (ranu.f:33)", p->seed_input);
   if (p->cfl <= 0. && !(p->dt > 0.)) return set_error("fixed dt must be positive when cfl <= 0");
+  if (p->rkmethod != 0 && p->rkmethod != 2 && p->rkmethod != 4)
+    return set_error("rkmethod must be 2 or 4 (0: 2)");
+  if (p->rkmethod == 4 && (p->nc != 0 || p->dft != PSDNS_DFT_FP32))
+    return set_error("RK4 advances the velocity only (nc = 0) with the FP32 transforms");
   if (p->dft != PSDNS_DFT_FP32 && p->dft != PSDNS_DFT_TC_BF16X3)
     return set_error("dft must be PSDNS_DFT_FP32 or PSDNS_DFT_TC_BF16X3");
   if (p->dft == PSDNS_DFT_TC_BF16X3 && (p->precision != PSDNS_PREC_FP32 || p->nx != 1024))
@@ -1278,6 +1317,11 @@ int psdns_gpu_init(const psdns_params* p, void** out) {
     return fail(set_error("geometry upload failed"));
   if (o.twiddles(*c)) return fail(1);
   c->dft = p->dft;
+  c->rk = p->rkmethod == 4 ? 4 : 2;
+  if (c->rk == 4) {
+    ALLOC2(c->d_u1, c->csz * c->st_elems);
+    if (cudaMemset(c->d_u1, 0, c->csz * c->st_elems) != cudaSuccess) return fail(set_error("memset failed"));
+  }
   if (c->dft == PSDNS_DFT_TC_BF16X3) {
     std::vector<uint16_t> bt(tc::kBBytes / 2);
     std::vector<float2> tw2(1024);
@@ -1322,10 +1366,10 @@ int psdns_gpu_finalize(void* ctx) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->d_colstart, c->d_ax, c->d_az, c->d_kymax, c->d_tw, c->d_tabs, c->d_u, c->d_un,
                   c->d_ub, c->d_uz, c->d_forc, c->d_efkz, c->d_velmax, c->d_pos, c->d_vel, c->d_bs, c->d_spf,
-                  c->d_tcb, c->d_tw2, c->d_tcerr, c->d_shf};
+                  c->d_tcb, c->d_tw2, c->d_tcerr, c->d_shf, c->d_u1};
   for (void* q : ptrs)
     if (q) cudaFree(q);
-  for (int s = 0; s < 2; s++)
+  for (int s = 0; s < 4; s++)
     for (int k = 0; k < 6; k++)
       for (int e = 0; e < 2; e++)
         if (c->ev[s][k][e]) cudaEventDestroy(c->ev[s][k][e]);
@@ -1743,11 +1787,11 @@ int psdns_gpu_step(void* ctx, double* info) {
   }
   if (upload_tables(*c)) return 1;
   int ctl = 0;
-  if (run_stage(*c, o, 1, &ctl)) return 1;
-  if (run_stage(*c, o, 2, &ctl)) return 1;
+  for (int k = 1; k <= c->rk; k++)
+    if (run_stage(*c, o, k, &ctl)) return 1;
   CK(cudaStreamSynchronize(c->stream));
   prof_collect(*c, 0, 4, 5);
-  prof_collect(*c, 1, 0, 5);
+  for (int k = 1; k < c->rk; k++) prof_collect(*c, k, 0, 5);
   if (collect_forcing_stats(*c)) return 1;
   if (info) {
     info[0] = c->dt;
@@ -1767,7 +1811,7 @@ int psdns_gpu_rk_stage(void* ctx, int32_t kstep, const double* gsh, const double
   Ctx* c = (Ctx*)ctx;
   touch(c);
   if (!c || !gsh) return set_error("null argument");
-  if (kstep != 1 && kstep != 2) return set_error("kstep must be 1 or 2");
+  if (kstep < 1 || kstep > c->rk) return set_error("kstep must be 1 .. %d (rkmethod)", c->rk);
   if (forcing != nullptr && !(c->p.kforce > 0))
     return set_error("a forcing table was passed but the context was created with kforce = 0");
   Ops o;
@@ -1896,6 +1940,7 @@ int psdns_gpu_particles_set(void* ctx, int64_t np, const double* pos) {
   touch(c);
   if (!c) return set_error("null context");
   if (np < 0) return set_error("negative particle count");
+  if (np > 0 && c->rk != 2) return set_error("particles are advanced with the RK2 step only");
   if (np > 0 && !pos) return set_error("null positions");
   if (c->d_pos) { cudaFree(c->d_pos); c->d_pos = nullptr; }
   if (c->d_vel) { cudaFree(c->d_vel); c->d_vel = nullptr; }
@@ -1923,6 +1968,7 @@ int psdns_gpu_particles_init(void* ctx, int64_t nop, int32_t pstart, int32_t kip
   touch(c);
   if (!c) return set_error("null context");
   if (pstart != 0 && pstart != -1) return set_error("pstart must be 0 (random) or -1 (lattice)");
+  if (c->rk != 2) return set_error("particles are advanced with the RK2 step only");
   if (nop <= 0) return set_error("nop must be positive");
   if (kipran < 1 || kipran > 20) return set_error("kipran must be 1..20 (ranseq.f:131)");
   const long long tot = pstart == -1 ? (long long)nop * nop * nop : nop;
@@ -2036,7 +2082,7 @@ int psdns_gpu_profile(void* ctx, int32_t enable) {
   touch(c);
   if (!c) return set_error("null context");
   if (enable && !c->ev[0][0][0]) {
-    for (int s = 0; s < 2; s++)
+    for (int s = 0; s < 4; s++)
       for (int k = 0; k < 6; k++)
         for (int e = 0; e < 2; e++) CK(cudaEventCreate(&c->ev[s][k][e]));
   }

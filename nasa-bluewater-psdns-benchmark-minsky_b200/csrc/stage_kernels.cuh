@@ -746,7 +746,17 @@ __device__ __forceinline__ void project3(C2<T>& u1, C2<T>& u2, C2<T>& u3, T kx, 
 template <typename T, int N, int KSTEP, int NC = 0, bool TCM = false>
 __global__ void __launch_bounds__(K5Launch<T, N, NC>::THREADS)
 k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __restrict__ u,
-       C2<T>* __restrict__ un, const C2<T>* __restrict__ tw_g, double* __restrict__ efkz, TcArgs tca = TcArgs()) {
+       C2<T>* __restrict__ un, const C2<T>* __restrict__ tw_g, double* __restrict__ efkz, TcArgs tca = TcArgs(),
+       C2<T>* __restrict__ racc = nullptr) {
+  // KSTEP = 11 .. 14: the RK4 sub-stages advanc_1 .. advanc_4
+  // (homogeneous/advanc_1.f .. advanc_4.f, -DRKFOUR), velocity only (NC = 0);
+  // racc is their accumulator u1 (comp_set.f:72):
+  //   11: racc = f (un + w/3), u = f (un + w), f = xfac yfac zfac; u
+  //       projected; forcing (with efkz) added to u
+  //   12, 13: racc += w*2/3, u = un + w (12) or un + w*2 (13); u projected;
+  //       forcing added to u
+  //   14: racc += w*1/3, projected; un = u = racc, mean mode zeroed (the
+  //       forcing that advanc_4.f adds to u is overwritten by that copy)
   // grid (nab_f, boxes); forcing (efkz) is for single boxes only.
   // KSTEP = 0: transfer spectrum only (trfsp.f:62-83): the shell sums of
   // tfact Re(conj(un) . w) go to efkz[n/2] (shell ik = int(|k|/st.tdk + 1.5));
@@ -851,7 +861,36 @@ k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __rest
       continue;
     }
     C u1, u2, u3;
-    if constexpr (KSTEP == 1) {
+    constexpr bool RK4 = KSTEP >= 11;
+    C r1 = cmk<C>(0, 0), r2 = cmk<C>(0, 0), r3 = cmk<C>(0, 0);
+    if constexpr (RK4) {
+      static_assert(NC == 0, "RK4 advances the velocity only");
+      if constexpr (KSTEP == 11) {
+        const T f = __ldg(st.xfac + x) * __ldg(st.yfac + y) * __ldg(st.zfac + z);
+        r1 = cscale(f, cadd(n1, cmk<C>(w1.x / T(3), w1.y / T(3))));
+        r2 = cscale(f, cadd(n2, cmk<C>(w2.x / T(3), w2.y / T(3))));
+        r3 = cscale(f, cadd(n3, cmk<C>(w3.x / T(3), w3.y / T(3))));
+        u1 = cscale(f, cadd(n1, w1));
+        u2 = cscale(f, cadd(n2, w2));
+        u3 = cscale(f, cadd(n3, w3));
+      } else {
+        r1 = racc[o];
+        r2 = racc[vs + o];
+        r3 = racc[2 * vs + o];
+        constexpr T cw = KSTEP == 14 ? T(1) : T(2);
+        r1 = cadd(r1, cmk<C>(w1.x * cw / T(3), w1.y * cw / T(3)));
+        r2 = cadd(r2, cmk<C>(w2.x * cw / T(3), w2.y * cw / T(3)));
+        r3 = cadd(r3, cmk<C>(w3.x * cw / T(3), w3.y * cw / T(3)));
+        if constexpr (KSTEP == 14) {
+          u1 = r1; u2 = r2; u3 = r3;
+        } else {
+          constexpr T cu = KSTEP == 12 ? T(1) : T(2);
+          u1 = cadd(n1, cmk<C>(w1.x * cu, w1.y * cu));
+          u2 = cadd(n2, cmk<C>(w2.x * cu, w2.y * cu));
+          u3 = cadd(n3, cmk<C>(w3.x * cu, w3.y * cu));
+        }
+      }
+    } else if constexpr (KSTEP == 1) {
       // proc4a.f:427, 479-486
       const T f = k0 ? T(1) : __ldg(st.xfac + x) * __ldg(st.yfac + y) * __ldg(st.zfac + z);
       u1 = cscale(f, cmk<C>(n1.x + T(2) * w1.x, n1.y + T(2) * w1.y));
@@ -867,15 +906,16 @@ k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __rest
       u3 = cadd(n3, w3);
     }
     if (!k0) project3<T>(u1, u2, u3, kx, ky, kz, st.b11, st.b22, st.b33);
-    // Eswaran-Pope forcing (proc4a.f:588-651, proc4b.f:118-163)
-    if (st.forc != nullptr && x < st.kfor) {
+    // Eswaran-Pope forcing (proc4a.f:588-651, proc4b.f:118-163; advanc_1.f:164-216)
+    constexpr bool FIRST = KSTEP == 1 || KSTEP == 11;
+    if (KSTEP != 14 && st.forc != nullptr && x < st.kfor) {
       const int kf = st.kfor, k2 = st.k2fo;
       int izi = (ikz >= 0 && ikz < kf) ? ikz : ((ikz < 0 && ikz > -kf) ? ikz + k2 : -1);
       int iyi = (iky >= 0 && iky < kf) ? iky : ((iky < 0 && iky > -kf) ? iky + k2 : -1);
       if (izi >= 0 && iyi >= 0) {
         bool add = true;
         double rks = 0.0;
-        if constexpr (KSTEP == 1) {
+        if constexpr (FIRST) {
           rks = (double)x * x * (double)st.b11 + (double)iky * iky * (double)st.b22 +
                 (double)ikz * ikz * (double)st.b33;
           add = rks <= st.kforce2;
@@ -884,7 +924,7 @@ k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __rest
           const size_t fo = ((size_t)izi * k2 + iyi) * kf + x;
           const size_t fs = (size_t)kf * k2 * k2;
           const C f1 = st.forc[fo], f2 = st.forc[fs + fo], f3 = st.forc[2 * fs + fo];
-          if constexpr (KSTEP == 1) {
+          if constexpr (FIRST) {
             if (efkz != nullptr) {
               const int kk = (int)(sqrt(rks) + 1.5);
               const double tf = (x == 0) ? 1.0 : 2.0;
@@ -918,14 +958,18 @@ k_yfwd(Geo g, StageTables<T> st_all, const C2<T>* __restrict__ ub, C2<T>* __rest
       u[3 * vs + o] = u4;
       un[3 * vs + o] = n4;
     }
-    if constexpr (KSTEP == 2) {
+    if constexpr (KSTEP == 2 || KSTEP == 14) {
       if (k0) {
         u1 = u2 = u3 = cmk<C>(0, 0);
       }
       n1 = u1; n2 = u2; n3 = u3;
     }
     u[o] = u1; u[vs + o] = u2; u[2 * vs + o] = u3;
-    un[o] = n1; un[vs + o] = n2; un[2 * vs + o] = n3;
+    if constexpr (RK4 && KSTEP != 14) {
+      racc[o] = r1; racc[vs + o] = r2; racc[2 * vs + o] = r3;
+    } else {
+      un[o] = n1; un[vs + o] = n2; un[2 * vs + o] = n3;
+    }
   }
   if constexpr (KSTEP == 0) {
     __syncthreads();

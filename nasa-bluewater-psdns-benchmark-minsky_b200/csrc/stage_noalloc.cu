@@ -239,6 +239,7 @@ extern "C" int psdns_gpu_rk_stage_noalloc(const psdns_params* p, int32_t kstep, 
   if (p->nx != p->ny || p->nx != p->nz) return set_error("noalloc: only cubic boxes are supported");
   if (p->nc != 0) return set_error("noalloc: passive scalars are not supported");
   if (p->kforce > 0) return set_error("noalloc: forcing is not supported by this entry point");
+  if (p->rkmethod == 4) return set_error("noalloc: this entry point runs the RK2 stages");
   const int n = p->nx;
   if (n > noalloc::kMaxN)
     return set_error("noalloc: grid %d^3 exceeds the largest box the static scratch holds (%d^3)", n,

@@ -16,8 +16,8 @@ module psdns_gpu_mod
   type, bind(c) :: psdns_params
     integer(c_int32_t) :: nx, ny, nz, nc, precision, kshift, ksran, seed_input
     integer(c_int32_t) :: kranf1, kranf2
-    integer(c_int32_t) :: dft
-    integer(c_int32_t) :: reserved_i(5)
+    integer(c_int32_t) :: dft, rkmethod
+    integer(c_int32_t) :: reserved_i(4)
     real(c_double) :: viscos, beta1, beta2, beta3, cfl, dt
     real(c_double) :: kforce, tforce, epsfor, tfiuo, pr
     real(c_double) :: grad(3)

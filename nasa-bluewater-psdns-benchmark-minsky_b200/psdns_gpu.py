@@ -94,7 +94,7 @@ class Params(ctypes.Structure):
         ("nc", ctypes.c_int32), ("precision", ctypes.c_int32), ("kshift", ctypes.c_int32),
         ("ksran", ctypes.c_int32), ("seed_input", ctypes.c_int32),
         ("kranf1", ctypes.c_int32), ("kranf2", ctypes.c_int32),
-        ("dft", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 5),
+        ("dft", ctypes.c_int32), ("rkmethod", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 4),
         ("viscos", ctypes.c_double), ("beta1", ctypes.c_double), ("beta2", ctypes.c_double),
         ("beta3", ctypes.c_double), ("cfl", ctypes.c_double), ("dt", ctypes.c_double),
         ("kforce", ctypes.c_double), ("tforce", ctypes.c_double), ("epsfor", ctypes.c_double),

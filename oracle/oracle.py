@@ -48,6 +48,7 @@ def lib():
         L.orc_get_scalars.argtypes = [vp, dp]
         L.orc_step.argtypes = [vp]
         L.orc_stage.argtypes = [vp, ctypes.c_int]
+        L.orc_set_rkmethod.argtypes = [vp, ctypes.c_int]
         L.orc_set_shifts.argtypes = [vp, dp]
         L.orc_itransform_only.argtypes = [vp, ctypes.c_int, dp, dp]
         L.orc_fft.argtypes = [dp, ctypes.c_int, ctypes.c_int]
@@ -105,12 +106,14 @@ class Oracle:
     """One periodic box advanced by the FP64 restatement of the RK2 step."""
 
     def __init__(self, n, viscos, cfl=-1.0, dt=0.005, kshift=1, seed_input=122929298, ksran=1,
-                 beta=(1.0, 1.0, 1.0)):
+                 beta=(1.0, 1.0, 1.0), rkmethod=2):
         self.n = n
         self.nc = 0
         self._c = lib().orc_create(n, viscos, cfl, dt, kshift, seed_input, ksran, *beta)
         self.kxn = lib().orc_kxn(self._c)
         self.xz_tot = lib().orc_xz_tot(self._c)
+        if rkmethod != 2:
+            assert lib().orc_set_rkmethod(self._c, int(rkmethod)) == 0, "rkmethod must be 2 or 4 (4: no scalar)"
 
     def close(self):
         if self._c:

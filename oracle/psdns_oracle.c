@@ -200,6 +200,10 @@ typedef struct {
     int part_first;
     long pin_nop;          /* partin request pending at the first particle phase */
     int pin_pstart, pin_kipran;
+    /* timestep_module.f:295-308: rkmethod 2 (proc4a/proc4b) or 4
+     * (advanc_1..4 with the accumulator u1 of comp_set.f:72) */
+    int rkmethod;
+    cx *u1;
 } orc_ctx;
 
 static int mask_ok(const orc_ctx *c, int a, int y)
@@ -302,7 +306,7 @@ void orc_destroy(orc_ctx *c)
 {
     if (!c) return;
     free(c->kx); free(c->ky); free(c->kz); free(c->cut); free(c->kc); free(c->colstart);
-    free(c->ax); free(c->az); free(c->kymax); free(c->u); free(c->un);
+    free(c->ax); free(c->az); free(c->kymax); free(c->u); free(c->un); free(c->u1);
     free(c->sx); free(c->sy); free(c->sz); free(c->xfac); free(c->yfac); free(c->zfac);
     free(c->xdif); free(c->ydif); free(c->zdif);
     free(c->tw.w);
@@ -798,6 +802,70 @@ static void proc4b(orc_ctx *c, cx *w, cx *un)
     if (c->nc) { w[4 * vs] = CZERO; un[3 * vs] = CZERO; }
 }
 
+
+/* RK4 (-DRKFOUR), homogeneous/advanc_1.f..advanc_4.f as written, nc = 0.
+ * w holds the stage's wavespace term (dt/2 attached), u1 the accumulator.
+ * advanc_1.f:102-117: f = xfac yfac zfac; u1 = f (un + w/3), u = f (un + w);
+ *   projection of u (:131-156, the mean mode skipped); forcing with efkz
+ *   (:164-216).
+ * advanc_2.f/advanc_3.f:46-54: u1 = u1 + w*2/3; u = un + w (stage 2) or
+ *   un + w*2 (stage 3); projection of u (:62-82); forcing without the
+ *   |k| <= kforce test (:94-141).
+ * advanc_4.f:46-54: u1 = u1 + w*1/3; projection of u1 (:62-82); the forcing
+ *   is added to u (:94-141) and then overwritten by the copy
+ *   un = u = u1 (:149-161); the mean mode of u and un is zeroed (:168-174). */
+static void advanc(orc_ctx *c, int kstep, cx *w, cx *un, cx *u1)
+{
+    int n = c->n, tot = c->xz_tot;
+    size_t vs = (size_t)tot * n;
+    #pragma omp parallel for schedule(static)
+    for (int a = 0; a < tot; a++) {
+        int x = c->ax[a], z = c->az[a];
+        for (int y = 0; y < n; y++) {
+            if (!mask_ok(c, a, y)) continue;
+            double f = c->xfac[x] * c->yfac[y] * c->zfac[z];
+            for (int i = 0; i < 3; i++) {
+                size_t o = i * vs + (size_t)a * n + y;
+                cx wv = w[o];
+                if (kstep == 1) {
+                    cx untemp = un[o];
+                    u1[o] = cscale(f, cadd(untemp, cmk(wv.re / 3., wv.im / 3.)));
+                    w[o] = cscale(f, cadd(untemp, wv));
+                } else if (kstep == 2 || kstep == 3) {
+                    u1[o] = cadd(u1[o], cmk(wv.re * 2. / 3., wv.im * 2. / 3.));
+                    w[o] = kstep == 2 ? cadd(un[o], wv) : cadd(un[o], cmk(wv.re * 2., wv.im * 2.));
+                } else {
+                    u1[o] = cadd(u1[o], cmk(wv.re * 1. / 3., wv.im * 1. / 3.));
+                }
+            }
+            if (a == 0 && y == 0) continue;
+            project(c, kstep == 4 ? u1 : w, a, y);
+        }
+    }
+    add_forcing(c, w, kstep == 1);
+    if (kstep == 4) {
+        #pragma omp parallel for schedule(static)
+        for (int a = 0; a < tot; a++)
+            for (int y = 0; y < n; y++) {
+                if (!mask_ok(c, a, y)) continue;
+                for (int i = 0; i < 3; i++) {
+                    size_t o = i * vs + (size_t)a * n + y;
+                    un[o] = u1[o];
+                    w[o] = u1[o];
+                }
+            }
+        for (int i = 0; i < 3; i++) { w[i * vs] = CZERO; un[i * vs] = CZERO; }
+    }
+}
+
+int orc_set_rkmethod(orc_ctx *c, int rk)
+{
+    if (rk != 2 && rk != 4) return 1;
+    if (rk == 4 && c->nc != 0) return 2;
+    c->rkmethod = rk;
+    if (rk == 4 && !c->u1) c->u1 = (cx *)calloc((size_t)3 * c->xz_tot * c->n, sizeof(cx));
+    return 0;
+}
 
 /* ------------------------------------------------------------------------ */
 /* Eswaran-Pope forcing                                                     */
@@ -1302,7 +1370,9 @@ static void particles_stage1(orc_ctx *c, const double *p)
 static int rk_stage(orc_ctx *c, int kstep)
 {
     int n = c->n, tot = c->xz_tot;
-    int ks = kstep - 1;
+    /* RK4: stages 3 and 4 reuse the shifts of stages 1 and 2
+     * (shifts.f:133-136, gsh(:,3) = gsh(:,1), gsh(:,4) = gsh(:,2)) */
+    int ks = (kstep - 1) % 2;
     size_t vs = (size_t)tot * n;
     size_t np = (size_t)n * n * n;
     int nc = c->nc;
@@ -1331,7 +1401,8 @@ static int rk_stage(orc_ctx *c, int kstep)
     int err = 0;
     if (kstep == 1) { err = step_control(c); force(c); }
     wavespace(c, w, ks);
-    if (kstep == 1) proc4a(c, w, c->un);
+    if (c->rkmethod == 4) advanc(c, kstep, w, c->un, c->u1);
+    else if (kstep == 1) proc4a(c, w, c->un);
     else proc4b(c, w, c->un);
     memcpy(c->u, w, sizeof(cx) * 3 * vs);
     if (nc) memcpy(c->u + 3 * vs, w + 4 * vs, sizeof(cx) * vs);
@@ -1345,9 +1416,12 @@ int orc_step(orc_ctx *c)
 {
     c->jstep += 1;
     shifts(c);
-    int e1 = rk_stage(c, 1);
-    int e2 = rk_stage(c, 2);
-    c->status = e1 ? e1 : e2;
+    int e = rk_stage(c, 1);
+    for (int k = 2; k <= (c->rkmethod == 4 ? 4 : 2); k++) {
+        int ek = rk_stage(c, k);
+        if (!e) e = ek;
+    }
+    c->status = e;
     return c->status;
 }
 
