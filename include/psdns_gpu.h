@@ -357,6 +357,33 @@ int psdns_gpu_particles_init(void *ctx, int64_t nop, int32_t pstart, int32_t kip
  * e.g. outpen/0/outpenc.p0.  write: u or un of the context; read: sets un
  * and u (modes outside the truncation cylinder are dropped).  path is a
  * NUL-terminated file name. */
+/* Multi-task pencil sets (homogeneous/outpen_write_r.f, inpen_read_r.f):
+ * write_checkpoint_set writes iproc*jproc files "<prefix>.p<t>", task
+ * t = jp*iproc + ip holding x in [ip xisz, (ip+1) xisz) and z in
+ * [jp zjsz, (jp+1) zjsz), xisz = (n/2)/iproc, zjsz = n/jproc, each in the
+ * one-task file's record layout with its own xist/xisz/zjst/zjsz header;
+ * read_checkpoint_set reads any set of such files (paths[nfiles]), placing
+ * each pencil by its header, and checks that the set covers every (x, z)
+ * of the box once. */
+int psdns_gpu_write_checkpoint_set(void *ctx, const char *prefix, int32_t iproc, int32_t jproc, int32_t which);
+int psdns_gpu_read_checkpoint_set(void *ctx, const char *const *paths, int32_t nfiles);
+/* Checkpoint metadata.  write_chkptou: PSDNS/store.f icall 1 + 2 (called
+ * at PSDNS/main.f:583): the integers nx ny nz my mz nxhvs nyvs nzvs nc ncd
+ * kfor iostep kshift and istep (format 10i8; my..nzvs are never set by
+ * store.f and are written as 0) and the reals viscos pr a11 a22 a33 shear
+ * grad beta1-3 cfl dt tforce epsfor kforce tfiuo, then time gsh(:,2)
+ * b11 b22 b33 b12 (2 each) and the forcing processes suo svo (format
+ * 1p5e15.8).  read_chkptou: store.f icall 3 (incond.f:262): with strict,
+ * the stored parameters must be this run's (kstop = 1, store.f:272-301);
+ * restores time, gsh(:,2), suo and svo, returns istep in *istep, and makes
+ * the next step the first of a restarted run (no initial shift draw,
+ * shifts.f:47; forcing processes kept, vfuo.f/vfiuo.f with istart > 0).
+ * write_ranout / read_ranin: the 20 RNG seeds of PSDNS/ranseq.f (k = -2,
+ * :174-183, and k = -1, :83-118; format 5i15). */
+int psdns_gpu_write_chkptou(void *ctx, const char *path, int32_t istep, int32_t iostep);
+int psdns_gpu_read_chkptou(void *ctx, const char *path, int32_t strict, int32_t *istep);
+int psdns_gpu_write_ranout(void *ctx, const char *path);
+int psdns_gpu_read_ranin(void *ctx, const char *path);
 int psdns_gpu_write_checkpoint(void *ctx, const char *path, int32_t which);
 int psdns_gpu_read_checkpoint(void *ctx, const char *path);
 

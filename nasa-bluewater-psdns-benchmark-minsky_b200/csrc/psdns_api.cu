@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <algorithm>
 #include <new>
@@ -174,6 +175,10 @@ struct Ctx {
   double gsh[3][2] = {{0, 0}, {0, 0}, {0, 0}}, gsh4[3][2] = {{0, 0}, {0, 0}, {0, 0}};
   int jstep = 0;
   double time = 0, dt = 0, dt0 = 0, dt2 = 0, velmax = 0;
+  // > 0 after a restart from chkptin/ranin (store.f icall 3): the first
+  // step draws no initial gsh(:,2) (shifts.f:47) and the forcing keeps the
+  // restored processes (vfuo.f, vfiuo.f: istart > 0)
+  int istart = 0;
   int kfor = 0, k2fo = 0;
   EPForcing forcing;
   // Lagrangian particles (positions/velocities FP64, spline coefficients in
@@ -700,7 +705,7 @@ static double cancel(double d) { return std::fmod(d + 0.5, 1.); }
 
 static void draw_shifts(Ctx& c) {
   const int ks = c.p.kshift;
-  if (c.jstep == 1 && (ks == 1 || ks == 3)) {
+  if (c.istart <= 0 && c.jstep == 1 && (ks == 1 || ks == 3)) {
     c.rng.ranseq(c.p.ksran);
     for (int i = 0; i < 3; i++) c.gsh[i][1] = c.rng.ranu();
     for (int i = 0; i < 3; i++) c.gsh4[i][1] = c.rng.ranu();
@@ -880,7 +885,7 @@ static int run_stage(Ctx& c, const Ops& o, int kstep, int* ctl_err) {
     if (upload_tables(c)) return 1;
     if (c.p.kforce > 0) {
       // force.f, called after step at stage 1 (timestep_module.f:261-263)
-      c.forcing.step(c.rng, c.dt, 0);
+      c.forcing.step(c.rng, c.dt, c.istart);
       if (upload_forcing(c, c.forcing.table.data())) return 1;
       CK(cudaMemsetAsync(c.d_efkz, 0, sizeof(double) * 3 * (c.n / 2 + 2), c.stream));
     }
@@ -1714,6 +1719,334 @@ int psdns_gpu_read_checkpoint(void* ctx, const char* path) {
     if (!err && full_var_set(*c, v, full.data())) err = 1;
   }
   std::fclose(f);
+  return err;
+}
+
+// ---------------------------------------------------------------------------
+// Checkpoint metadata (store.f, ranseq.f) and multi-task pencil sets
+// (homogeneous/outpen_write_r.f, inpen_read_r.f)
+// ---------------------------------------------------------------------------
+// store.f:347-348: format 900 = (10i8), format 910 = (1p,5e15.8)
+static bool fmt_ints(FILE* f, const std::vector<long long>& v, int per, int w) {
+  for (size_t i = 0; i < v.size(); i++) {
+    if (std::fprintf(f, "%*lld", w, v[i]) < 0) return false;
+    if ((i + 1) % per == 0 || i + 1 == v.size())
+      if (std::fputc('\n', f) == EOF) return false;
+  }
+  return true;
+}
+static bool fmt_reals(FILE* f, const std::vector<double>& v) {
+  for (size_t i = 0; i < v.size(); i++) {
+    if (std::fprintf(f, "%15.8E", v[i]) < 0) return false;
+    if ((i + 1) % 5 == 0 || i + 1 == v.size())
+      if (std::fputc('\n', f) == EOF) return false;
+  }
+  return true;
+}
+// fixed-width fields, `per` to a line (Fortran list of a repeated format)
+static bool read_fields(FILE* f, size_t count, int per, int w, std::vector<std::string>& out) {
+  out.clear();
+  char line[4096];
+  while (out.size() < count) {
+    if (!std::fgets(line, sizeof line, f)) return false;
+    std::string l(line);
+    while (!l.empty() && (l.back() == '\n' || l.back() == '\r')) l.pop_back();
+    for (int k = 0; k < per && out.size() < count; k++) {
+      if ((size_t)(k + 1) * w > l.size()) {
+        if ((size_t)k * w >= l.size()) break;
+      }
+      out.push_back(l.substr((size_t)k * w, (size_t)w));
+    }
+  }
+  return true;
+}
+static bool parse_real(const std::string& s, double& d) {
+  std::string t = s;
+  for (char& ch : t)
+    if (ch == 'D' || ch == 'd') ch = 'E';
+  char* e = nullptr;
+  d = std::strtod(t.c_str(), &e);
+  return e != t.c_str();
+}
+
+// the store.f record of a context: isdata (icall 1 then istep), rsdata
+// (icall 1 then time, gsh(:,2), b11 b22 b33 b12 (2 each), suo, svo)
+static void store_data(const Ctx& c, int istep, int iostep, std::vector<long long>& is, int& nic2,
+                       std::vector<double>& rs, int& nrc2) {
+  const psdns_params& p = c.p;
+  const int ncd = p.nc == 0 ? 1 : p.nc;   // param_set.f:19-24
+  // my, mz, nxhvs, nyvs, nzvs are locals that store.f never sets; 0 here
+  is = {p.nx, p.ny, p.nz, 0, 0, 0, 0, 0, p.nc, ncd, c.kfor, iostep, p.kshift};
+  nic2 = (int)is.size();
+  is.push_back(istep);
+  rs.clear();
+  rs.push_back(p.viscos);
+  for (int i = 0; i < ncd; i++) rs.push_back(p.pr);
+  for (int i = 0; i < 4; i++) rs.push_back(0.0);   // a11, a22, a33, shear
+  for (int i = 0; i < ncd; i++)
+    for (int j = 0; j < 3; j++) rs.push_back(p.grad[j]);
+  for (double v : {p.beta1, p.beta2, p.beta3, p.cfl, c.dt, p.tforce, p.epsfor, p.kforce, p.tfiuo}) rs.push_back(v);
+  nrc2 = (int)rs.size();
+  rs.push_back(c.time);
+  for (int i = 0; i < 3; i++) rs.push_back(c.gsh[i][1]);
+  for (double b : {p.beta1 * p.beta1, p.beta2 * p.beta2, p.beta3 * p.beta3, 0.0}) {
+    rs.push_back(b);
+    rs.push_back(b);
+  }
+  const int nrproc = c.forcing.nrproc;
+  for (int i = 0; i < nrproc; i++) rs.push_back(c.forcing.suo[i]);
+  for (int i = 0; i < nrproc; i++) rs.push_back(c.forcing.svo[i]);
+}
+
+int psdns_gpu_write_chkptou(void* ctx, const char* path, int32_t istep, int32_t iostep) {
+  Ctx* c = (Ctx*)ctx;
+  touch(c);
+  if (!c || !path) return set_error("null argument");
+  std::vector<long long> is;
+  std::vector<double> rs;
+  int nic2 = 0, nrc2 = 0;
+  store_data(*c, istep, iostep, is, nic2, rs, nrc2);
+  FILE* f = std::fopen(path, "w");
+  if (!f) return set_error("cannot open %s for writing", path);
+  bool ok = fmt_ints(f, {nic2, nrc2, (long long)is.size(), (long long)rs.size()}, 10, 8) && fmt_ints(f, is, 10, 8) &&
+            fmt_reals(f, rs);
+  if (std::fclose(f) != 0) ok = false;
+  return ok ? 0 : set_error("write to %s failed", path);
+}
+
+int psdns_gpu_read_chkptou(void* ctx, const char* path, int32_t strict, int32_t* istep) {
+  Ctx* c = (Ctx*)ctx;
+  touch(c);
+  if (!c || !path) return set_error("null argument");
+  FILE* f = std::fopen(path, "r");
+  if (!f) return set_error("cannot open %s", path);
+  std::vector<std::string> fld;
+  long long hdr[4] = {0, 0, 0, 0};
+  bool ok = read_fields(f, 4, 10, 8, fld);
+  for (int i = 0; ok && i < 4; i++) hdr[i] = std::atoll(fld[i].c_str());
+  std::vector<long long> ird;
+  std::vector<double> rrd;
+  if (ok) ok = hdr[2] > 0 && hdr[2] < 100 && hdr[3] > 0 && hdr[3] < 100000000 && read_fields(f, hdr[2], 10, 8, fld);
+  if (ok) for (auto& x : fld) ird.push_back(std::atoll(x.c_str()));
+  if (ok) ok = read_fields(f, hdr[3], 5, 15, fld);
+  if (ok)
+    for (auto& x : fld) {
+      double d;
+      if (!parse_real(x, d)) { ok = false; break; }
+      rrd.push_back(d);
+    }
+  std::fclose(f);
+  if (!ok) return set_error("%s: not a chkptou file (store.f formats 900/910)", path);
+  std::vector<long long> is;
+  std::vector<double> rs;
+  int nic2 = 0, nrc2 = 0;
+  store_data(*c, 0, 0, is, nic2, rs, nrc2);
+  if (hdr[0] != nic2 || hdr[1] != nrc2 || (long long)ird.size() != (long long)is.size() ||
+      (long long)rrd.size() != (long long)rs.size())
+    return set_error("%s: %lld/%lld integers and %lld/%lld reals, this run stores %d/%zu and %d/%zu", path, hdr[0],
+                     hdr[2], hdr[1], hdr[3], nic2, is.size(), nrc2, rs.size());
+  if (strict) {
+    // store.f:272-301 (kstop = 1): the stored parameters must be this run's;
+    // the unset locals (3..7) and iostep (11) are not compared, reals to
+    // the 9 digits of format 910
+    for (int j = 0; j < nic2; j++) {
+      if ((j >= 3 && j <= 7) || j == 11) continue;
+      if (ird[j] != is[j]) return set_error("%s: integer no. %d is %lld, this run has %lld", path, j + 1, ird[j], is[j]);
+    }
+    for (int j = 0; j < nrc2; j++) {
+      if (j == 1 + (c->p.nc == 0 ? 1 : c->p.nc) + 4 + 3 * (c->p.nc == 0 ? 1 : c->p.nc) + 4) continue;   // dt (cfl > 0: the last step's)
+      if (std::fabs(rrd[j] - rs[j]) > 5e-9 * std::max(1.0, std::fabs(rs[j])))
+        return set_error("%s: real no. %d is %.9g, this run has %.9g", path, j + 1, rrd[j], rs[j]);
+    }
+  }
+  // store.f:303-320: istep0, time0, gsh(:,2), suo, svo
+  size_t o = nrc2;
+  c->time = rrd[o++];
+  for (int i = 0; i < 3; i++) c->gsh[i][1] = rrd[o++];
+  o += 8;
+  const int nrproc = c->forcing.nrproc;
+  for (int i = 0; i < nrproc; i++) c->forcing.suo[i] = rrd[o++];
+  for (int i = 0; i < nrproc; i++) c->forcing.svo[i] = rrd[o++];
+  c->jstep = 0;
+  c->istart = 1;
+  if (istep) *istep = (int32_t)ird[nic2];
+  return 0;
+}
+
+int psdns_gpu_write_ranout(void* ctx, const char* path) {
+  Ctx* c = (Ctx*)ctx;
+  touch(c);
+  if (!c || !path) return set_error("null argument");
+  // ranseq.f:174-183 (k = -2): the active sequence's seed goes back into
+  // its slot, then the 20 seeds are written with format (5i15)
+  if (c->rng.ifst) c->rng.iseq[c->rng.klast - 1] = c->rng.iseed;
+  else
+    for (int i = 0; i < 20; i++) c->rng.iseq[i] = c->rng.seed_input;
+  std::vector<long long> v(c->rng.iseq, c->rng.iseq + 20);
+  FILE* f = std::fopen(path, "w");
+  if (!f) return set_error("cannot open %s for writing", path);
+  bool ok = fmt_ints(f, v, 5, 15);
+  if (std::fclose(f) != 0) ok = false;
+  return ok ? 0 : set_error("write to %s failed", path);
+}
+
+int psdns_gpu_read_ranin(void* ctx, const char* path) {
+  Ctx* c = (Ctx*)ctx;
+  touch(c);
+  if (!c || !path) return set_error("null argument");
+  FILE* f = std::fopen(path, "r");
+  if (!f) return set_error("cannot open %s", path);
+  std::vector<std::string> fld;
+  const bool ok = read_fields(f, 20, 5, 15, fld);
+  std::fclose(f);
+  if (!ok) return set_error("%s: not a ranout file (20 seeds, format 5i15)", path);
+  // ranseq.f:83-118 (first call with k = -1): the table is read, the
+  // active sequence is the first
+  for (int i = 0; i < 20; i++) c->rng.iseq[i] = (int32_t)std::atoll(fld[i].c_str());
+  c->rng.ifst = 1;
+  c->rng.klast = 1;
+  c->rng.iseed = c->rng.iseq[0];
+  return 0;
+}
+
+// one variable's records of one pencil (outpen_write_r.f:62-72)
+static bool pencil_write(FILE* f, int v, int n, const double* u, int xist, int xisz, int zjst, int zjsz,
+                         std::vector<unsigned char>& row) {
+  const int nxh = n / 2 + 1;
+  std::vector<unsigned char> rec;
+  for (uint32_t x : {(uint32_t)(v + 1), (uint32_t)n, (uint32_t)n, (uint32_t)n}) be32(rec, x);
+  bool ok = write_record(f, rec.data(), rec.size());
+  rec.clear();
+  for (uint32_t x : {(uint32_t)xist, (uint32_t)xisz, (uint32_t)zjst, (uint32_t)zjsz, 1u, (uint32_t)n}) be32(rec, x);
+  ok = ok && write_record(f, rec.data(), rec.size());
+  for (int zp = 0; zp < zjsz && ok; zp++) {
+    const int z = zjst - 1 + zp;
+    if (z == n / 2) continue;   // nzhp
+    for (int half = 0; half < 2 && ok; half++) {
+      const int y0 = half == 0 ? 0 : n / 2 + 1, y1 = half == 0 ? n / 2 : n;
+      size_t o = 0;
+      for (int y = y0; y < y1; y++)
+        for (int x = xist - 1; x < xist - 1 + xisz; x++) {
+          const double* e = u + 2 * (((size_t)z * n + y) * nxh + x);
+          be64(&row[o], e[0]);
+          be64(&row[o + 8], e[1]);
+          o += 16;
+        }
+      ok = write_record(f, row.data(), o);
+    }
+  }
+  return ok;
+}
+
+int psdns_gpu_write_checkpoint_set(void* ctx, const char* prefix, int32_t iproc, int32_t jproc, int32_t which) {
+  Ctx* c = (Ctx*)ctx;
+  touch(c);
+  if (!c || !prefix) return set_error("null argument");
+  if (which != PSDNS_FIELD_U && which != PSDNS_FIELD_UN) return set_error("which must be U or UN");
+  const int n = c->n, xh = n / 2;
+  if (iproc < 1 || jproc < 1 || xh % iproc || n % jproc || iproc * jproc > 4096)
+    return set_error("checkpoint set: iproc must divide n/2 = %d and jproc n = %d (at most 4096 tasks)", xh, n);
+  const int xisz = xh / iproc, zjsz = n / jproc, nt = iproc * jproc;
+  std::vector<double> full;
+  std::vector<unsigned char> row;
+  try {
+    full.resize(2 * full_elems(*c));
+    row.resize((size_t)16 * xisz * (n / 2));
+  } catch (const std::bad_alloc&) {
+    return set_error("checkpoint: cannot allocate %.2f GB of host memory", 16.0 * full_elems(*c) / 1e9);
+  }
+  // task t = jp * iproc + ip holds x in [ip xisz, (ip+1) xisz), z in [jp zjsz, (jp+1) zjsz)
+  std::vector<FILE*> fs(nt, nullptr);
+  int err = 0;
+  for (int t = 0; t < nt && !err; t++) {
+    const std::string fn = std::string(prefix) + ".p" + std::to_string(t);
+    fs[t] = std::fopen(fn.c_str(), "wb");
+    if (!fs[t]) err = set_error("cannot open %s for writing", fn.c_str());
+  }
+  for (int v = 0; v < c->nv && !err; v++) {
+    if (full_var_get(*c, which, v, full.data())) { err = 1; break; }
+    for (int t = 0; t < nt && !err; t++) {
+      const int ip = t % iproc, jp = t / iproc;
+      if (!pencil_write(fs[t], v, n, full.data(), ip * xisz + 1, xisz, jp * zjsz + 1, zjsz, row))
+        err = set_error("write of %s.p%d failed", prefix, t);
+    }
+  }
+  for (FILE* f : fs)
+    if (f && std::fclose(f) != 0 && !err) err = set_error("closing a pencil file of %s failed", prefix);
+  return err;
+}
+
+int psdns_gpu_read_checkpoint_set(void* ctx, const char* const* paths, int32_t nfiles) {
+  Ctx* c = (Ctx*)ctx;
+  touch(c);
+  if (!c || !paths || nfiles < 1 || nfiles > 4096) return set_error("read_checkpoint_set: bad argument");
+  const int n = c->n, nxh = n / 2 + 1, xh = n / 2;
+  std::vector<double> full;
+  std::vector<unsigned char> cover;
+  try {
+    full.resize(2 * full_elems(*c));
+    cover.resize((size_t)xh * n);
+  } catch (const std::bad_alloc&) {
+    return set_error("checkpoint: cannot allocate %.2f GB of host memory", 16.0 * full_elems(*c) / 1e9);
+  }
+  std::vector<FILE*> fs(nfiles, nullptr);
+  int err = 0;
+  for (int t = 0; t < nfiles && !err; t++) {
+    fs[t] = paths[t] ? std::fopen(paths[t], "rb") : nullptr;
+    if (!fs[t]) err = set_error("cannot open pencil file %d (%s)", t, paths[t] ? paths[t] : "null");
+  }
+  std::vector<unsigned char> rec;
+  for (int v = 0; v < c->nv && !err; v++) {
+    std::fill(full.begin(), full.end(), 0.0);
+    std::fill(cover.begin(), cover.end(), 0);
+    for (int t = 0; t < nfiles && !err; t++) {
+      FILE* f = fs[t];
+      if (!read_record(f, rec) || rec.size() != 16 || (int)rd_be32(&rec[0]) != v + 1 ||
+          (int)rd_be32(&rec[4]) != n || (int)rd_be32(&rec[8]) != n || (int)rd_be32(&rec[12]) != n) {
+        err = set_error("%s: variable %d of a %d^3 field expected", paths[t], v + 1, n);
+        break;
+      }
+      if (!read_record(f, rec) || rec.size() != 24) { err = set_error("%s: bad pencil header", paths[t]); break; }
+      const int xist = (int)rd_be32(&rec[0]), xisz = (int)rd_be32(&rec[4]), zjst = (int)rd_be32(&rec[8]),
+                zjsz = (int)rd_be32(&rec[12]);
+      if (xist < 1 || xisz < 1 || xist - 1 + xisz > xh || zjst < 1 || zjsz < 1 || zjst - 1 + zjsz > n ||
+          rd_be32(&rec[16]) != 1 || (int)rd_be32(&rec[20]) != n) {
+        err = set_error("%s: pencil x %d+%d, z %d+%d outside the %d^3 box", paths[t], xist, xisz, zjst, zjsz, n);
+        break;
+      }
+      for (int zp = 0; zp < zjsz && !err; zp++) {
+        const int z = zjst - 1 + zp;
+        if (z == n / 2) continue;
+        for (int x = xist - 1; x < xist - 1 + xisz; x++) {
+          if (cover[(size_t)x * n + z]++) { err = set_error("%s: x %d, z %d given twice", paths[t], x + 1, z + 1); break; }
+        }
+        for (int half = 0; half < 2 && !err; half++) {
+          const int y0 = half == 0 ? 0 : n / 2 + 1, y1 = half == 0 ? n / 2 : n;
+          if (!read_record(f, rec) || rec.size() != (size_t)16 * xisz * (y1 - y0)) {
+            err = set_error("%s: short record at z = %d", paths[t], z + 1);
+            break;
+          }
+          size_t o = 0;
+          for (int y = y0; y < y1; y++)
+            for (int x = xist - 1; x < xist - 1 + xisz; x++) {
+              double* e = full.data() + 2 * (((size_t)z * n + y) * nxh + x);
+              e[0] = rd_be64(&rec[o]);
+              e[1] = rd_be64(&rec[o + 8]);
+              o += 16;
+            }
+        }
+      }
+    }
+    for (int x = 0; x < xh && !err; x++)
+      for (int z = 0; z < n; z++)
+        if (z != n / 2 && !cover[(size_t)x * n + z]) {
+          err = set_error("the pencil set does not cover x %d, z %d", x + 1, z + 1);
+          break;
+        }
+    if (!err && full_var_set(*c, v, full.data())) err = 1;
+  }
+  for (FILE* f : fs)
+    if (f) std::fclose(f);
   return err;
 }
 

@@ -145,6 +145,43 @@ module psdns_gpu_mod
       character(kind=c_char), intent(in) :: path(*)   ! terminated by c_null_char
       integer(c_int32_t), value :: which
     end function
+    integer(c_int) function psdns_gpu_write_checkpoint_set(ctx, prefix, iproc, jproc, which) &
+        bind(c, name='psdns_gpu_write_checkpoint_set')
+      import :: c_int, c_ptr, c_char, c_int32_t
+      type(c_ptr), value :: ctx
+      character(kind=c_char), intent(in) :: prefix(*)
+      integer(c_int32_t), value :: iproc, jproc, which
+    end function
+    integer(c_int) function psdns_gpu_read_checkpoint_set(ctx, paths, nfiles) &
+        bind(c, name='psdns_gpu_read_checkpoint_set')
+      import :: c_int, c_ptr, c_int32_t
+      type(c_ptr), value :: ctx
+      type(c_ptr), value :: paths        ! c_loc of an array of c_loc(path(1)) pointers
+      integer(c_int32_t), value :: nfiles
+    end function
+    integer(c_int) function psdns_gpu_write_chkptou(ctx, path, istep, iostep) bind(c, name='psdns_gpu_write_chkptou')
+      import :: c_int, c_ptr, c_char, c_int32_t
+      type(c_ptr), value :: ctx
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int32_t), value :: istep, iostep
+    end function
+    integer(c_int) function psdns_gpu_read_chkptou(ctx, path, strict, istep) bind(c, name='psdns_gpu_read_chkptou')
+      import :: c_int, c_ptr, c_char, c_int32_t
+      type(c_ptr), value :: ctx
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int32_t), value :: strict
+      integer(c_int32_t), intent(out) :: istep
+    end function
+    integer(c_int) function psdns_gpu_write_ranout(ctx, path) bind(c, name='psdns_gpu_write_ranout')
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: ctx
+      character(kind=c_char), intent(in) :: path(*)
+    end function
+    integer(c_int) function psdns_gpu_read_ranin(ctx, path) bind(c, name='psdns_gpu_read_ranin')
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: ctx
+      character(kind=c_char), intent(in) :: path(*)
+    end function
     integer(c_int) function psdns_gpu_read_checkpoint(ctx, path) bind(c, name='psdns_gpu_read_checkpoint')
       import :: c_int, c_ptr, c_char
       type(c_ptr), value :: ctx

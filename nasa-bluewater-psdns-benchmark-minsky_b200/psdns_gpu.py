@@ -69,6 +69,12 @@ EXPORTS = (
     "psdns_gpu_rk_stage_noalloc",
     "psdns_gpu_dft_lines",
     "psdns_gpu_filter_state",
+    "psdns_gpu_write_checkpoint_set",
+    "psdns_gpu_read_checkpoint_set",
+    "psdns_gpu_write_chkptou",
+    "psdns_gpu_read_chkptou",
+    "psdns_gpu_write_ranout",
+    "psdns_gpu_read_ranin",
     "psdns_gpu_shell_factor",
     "psdns_gpu_corrector_features",
     "psdns_gpu_corrector_apply",
@@ -145,6 +151,13 @@ def load():
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
     L.psdns_gpu_filter_state.argtypes = [vp, vp]
+    cp = ctypes.c_char_p
+    L.psdns_gpu_write_checkpoint_set.argtypes = [vp, cp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+    L.psdns_gpu_read_checkpoint_set.argtypes = [vp, ctypes.POINTER(cp), ctypes.c_int32]
+    L.psdns_gpu_write_chkptou.argtypes = [vp, cp, ctypes.c_int32, ctypes.c_int32]
+    L.psdns_gpu_read_chkptou.argtypes = [vp, cp, ctypes.c_int32, ip]
+    L.psdns_gpu_write_ranout.argtypes = [vp, cp]
+    L.psdns_gpu_read_ranin.argtypes = [vp, cp]
     L.psdns_gpu_shell_factor.argtypes = [vp, ctypes.c_int32, dp]
     fq = ctypes.POINTER(ctypes.c_float)
     L.psdns_gpu_corrector_features.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, fq]
@@ -508,6 +521,31 @@ class Solver:
         ek = np.zeros(n); dk = np.zeros(n); e6 = np.zeros(n * 6); st = np.zeros(7)
         _check(load().psdns_gpu_spectra(self._ctx, int(which), _dp(ek), _dp(dk), _dp(e6), _dp(st)), "spectra")
         return ek, dk, e6.reshape(n, 6), dict(zip(["tke", "eps", "skew", "klen", "kvel", "ktime", "ekl"], st))
+
+    def write_checkpoint_set(self, prefix, iproc, jproc, which=FIELD_UN):
+        """iproc*jproc pencil files <prefix>.p<t> (outpen_write_r.f layout)."""
+        _check(load().psdns_gpu_write_checkpoint_set(self._ctx, os.fsencode(prefix), int(iproc), int(jproc),
+                                                     int(which)), "write_checkpoint_set")
+
+    def read_checkpoint_set(self, paths):
+        arr = (ctypes.c_char_p * len(paths))(*[os.fsencode(p) for p in paths])
+        _check(load().psdns_gpu_read_checkpoint_set(self._ctx, arr, len(paths)), "read_checkpoint_set")
+
+    def write_chkptou(self, path, istep, iostep=1):
+        _check(load().psdns_gpu_write_chkptou(self._ctx, os.fsencode(path), int(istep), int(iostep)), "write_chkptou")
+
+    def read_chkptou(self, path, strict=True):
+        """store.f icall 3; returns the stored istep."""
+        ist = ctypes.c_int32()
+        _check(load().psdns_gpu_read_chkptou(self._ctx, os.fsencode(path), 1 if strict else 0, ctypes.byref(ist)),
+               "read_chkptou")
+        return ist.value
+
+    def write_ranout(self, path):
+        _check(load().psdns_gpu_write_ranout(self._ctx, os.fsencode(path)), "write_ranout")
+
+    def read_ranin(self, path):
+        _check(load().psdns_gpu_read_ranin(self._ctx, os.fsencode(path)), "read_ranin")
 
     def filter_from(self, fine):
         """This (coarse) box's u and un := fine box's un inside this box's

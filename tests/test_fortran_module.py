@@ -51,6 +51,7 @@ def _c_args():
             a = " ".join(a.split())
             if not a or a == "void":
                 continue
+            a = re.sub(r"\*\s*const\b", "*", a)   # pointer to const pointers
             stars = a.count("*")
             mm = re.match(r"(const\s+)?(\w+)\s+(\w+)$", " ".join(a.replace("*", " ").split()))
             assert mm, a
