@@ -64,6 +64,9 @@ def parse():
                     help="skip the learned arm (128^3 + spectral-correction network against 512^3 DNS)")
     ap.add_argument("--accuracy-steps", type=int, default=3,
                     help="steps of the same-seed FP64 run that judges the error of the timed arm (0: skip)")
+    ap.add_argument("--dft-lines", type=int, default=0,
+                    help="instead: the 1024-point line DFT on its own (FP32 Stockham and split-BF16 tensor cores), "
+                         "L lines through psdns_gpu_dft_lines")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="instead: B boxes of n in {32,48,64,96}, log-uniform viscosity, fixed dt")
     return ap.parse_args()
@@ -294,10 +297,33 @@ def run_ensemble(args):
     return 0
 
 
+def run_dft_lines(args):
+    """The DFT primitive alone: L random complex lines of 1024 points through
+    psdns_gpu_dft_lines in both modes (host copies included in the call),
+    errors against numpy's float64 FFT."""
+    import numpy as np
+    import psdns_gpu as P
+    rng = np.random.default_rng(1)
+    L = args.dft_lines
+    x = (rng.standard_normal((L, 1024)) + 1j * rng.standard_normal((L, 1024))).astype(np.complex64)
+    x = x.astype(np.complex128)
+    ref = np.fft.fft(x, axis=-1)
+    out = {"metric": "1024-point line DFT", "lines": L}
+    for name, mode in (("fp32_stockham", P.DFT_FP32), ("tc_bf16x3", P.DFT_TC_BF16X3)):
+        t0 = time.perf_counter()
+        y = P.dft_lines(x, mode)
+        out[name] = {"rel_l2": float(np.linalg.norm(y - ref) / np.linalg.norm(ref)),
+                     "call_s": time.perf_counter() - t0}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.dft_lines > 0:
+        return run_dft_lines(args)
     if args.ensemble > 0:
         return run_ensemble(args)
     import torch

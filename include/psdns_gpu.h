@@ -189,6 +189,15 @@ int psdns_gpu_particles_set(void *ctx, int64_t np, const double *pos);
 /* Positions pp(np,1:3) and velocities pp(np,4:6), column-major (np,3) each
  * (either may be NULL). */
 int psdns_gpu_particles_get(void *ctx, double *pos, double *vel);
+/* Particle output of one writing task (hooks/LAG_LOCAL/lagout1.f ->
+ * pop1_file_local.f + pop1_write_local2.f with nsubset = 1): particles
+ * ordered as the reference's tetrad groups, np = nrefp (1 + 3 ngp) (the
+ * reference particles, then for each group three satellite sets).  Files
+ * <prefix>/<igp>/pvel1g<igp>_s0 and .../ppos1g<igp>_s0 (directories made by
+ * the caller), big-endian unformatted; append = 0 starts them with the
+ * record (4 nrefp, nrefp, 4, 3); each call adds (istep - 1, time) and, per
+ * component, the reference set and the group's three satellite sets. */
+int psdns_gpu_particles_write(void *ctx, const char *prefix, int32_t ngp, int32_t istep, int32_t append);
 
 /* The particle phase of psdns_gpu_step for a driver that runs the stages
  * itself with psdns_gpu_rk_stage: call it before rk_stage(kstep = 1) of each

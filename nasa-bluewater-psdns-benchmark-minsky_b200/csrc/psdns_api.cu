@@ -2343,6 +2343,62 @@ int psdns_gpu_particles_get(void* ctx, double* pos, double* vel) {
   return 0;
 }
 
+// hooks/LAG_LOCAL/pop1_file_local.f + pop1_write_local2.f for one writing
+// task (nsubset = 1): per group igp = 1..ngp, files <prefix>/<igp>/pvel1g<igp>_s0
+// and <prefix>/<igp>/ppos1g<igp>_s0, big-endian unformatted (makefile:251).
+// Opened (append = 0) with the record (nopg, nrefp, 4, 3), nopg = 4 nrefp,
+// nrefp = np / (1 + 3 ngp); every call appends the record (istep - 1,
+// time) and, for each of the three components (velocities u v w, or
+// positions x y z), the reference particles pp(1:nrefp) and the three
+// satellite sets of the group, pp(nrefp + ((igp-1) 3 + ii - 1) nrefp + 1 :
+// ... + nrefp), ii = 1..3 (pop1_write_local2.f:238-262).
+int psdns_gpu_particles_write(void* ctx, const char* prefix, int32_t ngp, int32_t istep, int32_t append) {
+  Ctx* c = (Ctx*)ctx;
+  touch(c);
+  if (!c || !prefix) return set_error("null argument");
+  if (c->np == 0) return set_error("no particles");
+  if (ngp < 1 || c->np % (1 + 3 * (long long)ngp) != 0)
+    return set_error("particles_write: np = %lld is not nrefp (1 + 3 ngp) for ngp = %d", c->np, ngp);
+  const long long nrefp = c->np / (1 + 3 * (long long)ngp);
+  if (nrefp > (1LL << 28)) return set_error("particles_write: too many particles for one record");
+  std::vector<double> pos(3 * (size_t)c->np), vel(3 * (size_t)c->np);
+  if (psdns_gpu_particles_get(c, pos.data(), vel.data())) return 1;
+  std::vector<unsigned char> rec;
+  for (int igp = 1; igp <= ngp; igp++) {
+    for (int kind = 0; kind < 2; kind++) {
+      const std::string fn = std::string(prefix) + "/" + std::to_string(igp) + "/" + (kind == 0 ? "pvel" : "ppos") +
+                             "1g" + std::to_string(igp) + "_s0";
+      FILE* f = std::fopen(fn.c_str(), append ? "ab" : "wb");
+      if (!f) return set_error("cannot open %s (the directory %s/%d must exist)", fn.c_str(), prefix, igp);
+      bool ok = true;
+      if (!append) {
+        rec.clear();
+        for (uint32_t v : {(uint32_t)(4 * nrefp), (uint32_t)nrefp, 4u, 3u}) be32(rec, v);
+        ok = write_record(f, rec.data(), rec.size());
+      }
+      rec.assign(12, 0);
+      rec.clear();
+      be32(rec, (uint32_t)(istep - 1));
+      rec.resize(12);
+      be64(&rec[4], c->time);
+      ok = ok && write_record(f, rec.data(), rec.size());
+      const double* src = kind == 0 ? vel.data() : pos.data();
+      std::vector<unsigned char> row((size_t)8 * nrefp);
+      for (int comp = 0; comp < 3 && ok; comp++) {
+        const double* a = src + (size_t)comp * c->np;
+        for (int set = 0; set < 4 && ok; set++) {
+          const long long i0 = set == 0 ? 0 : nrefp + ((long long)(igp - 1) * 3 + set - 1) * nrefp;
+          for (long long i = 0; i < nrefp; i++) be64(&row[(size_t)8 * i], a[i0 + i]);
+          ok = write_record(f, row.data(), row.size());
+        }
+      }
+      if (std::fclose(f) != 0) ok = false;
+      if (!ok) return set_error("write to %s failed", fn.c_str());
+    }
+  }
+  return 0;
+}
+
 int psdns_gpu_spectra(void* ctx, int32_t which, double* ek, double* dk, double* eijk, double* stats) {
   Ctx* c = (Ctx*)ctx;
   touch(c);

@@ -81,6 +81,13 @@ module psdns_gpu_mod
       type(c_ptr), value :: ctx
       real(c_double), intent(out) :: pos(*), vel(*)
     end function
+    integer(c_int) function psdns_gpu_particles_write(ctx, prefix, ngp, istep, append) &
+        bind(c, name='psdns_gpu_particles_write')
+      import :: c_int, c_ptr, c_char, c_int32_t
+      type(c_ptr), value :: ctx
+      character(kind=c_char), intent(in) :: prefix(*)
+      integer(c_int32_t), value :: ngp, istep, append
+    end function
     integer(c_int) function psdns_gpu_set_state_async(ctx, un, layout) bind(c, name='psdns_gpu_set_state_async')
       import :: c_int, c_ptr, c_int32_t
       type(c_ptr), value :: ctx

@@ -69,6 +69,7 @@ EXPORTS = (
     "psdns_gpu_rk_stage_noalloc",
     "psdns_gpu_dft_lines",
     "psdns_gpu_filter_state",
+    "psdns_gpu_particles_write",
     "psdns_gpu_write_checkpoint_set",
     "psdns_gpu_read_checkpoint_set",
     "psdns_gpu_write_chkptou",
@@ -151,6 +152,7 @@ def load():
     L.psdns_gpu_forcing_table.argtypes = [vp, dp, ip, ip]
     L.psdns_gpu_rk_stage_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, dp, dp, vp, vp, dp, vp]
     L.psdns_gpu_filter_state.argtypes = [vp, vp]
+    L.psdns_gpu_particles_write.argtypes = [vp, ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
     cp = ctypes.c_char_p
     L.psdns_gpu_write_checkpoint_set.argtypes = [vp, cp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
     L.psdns_gpu_read_checkpoint_set.argtypes = [vp, ctypes.POINTER(cp), ctypes.c_int32]
@@ -521,6 +523,11 @@ class Solver:
         ek = np.zeros(n); dk = np.zeros(n); e6 = np.zeros(n * 6); st = np.zeros(7)
         _check(load().psdns_gpu_spectra(self._ctx, int(which), _dp(ek), _dp(dk), _dp(e6), _dp(st)), "spectra")
         return ek, dk, e6.reshape(n, 6), dict(zip(["tke", "eps", "skew", "klen", "kvel", "ktime", "ekl"], st))
+
+    def particles_write(self, prefix, ngp, istep, append=False):
+        """pop1_write_local2.f output of one task (files under prefix/<igp>/)."""
+        _check(load().psdns_gpu_particles_write(self._ctx, os.fsencode(prefix), int(ngp), int(istep),
+                                                1 if append else 0), "particles_write")
 
     def write_checkpoint_set(self, prefix, iproc, jproc, which=FIELD_UN):
         """iproc*jproc pencil files <prefix>.p<t> (outpen_write_r.f layout)."""

@@ -110,3 +110,54 @@ def test_pencil_sets(gpu_mod, tmp_path):
     np.testing.assert_array_equal(b.get_state(P.FIELD_UN), a.get_state(P.FIELD_UN))
     a.close()
     b.close()
+
+
+def _records(path):
+    """Fortran sequential unformatted, big-endian 4-byte record markers
+    (an independent reader of the reference's particle files)."""
+    import struct
+    data = open(path, "rb").read()
+    out, o = [], 0
+    while o < len(data):
+        (m,) = struct.unpack(">i", data[o:o + 4])
+        out.append(data[o + 4:o + 4 + m])
+        (m2,) = struct.unpack(">i", data[o + 4 + m:o + 8 + m])
+        assert m2 == m
+        o += 8 + m
+    return out
+
+
+def test_particle_output_in_the_reference_layout(gpu_mod, tmp_path):
+    """psdns_gpu_particles_get's pp(np, 1:6) order through the writer of
+    pop1_write_local2.f (two groups of tetrads) and back."""
+    import struct
+    P = gpu_mod
+    ngp, nrefp = 2, 300
+    np_ = nrefp * (1 + 3 * ngp)
+    s = make(P, False)
+    s.field_init(3)
+    rng = np.random.default_rng(8)
+    s.particles_set(1.0 + rng.random((np_, 3)) * 32)
+    for g in range(1, ngp + 1):
+        os.makedirs(tmp_path / str(g))
+    s.step()
+    s.particles_write(str(tmp_path), ngp, istep=2)
+    s.step()
+    s.particles_write(str(tmp_path), ngp, istep=3, append=True)
+    pos, vel = s.particles_get()
+    t = s.time_info()["time"]
+    for g in range(1, ngp + 1):
+        for kind, arr in (("pvel", vel), ("ppos", pos)):
+            recs = _records(tmp_path / str(g) / f"{kind}1g{g}_s0")
+            assert struct.unpack(">4i", recs[0]) == (4 * nrefp, nrefp, 4, 3)
+            assert len(recs) == 1 + 2 * (1 + 3 * 4)
+            last = recs[1 + 13:]
+            step, time = struct.unpack(">id", last[0])
+            assert step == 2 and time == t
+            for comp in range(3):
+                sets = [np.frombuffer(last[1 + 4 * comp + k], dtype=">f8") for k in range(4)]
+                np.testing.assert_array_equal(sets[0], arr[:nrefp, comp])
+                for ii in range(1, 4):
+                    i0 = nrefp + ((g - 1) * 3 + ii - 1) * nrefp
+                    np.testing.assert_array_equal(sets[ii], arr[i0:i0 + nrefp, comp])
+    s.close()
