@@ -260,14 +260,16 @@ def run_ensemble(args):
                                seed_input=122929298 + i) for i in range(B)]
     ens = P.Ensemble(params)
     ens.field_init([1000 + i for i in range(B)])
-    # the first steps of each class also tune its sub-batch size (about
-    # log2(boxes per class) + 2 steps), then the graph is captured
-    warm = max(args.warmup, 12)
+    # the first steps of each class tune it (boxes per launch, then the K2 and
+    # K4 tiles: two steps per candidate, about 2 log2(boxes per class) + 14
+    # steps), then the graph is captured
+    warm = max(args.warmup, 40)
     ens.step(warm)
     t0 = time.perf_counter()
     rc, info = ens.step(args.steps)
     t = (time.perf_counter() - t0) / args.steps
     pts = float(sum(int(n) ** 3 for n in ns))
+    tuning = ens.tuning()
     # unbatched comparison: separate contexts, one step each, one after the other
     ctxs = [P.Solver(p) for p in params]
     for i, c in enumerate(ctxs):
@@ -291,7 +293,7 @@ def run_ensemble(args):
                                   "[0.005, 0.05], dt 0.005, unforced",
                       "boxes": B, "n_counts": {str(v): int((ns == v).sum()) for v in (32, 48, 64, 96)},
                       "timing": "host clock around synchronised ensemble steps"},
-           "status": rc, "separate_contexts_ms_per_step": t_sep * 1e3,
+           "status": rc, "tuning": tuning, "separate_contexts_ms_per_step": t_sep * 1e3,
            "batching_speedup": t_sep / t}
     print(json.dumps(out), flush=True)
     return 0

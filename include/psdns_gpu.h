@@ -349,6 +349,15 @@ int psdns_gpu_ensemble_get_state(void *ens, int32_t box, double *out, int32_t wh
  * psdns_gpu_step info of box i.  Returns 2 if a box met an abort condition
  * of step.f (the steps are completed). */
 int psdns_gpu_ensemble_step(void *ens, int32_t nsteps, double *info);
+/* The ensemble autotuner's choices (no reference routine; the counterpart
+ * of FFTW's planner and wisdom, PSDNS/epfftw.f, PSDNS/wisdom.c): per class
+ * of equal n, in the first steps of a fixed-dt class, the number of boxes
+ * per launch, then the FFT tiles of the z transforms (x lines per block of
+ * K2 and K4: the default, half, double; boxes of n <= 128), each candidate
+ * timed over two real steps.  out[8 * cap] rows: n, boxes, tuned (0/1),
+ * boxes per launch, K2 lines per block, K4 lines per block, step ms of the
+ * all-default candidate, step ms of the choice; *nclasses = classes. */
+int psdns_gpu_ensemble_tuning(void *ens, int32_t cap, double *out, int32_t *nclasses);
 /* Shell spectra of one box (as psdns_gpu_spectra). */
 int psdns_gpu_ensemble_spectra(void *ens, int32_t box, int32_t which, double *ek, double *dk, double *eijk,
                                double *stats);

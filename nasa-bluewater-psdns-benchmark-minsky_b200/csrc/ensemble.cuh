@@ -168,15 +168,24 @@ static int ens_step_fixed(EnsClass& e) {
   // this step's velmax and is made after the step
   for (Ctx* c : e.box) step_control(*c);
   if (!e.tuned) {
-    // tuning steps: one candidate sub-batch size per step, the first twice
-    // (its first run also warms up), timed with events on the class stream
+    // tuning steps (real steps: the sub-batch size and the tiles change no
+    // result), timed with events on the class stream
     if (e.cands.empty()) {
-      for (int s = e.nb; s >= 1; s /= 2) e.cands.push_back(s);
-      e.cand_ms.assign(e.cands.size(), 0.f);
-      ens_fill_factors(e);   // dt is fixed: the factor tables never change
+      if (e.phase == 0) {
+        for (int s = e.nb; s >= 1; s /= 2) e.cands.push_back({s, 0, 0});
+        ens_fill_factors(e);   // dt is fixed: the factor tables never change
+      } else {
+        for (int v = 0; v < 3; v++)
+          e.cands.push_back(e.phase == 1 ? EnsClass::Cand{e.sub, v, e.k4v} : EnsClass::Cand{e.sub, e.k2v, v});
+      }
+      e.cand_ms.assign(e.cands.size(), 1e30f);
+      e.trial = 0;
+      e.rep = 0;
     }
-    const int t = std::max(0, e.trial);
-    e.sub = e.cands[t];
+    const EnsClass::Cand cd = e.cands[e.trial];
+    e.sub = cd.sub;
+    e.k2v = cd.k2v;
+    e.k4v = cd.k4v;
     cudaEvent_t t0, t1;
     CK(cudaEventCreate(&t0));
     CK(cudaEventCreate(&t1));
@@ -189,14 +198,23 @@ static int ens_step_fixed(EnsClass& e) {
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     if (rc) return 1;
-    if (e.trial >= 0) e.cand_ms[t] = ms;
-    e.trial += 1;
+    e.cand_ms[e.trial] = std::min(e.cand_ms[e.trial], ms);
+    if (++e.rep == 2) {
+      e.rep = 0;
+      e.trial += 1;
+    }
     if (e.trial == (int)e.cands.size()) {
       int best = 0;
       for (size_t i = 1; i < e.cands.size(); i++)
         if (e.cand_ms[i] < e.cand_ms[best]) best = (int)i;
-      e.sub = e.cands[best];
-      e.tuned = true;
+      if (e.phase == 0) e.default_ms = e.cand_ms[0];
+      e.best_ms = e.cand_ms[best];
+      e.sub = e.cands[best].sub;
+      e.k2v = e.cands[best].k2v;
+      e.k4v = e.cands[best].k4v;
+      e.cands.clear();
+      e.phase += 1;
+      if (!e.tile_tune || e.phase == 3) e.tuned = true;
     }
     return 0;
   }
@@ -375,6 +393,28 @@ int psdns_gpu_ensemble_get_state(void* ens, int32_t box, double* out, int32_t wh
     CK(cudaMemcpyAsync(out + 2 * v * vs, e.d_ub, sizeof(double2) * vs, cudaMemcpyDeviceToHost, e.stream));
   }
   CK(cudaStreamSynchronize(e.stream));
+  return 0;
+}
+
+int psdns_gpu_ensemble_tuning(void* ens, int32_t cap, double* out, int32_t* nclasses) {
+  Ensemble* E = (Ensemble*)ens;
+  if (!E || !nclasses) return set_error("null argument");
+  *nclasses = (int32_t)E->cls.size();
+  for (size_t i = 0; i < E->cls.size() && (int32_t)i < cap && out; i++) {
+    const EnsClass& e = *E->cls[i];
+    const int xt2 = e.prec == PSDNS_PREC_FP64 ? Tiles<double>::XT2 : Tiles<float>::XT2;
+    const int xt4 = e.prec == PSDNS_PREC_FP64 ? Tiles<double>::XT4 : Tiles<float>::XT4;
+    const int m[3][2] = {{1, 1}, {1, 2}, {2, 1}};   // tile factor of variant 0, 1, 2: num/den
+    double* r = out + 8 * i;
+    r[0] = e.n;
+    r[1] = e.nb;
+    r[2] = e.tuned ? 1 : 0;
+    r[3] = e.sub > 0 ? e.sub : e.nb;
+    r[4] = xt2 * m[e.k2v][0] / m[e.k2v][1];
+    r[5] = xt4 * m[e.k4v][0] / m[e.k4v][1];
+    r[6] = e.default_ms;
+    r[7] = e.best_ms;
+  }
   return 0;
 }
 

@@ -40,9 +40,17 @@ struct EnsClass {
   // fastest is kept for the captured graph.
   int sub = 0;
   bool tuned = false;
-  int trial = -1;
-  std::vector<int> cands;
+  // the tuner also chooses the FFT tiles of K2 and K4 (x lines per block:
+  // variant 0 = Tiles<T>, 1 = half, 2 = double; boxes of n <= 128 only).
+  // Phases: 0 sub-batch size, 1 K2 tile, 2 K4 tile; every candidate runs
+  // two real steps and keeps the faster (the first also loads its kernels).
+  int k2v = 0, k4v = 0;
+  bool tile_tune = false;   // n <= 128
+  int phase = 0, trial = 0, rep = 0;
+  struct Cand { int sub, k2v, k4v; };
+  std::vector<Cand> cands;
   std::vector<float> cand_ms;
+  float default_ms = 0.f, best_ms = 0.f;   // the first candidate (all defaults) and the choice
 };
 
 struct Ensemble {
@@ -91,6 +99,27 @@ template <typename T, int N> struct EnsImpl {
   using C = C2<T>;
   using TL = Tiles<T>;
   using I = Impl<T, N, 0>;
+  // tile variants of K2 and K4 are instantiated for small boxes only
+  static constexpr bool kTiles = N <= 128;
+
+  // K2 / K4 with XT x lines per block (0: the default tile)
+  template <int XT>
+  static void k2(EnsClass& e, const Geo& g, const C* ub, C* uz, const C* tw, const StageTables<T>& st, int nb) {
+    if constexpr (XT == 0 || kTiles) {
+      constexpr int X = XT > 0 ? XT : TL::XT2;
+      k_zinv<T, N, 0, false, false, XT><<<dim3(N, (e.g.kxn + X - 1) / X, 3 * nb), Launch<T, N, X>::THREADS,
+                                          I::TWB + sizeof(C) * X * I::L, e.stream>>>(g, ub, uz, tw, st.b11, st.b33);
+    }
+  }
+  template <int XT>
+  static void k4(EnsClass& e, const Geo& g, const C* uz, C* ub, const C* tw, const StageTables<T>& st, int nb) {
+    if constexpr (XT == 0 || kTiles) {
+      constexpr int X = XT > 0 ? XT : TL::XT4;
+      k_zfwd<T, N, 0, false, XT><<<dim3(N / TL::YT4, (e.g.kxn + X - 1) / X, nb), K4LaunchX<T, N, X>::THREADS,
+                                   I::TWB + sizeof(C) * 2 * X * TL::YT4 * I::L, e.stream>>>(g, uz, ub, tw, st.b11,
+                                                                                            st.b33);
+    }
+  }
 
   // boxes b0 .. b0 + nb - 1
   static int stage_a(EnsClass& e, int kstep, int b0, int nb) {
@@ -102,12 +131,18 @@ template <typename T, int N> struct EnsImpl {
     C* uz = (C*)e.d_uz + (size_t)b0 * e.uz_elems;
     const int kxn = e.g.kxn;
     k_yinv<T, N><<<dim3(k1_blocks<T>(e.nab_i), 3, nb), K1Launch<T, N>::THREADS, I::sm1(), e.stream>>>(g, st, u, ub, tw);
-    k_zinv<T, N><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3 * nb), Launch<T, N, TL::XT2>::THREADS, I::sm2(),
-                   e.stream>>>(g, ub, uz, tw, st.b11, st.b33);
+    switch (kTiles ? e.k2v : 0) {
+      case 1: k2<TL::XT2 / 2>(e, g, ub, uz, tw, st, nb); break;
+      case 2: k2<TL::XT2 * 2>(e, g, ub, uz, tw, st, nb); break;
+      default: k2<0>(e, g, ub, uz, tw, st, nb);
+    }
     k_xchain<T, N><<<dim3(e.nzt, N, nb), K3Launch<T, N, 0>::THREADS, I::sm3(), e.stream>>>(
         g, uz, tw, st.b11, st.b22, st.b33, e.d_velmax + b0, kstep == 1 ? 1 : 0);
-    k_zfwd<T, N><<<dim3(N / TL::YT4, (kxn + TL::XT4 - 1) / TL::XT4, nb), K4Launch<T, N>::THREADS, I::sm4(),
-                   e.stream>>>(g, uz, ub, tw, st.b11, st.b33);
+    switch (kTiles ? e.k4v : 0) {
+      case 1: k4<TL::XT4 / 2>(e, g, uz, ub, tw, st, nb); break;
+      case 2: k4<TL::XT4 * 2>(e, g, uz, ub, tw, st, nb); break;
+      default: k4<0>(e, g, uz, ub, tw, st, nb);
+    }
     CK(cudaGetLastError());
     return 0;
   }
@@ -134,6 +169,7 @@ template <typename T, int N> struct EnsImpl {
     e.d_tw = tmp.d_tw;
     e.stage_a = &EnsImpl::stage_a;
     e.stage_b = &EnsImpl::stage_b;
+    e.tile_tune = kTiles;
     return 0;
   }
 };

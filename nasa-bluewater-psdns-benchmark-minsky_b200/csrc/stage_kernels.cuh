@@ -163,6 +163,9 @@ template <typename T, int N>
 struct K1Launch : Launch<T, N, Tiles<T>::TB_I, 1024> {};
 template <typename T, int N>
 struct K4Launch : Launch<T, N, 2 * Tiles<T>::XT4 * Tiles<T>::YT4, 1024> {};
+// K4 with XT x lines per block (the ensemble tuner's tile variants)
+template <typename T, int N, int XT>
+struct K4LaunchX : Launch<T, N, 2 * XT * Tiles<T>::YT4, 1024> {};
 
 // K5 holds one CTA per SM (its (4 + nc) * TB_F lines fill shared memory), so
 // it runs every line of a block at once
@@ -303,8 +306,10 @@ __host__ __device__ __forceinline__ int k1_blocks(int nab_i) { return nab_i; }
 // K2: cylinder unpack (zero fill) + z backward FFT, store to uz
 // grid (n, ceil(kxn/XT2), 3)
 // ---------------------------------------------------------------------------
-template <typename T, int N, int NC = 0, bool GRAD = false, bool TCM = false>
-__global__ void __launch_bounds__(Launch<T, N, Tiles<T>::XT2>::THREADS, TCM ? 2 : 3)
+// XTO > 0: XTO x lines per block instead of Tiles<T>::XT2 (a tile variant
+// of the ensemble autotuner; every line is transformed the same way)
+template <typename T, int N, int NC = 0, bool GRAD = false, bool TCM = false, int XTO = 0>
+__global__ void __launch_bounds__(Launch<T, N, (XTO > 0 ? XTO : Tiles<T>::XT2)>::THREADS, TCM ? 2 : 3)
 k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11 = T(1),
        T b33 = T(1), TcArgs tca = TcArgs()) {
   // GRAD (grid.z = 2): uz slot 0 = i b11 kx u, slot 1 = i b33 kz w, the
@@ -313,7 +318,7 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
   // 4 = i b11 kx theta and slot 5 = i b33 kz theta (both from ub 3),
   // itransform.f:188-198
   using C = C2<T>;
-  constexpr int XT = Tiles<T>::XT2, TB = Tiles<T>::TB_I, TZ = Tiles<T>::TZ;
+  constexpr int XT = XTO > 0 ? XTO : Tiles<T>::XT2, TB = Tiles<T>::TB_I, TZ = Tiles<T>::TZ;
   constexpr int THREADS = Launch<T, N, XT>::THREADS;
   constexpr int L = LS<N>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -573,12 +578,12 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
 // grid (n, ceil(kxn/XT4)).  Output slots: 0 = d/dx(u^2-v^2)+d/dz(uw) partial,
 // 1 = uv, 2 = d/dx(uw)+d/dz(w^2-v^2), 3 = vw (y derivatives added in K5).
 // ---------------------------------------------------------------------------
-template <typename T, int N>
+template <typename T, int N, int XT = Tiles<T>::XT4>
 __device__ __forceinline__ void zfwd_load(const Geo& g, const C2<T>* __restrict__ uz, int slot, int y0, int ny,
                                           int x0, int nl, C2<T>* buf, int L) {
-  // lines l = yy*nl + xl, rows y0+yy, columns x0+xl; full tiles (nl = XT4)
+  // lines l = yy*nl + xl, rows y0+yy, columns x0+xl; full tiles (nl = XT)
   // take the loop with compile-time divisors
-  constexpr int TZ = Tiles<T>::TZ, XT = Tiles<T>::XT4;
+  constexpr int TZ = Tiles<T>::TZ;
   auto copy = [&](auto nlc, const C2<T>* src, C2<T>* b) {
     constexpr int NLC = decltype(nlc)::value;
     const unsigned w = (NLC > 0 ? NLC : nl) * TZ;
@@ -599,7 +604,7 @@ __device__ __forceinline__ void zfwd_load(const Geo& g, const C2<T>* __restrict_
   }
 }
 
-template <typename T, int N, int MODE>
+template <typename T, int N, int MODE, int XT = Tiles<T>::XT4>
 __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const C2<T>* s1, int L,
                                            C2<T>* __restrict__ ub, int slot, int y0, int /*ny*/, int x0, int x1,
                                            T b11, T b33) {
@@ -614,7 +619,6 @@ __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const 
   C* dst = ub + (size_t)slot * ubf_var_elems<T>(g.nab_f, N);
   // column starts of the XT lines: x and z of a cylinder index follow from
   // them (column x0 + j holds kz = 0..kc then -kc..-1)
-  constexpr int XT = Tiles<T>::XT4;
   int csr[XT + 1];
 #pragma unroll
   for (int j = 0; j <= XT; j++) csr[j] = __ldg(g.colstart + min(x0 + j, g.kxn));
@@ -653,16 +657,17 @@ __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const 
   }
 }
 
-template <typename T, int N, int NC = 0, bool TCM = false>
-__global__ void __launch_bounds__(K4Launch<T, N>::THREADS, TCM ? 2 : 3)
+// XTO > 0: XTO x lines per block instead of Tiles<T>::XT4 (ensemble tuner)
+template <typename T, int N, int NC = 0, bool TCM = false, int XTO = 0>
+__global__ void __launch_bounds__(K4LaunchX<T, N, (XTO > 0 ? XTO : Tiles<T>::XT4)>::THREADS, TCM ? 2 : 3)
 k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>* __restrict__ tw_g,
        T b11, T b33, TcArgs tca = TcArgs()) {
   // NC = 1: the scalar advection term (uz slot 5) goes to ub slot 4 without
   // derivatives (transform.f: i2f = 4+nc)
   // grid (n / YT4, ceil(kxn / XT4)): YT4 adjacent y rows x XT4 x lines
   using C = C2<T>;
-  constexpr int XT = Tiles<T>::XT4, YT = Tiles<T>::YT4, NLT = XT * YT;
-  constexpr int THREADS = K4Launch<T, N>::THREADS;
+  constexpr int XT = XTO > 0 ? XTO : Tiles<T>::XT4, YT = Tiles<T>::YT4, NLT = XT * YT;
+  constexpr int THREADS = K4LaunchX<T, N, XT>::THREADS;
   constexpr int L = LS<N>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
@@ -680,8 +685,8 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
   const int nl = x1 - x0;
   const int nt = nl * YT;
   // round 1: P5 -> s0, P1 -> s1
-  zfwd_load<T, N>(g, uz, 4, y0, YT, x0, nl, s0, L);
-  zfwd_load<T, N>(g, uz, 0, y0, YT, x0, nl, s1, L);
+  zfwd_load<T, N, XT>(g, uz, 4, y0, YT, x0, nl, s0, L);
+  zfwd_load<T, N, XT>(g, uz, 0, y0, YT, x0, nl, s1, L);
   cp_async_wait_all();
   __syncthreads();
   if (nl == XT) {
@@ -690,18 +695,18 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
     lines_fft<T, N, THREADS, TCM>(s0, nt, L, tw, w);
     lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
   }
-  zfwd_store<T, N, 0>(g, s0, s1, L, ub, 0, y0, YT, x0, x1, b11, b33);
+  zfwd_store<T, N, 0, XT>(g, s0, s1, L, ub, 0, y0, YT, x0, x1, b11, b33);
   __syncthreads();
   // round 2: P3 -> s1
-  zfwd_load<T, N>(g, uz, 2, y0, YT, x0, nl, s1, L);
+  zfwd_load<T, N, XT>(g, uz, 2, y0, YT, x0, nl, s1, L);
   cp_async_wait_all();
   __syncthreads();
   lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
-  zfwd_store<T, N, 1>(g, s0, s1, L, ub, 2, y0, YT, x0, x1, b11, b33);
+  zfwd_store<T, N, 1, XT>(g, s0, s1, L, ub, 2, y0, YT, x0, x1, b11, b33);
   __syncthreads();
   // round 3: P2 -> s0, P4 -> s1
-  zfwd_load<T, N>(g, uz, 1, y0, YT, x0, nl, s0, L);
-  zfwd_load<T, N>(g, uz, 3, y0, YT, x0, nl, s1, L);
+  zfwd_load<T, N, XT>(g, uz, 1, y0, YT, x0, nl, s0, L);
+  zfwd_load<T, N, XT>(g, uz, 3, y0, YT, x0, nl, s1, L);
   cp_async_wait_all();
   __syncthreads();
   if (nl == XT) {
@@ -711,14 +716,14 @@ k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>*
     lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
   }
   // P2 -> ub slot 1 and P4 -> ub slot 3 in one pass over the cylinder indices
-  zfwd_store<T, N, 4>(g, s0, s1, L, ub, 1, y0, YT, x0, x1, b11, b33);
+  zfwd_store<T, N, 4, XT>(g, s0, s1, L, ub, 1, y0, YT, x0, x1, b11, b33);
   if constexpr (NC > 0) {
     __syncthreads();
-    zfwd_load<T, N>(g, uz, 5, y0, YT, x0, nl, s1, L);
+    zfwd_load<T, N, XT>(g, uz, 5, y0, YT, x0, nl, s1, L);
     cp_async_wait_all();
     __syncthreads();
     lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
-    zfwd_store<T, N, 3>(g, s0, s1, L, ub, 4, y0, YT, x0, x1, b11, b33);
+    zfwd_store<T, N, 3, XT>(g, s0, s1, L, ub, 4, y0, YT, x0, x1, b11, b33);
   }
   if constexpr (TCM) tc::teardown<NCOL>(w);
 }

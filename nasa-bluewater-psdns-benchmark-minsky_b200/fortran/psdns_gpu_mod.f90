@@ -251,6 +251,13 @@ module psdns_gpu_mod
       integer(c_int32_t), value :: nsteps
       real(c_double), intent(out) :: info(*)
     end function
+    integer(c_int) function psdns_gpu_ensemble_tuning(ens, cap, out, nclasses) bind(c, name='psdns_gpu_ensemble_tuning')
+      import :: c_int, c_ptr, c_int32_t, c_double
+      type(c_ptr), value :: ens
+      integer(c_int32_t), value :: cap
+      real(c_double), intent(out) :: out(*)
+      integer(c_int32_t), intent(out) :: nclasses
+    end function
     integer(c_int) function psdns_gpu_ensemble_spectra(ens, box, which, ek, dk, eijk, stats) &
         bind(c, name='psdns_gpu_ensemble_spectra')
       import :: c_int, c_ptr, c_int32_t, c_double

@@ -51,6 +51,7 @@ EXPORTS = (
     "psdns_gpu_ensemble_set_state",
     "psdns_gpu_ensemble_get_state",
     "psdns_gpu_ensemble_step",
+    "psdns_gpu_ensemble_tuning",
     "psdns_gpu_ensemble_spectra",
     "psdns_gpu_default_params",
     "psdns_gpu_geometry",
@@ -191,6 +192,7 @@ def load():
     L.psdns_gpu_ensemble_set_state.argtypes = [vp, ctypes.c_int32, dp, ctypes.c_int32]
     L.psdns_gpu_ensemble_get_state.argtypes = [vp, ctypes.c_int32, dp, ctypes.c_int32, ctypes.c_int32]
     L.psdns_gpu_ensemble_step.argtypes = [vp, ctypes.c_int32, dp]
+    L.psdns_gpu_ensemble_tuning.argtypes = [vp, ctypes.c_int32, dp, ip]
     L.psdns_gpu_ensemble_spectra.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, dp, dp, dp, dp]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
@@ -687,6 +689,17 @@ class Ensemble:
         if rc not in (0, 2):
             _check(rc, "psdns_gpu_ensemble_step")
         return rc, info
+
+    def tuning(self):
+        """The autotuner's choice per class (psdns_gpu_ensemble_tuning)."""
+        nc = ctypes.c_int32()
+        _check(load().psdns_gpu_ensemble_tuning(self._ens, 0, None, ctypes.byref(nc)), "ensemble_tuning")
+        out = np.zeros(8 * max(1, nc.value))
+        _check(load().psdns_gpu_ensemble_tuning(self._ens, nc.value, _dp(out), ctypes.byref(nc)), "ensemble_tuning")
+        keys = ("n", "boxes", "tuned", "boxes_per_launch", "k2_lines_per_block", "k4_lines_per_block",
+                "default_ms", "chosen_ms")
+        return [dict(zip(keys, [int(v) if j < 6 else float(v) for j, v in enumerate(out[8 * c:8 * c + 8])]))
+                for c in range(nc.value)]
 
     def spectra(self, box, which=FIELD_UN):
         n = self.params[box].nx

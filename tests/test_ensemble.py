@@ -76,3 +76,31 @@ def test_ensemble_rejects_mixed_precision(gpu_mod):
     b = gpu_mod.default_params(n=32, precision=1, cfl=-1.0, dt=0.01)
     with pytest.raises(gpu_mod.PsdnsError):
         gpu_mod.Ensemble([a, b])
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_tile_autotuner_keeps_results_bit_identical(gpu_mod, prec):
+    """Fixed-dt classes through the whole tuning (boxes per launch, then the
+    K2 and K4 tiles, two steps per candidate) and on into the captured graph:
+    every class reports a tuned choice, and every box equals its single-box
+    run to roundoff (a tile variant is another compiled instance of the
+    kernel, whose floating-point contraction may differ: FP64 1e-14, FP32
+    1e-6 relative L2; the sub-batch size alone changes nothing, see above)."""
+    boxes = [b for b in BOXES if b[2] < 0] + [(64, 0.02, -1.0, 0.003, 1, 31, 21), (64, 0.01, -1.0, 0.004, 3, 32, 22)]
+    steps = 36
+    ens = gpu_mod.Ensemble([_params(gpu_mod, prec, b) for b in boxes])
+    ens.field_init([b[6] for b in boxes])
+    rc, info = ens.step(steps)
+    assert rc == 0
+    tun = ens.tuning()
+    assert len(tun) == 3 and all(t["tuned"] == 1 for t in tun), tun
+    print("tuner:", tun)
+    for i, b in enumerate(boxes):
+        s = gpu_mod.Solver(_params(gpu_mod, prec, b))
+        s.field_init(b[6])
+        for _ in range(steps):
+            s.step()
+        a, b_ = ens.get_state(i, gpu_mod.FIELD_UN), s.get_state(gpu_mod.FIELD_UN)
+        assert np.linalg.norm(a - b_) / np.linalg.norm(b_) < (1e-14 if prec else 1e-6)
+        s.close()
+    ens.close()
