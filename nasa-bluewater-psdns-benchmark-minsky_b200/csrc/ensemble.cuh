@@ -403,7 +403,7 @@ int psdns_gpu_ensemble_tuning(void* ens, int32_t cap, double* out, int32_t* ncla
   for (size_t i = 0; i < E->cls.size() && (int32_t)i < cap && out; i++) {
     const EnsClass& e = *E->cls[i];
     const int xt2 = e.prec == PSDNS_PREC_FP64 ? Tiles<double>::XT2 : Tiles<float>::XT2;
-    const int xt4 = e.prec == PSDNS_PREC_FP64 ? Tiles<double>::XT4 : Tiles<float>::XT4;
+    const int xt4 = k4_xt(e.prec == PSDNS_PREC_FP64, e.n);
     const int m[3][2] = {{1, 1}, {1, 2}, {2, 1}};   // tile factor of variant 0, 1, 2: num/den
     double* r = out + 8 * i;
     r[0] = e.n;

@@ -114,10 +114,9 @@ template <typename T, int N> struct EnsImpl {
   template <int XT>
   static void k4(EnsClass& e, const Geo& g, const C* uz, C* ub, const C* tw, const StageTables<T>& st, int nb) {
     if constexpr (XT == 0 || kTiles) {
-      constexpr int X = XT > 0 ? XT : TL::XT4;
+      constexpr int X = XT > 0 ? XT : k4_xt(sizeof(T) == 8, N);
       k_zfwd<T, N, 0, false, XT><<<dim3(N / TL::YT4, (e.g.kxn + X - 1) / X, nb), K4LaunchX<T, N, X>::THREADS,
-                                   I::TWB + sizeof(C) * 2 * X * TL::YT4 * I::L, e.stream>>>(g, uz, ub, tw, st.b11,
-                                                                                            st.b33);
+                                   K4LaunchX<T, N, X>::SMEM, e.stream>>>(g, uz, ub, tw, st.b11, st.b33);
     }
   }
 
@@ -139,8 +138,8 @@ template <typename T, int N> struct EnsImpl {
     k_xchain<T, N><<<dim3(e.nzt, N, nb), K3Launch<T, N, 0>::THREADS, I::sm3(), e.stream>>>(
         g, uz, tw, st.b11, st.b22, st.b33, e.d_velmax + b0, kstep == 1 ? 1 : 0);
     switch (kTiles ? e.k4v : 0) {
-      case 1: k4<TL::XT4 / 2>(e, g, uz, ub, tw, st, nb); break;
-      case 2: k4<TL::XT4 * 2>(e, g, uz, ub, tw, st, nb); break;
+      case 1: k4<k4_xt(sizeof(T) == 8, N) / 2>(e, g, uz, ub, tw, st, nb); break;
+      case 2: k4<k4_xt(sizeof(T) == 8, N) * 2>(e, g, uz, ub, tw, st, nb); break;
       default: k4<0>(e, g, uz, ub, tw, st, nb);
     }
     CK(cudaGetLastError());

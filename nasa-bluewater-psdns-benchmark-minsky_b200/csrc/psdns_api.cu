@@ -334,8 +334,10 @@ template <typename T, int N, int NC> struct Impl {
   static size_t sm1() { return TWB + sizeof(C) * TL::TB_I * L; }
   static size_t sm2() { return TWB + sizeof(C) * TL::XT2 * L; }
   static size_t sm3() { return K3Launch<T, N, NC>::SMEM; }
-  static size_t sm4() { return TWB + sizeof(C) * 2 * TL::XT4 * TL::YT4 * L; }
+  static size_t sm4() { return K4Launch<T, N>::SMEM; }
   static size_t sm5() { return TWB + sizeof(C) * (4 + NC) * TL::TB_F * L; }
+  static size_t sm2tc() { return TWB + sizeof(C) * kTcXT2 * L + kTcTail; }
+  static size_t sm4tc() { return K4LaunchX<T, N, kTcXT4, true>::SMEM + kTcTail; }
 
   // the tensor-core form (FP32 state at n = 1024): the same kernels with
   // their 1-D transforms on the tensor cores, and a shared-memory tail
@@ -346,12 +348,12 @@ template <typename T, int N, int NC> struct Impl {
     if constexpr (kTc) {
       CK(cudaFuncSetAttribute(k_yinv<T, N, false, NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)(sm1() + kTcTail)));
-      CK(cudaFuncSetAttribute(k_zinv<T, N, NC, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)(sm2() + kTcTail)));
+      CK(cudaFuncSetAttribute(k_zinv<T, N, NC, false, true, kTcXT2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sm2tc()));
       CK(cudaFuncSetAttribute(k_xchain<T, N, NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)K3Launch<T, N, NC>::SMEM_TC));
-      CK(cudaFuncSetAttribute(k_zfwd<T, N, NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)(sm4() + kTcTail)));
+      CK(cudaFuncSetAttribute(k_zfwd<T, N, NC, true, kTcXT4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sm4tc()));
       CK(cudaFuncSetAttribute(k_yfwd<T, N, 1, NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)(sm5() + kTcTail)));
       CK(cudaFuncSetAttribute(k_yfwd<T, N, 2, NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -533,7 +535,8 @@ template <typename T, int N, int NC> struct Impl {
     {
       constexpr int TH = K4Launch<T, N>::THREADS;
       prof_mark(c, s, 3, 0);
-      k_zfwd<T, N, NC><<<dim3(N / TL::YT4, (kxn + TL::XT4 - 1) / TL::XT4), TH, sm4(), c.stream>>>(g, uz, ub, tw,
+      constexpr int XT4 = k4_xt(sizeof(T) == 8, N);
+      k_zfwd<T, N, NC><<<dim3(N / TL::YT4, (kxn + XT4 - 1) / XT4), TH, sm4(), c.stream>>>(g, uz, ub, tw,
                                                                                                    st.b11, st.b33);
       prof_mark(c, s, 3, 1);
     }
@@ -558,8 +561,8 @@ template <typename T, int N, int NC> struct Impl {
                                     sm1() + kTcTail, c.stream>>>(g, st, u, ub, tw, ta);
     prof_mark(c, s, 0, 1);
     prof_mark(c, s, 1, 0);
-    k_zinv<T, N, NC, false, true><<<dim3(N, (kxn + TL::XT2 - 1) / TL::XT2, 3 + 3 * NC),
-                                    Launch<T, N, TL::XT2>::THREADS, sm2() + kTcTail, c.stream>>>(
+    k_zinv<T, N, NC, false, true, kTcXT2><<<dim3(N, (kxn + kTcXT2 - 1) / kTcXT2, 3 + 3 * NC),
+                                            Launch<T, N, kTcXT2>::THREADS, sm2tc(), c.stream>>>(
         g, ub, uz, tw, st.b11, st.b33, ta);
     prof_mark(c, s, 1, 1);
     prof_mark(c, s, 2, 0);
@@ -570,8 +573,9 @@ template <typename T, int N, int NC> struct Impl {
                                            cb2, cb3, ta);
     prof_mark(c, s, 2, 1);
     prof_mark(c, s, 3, 0);
-    k_zfwd<T, N, NC, true><<<dim3(N / TL::YT4, (kxn + TL::XT4 - 1) / TL::XT4), K4Launch<T, N>::THREADS,
-                             sm4() + kTcTail, c.stream>>>(g, uz, ub, tw, st.b11, st.b33, ta);
+    k_zfwd<T, N, NC, true, kTcXT4><<<dim3(N / TL::YT4, (kxn + kTcXT4 - 1) / kTcXT4),
+                                     K4LaunchX<T, N, kTcXT4, true>::THREADS, sm4tc(), c.stream>>>(g, uz, ub, tw, st.b11,
+                                                                                          st.b33, ta);
     prof_mark(c, s, 3, 1);
     CK(cudaGetLastError());
     return 0;

@@ -85,19 +85,27 @@ template <typename T> struct StageTables {
 
 // per-precision tile sizes: TB_I = columns per K1 block (64 B runs in ub
 // for K2), TB_F = columns per K5 block, TZ = z lines per K3 tile (32 B
-// runs), XT2/XT4 = x lines per K2/K4 block, YT4 = y rows per K4 block.
+// runs), XT2 = x lines per K2 block (K4's: k4_xt), YT4 = y rows per K4 block.
 // Eight lines per block keep two to three blocks resident per SM, so that
 // one block's copies overlap another's transforms; sixteen-line blocks (one
-// per SM) measured slower for K1 and K4.
+// per SM) measured slower for K1 and K4.  The z transforms run smaller
+// blocks in FP32: K2 four lines (XT2 = 4) and K4 four (two x lines of two
+// fields), 4-9% faster at 512^3 and 1024^3 than eight and eight; sixteen-line
+// K2 blocks were 30% slower.
 // The inverse ub layout is blocked by TBL_I = 2 TB_I columns (128 B runs for
 // K2's reads), filled by pairs of K1 blocks.
 template <typename T> struct Tiles;
 template <> struct Tiles<float> {
-  static constexpr int TB_I = 8, TBL_I = 16, TB_F = 4, TBL_F = 8, TZ = 4, XT2 = 8, XT4 = 4, YT4 = 1;
+  static constexpr int TB_I = 8, TBL_I = 16, TB_F = 4, TBL_F = 8, TZ = 4, XT2 = 4, YT4 = 1;
 };
 template <> struct Tiles<double> {
-  static constexpr int TB_I = 4, TBL_I = 8, TB_F = 2, TBL_F = 4, TZ = 2, XT2 = 4, XT4 = 2, YT4 = 1;
+  static constexpr int TB_I = 4, TBL_I = 8, TB_F = 2, TBL_F = 4, TZ = 2, XT2 = 4, YT4 = 1;
 };
+
+// x lines per K4 block by box size (dbl: FP64 state).  FP32: four from
+// 512^3 up (1024^3: 11.44 ms against 11.77 with two), two below (256^3:
+// 0.148 ms against 0.150)
+__host__ __device__ constexpr int k4_xt(bool dbl, int n) { return dbl ? 2 : (n >= 512 ? 4 : 2); }
 
 // elements of one variable of the forward ub layout [a/TBL_F][y][a%TBL_F]
 // (K4 writes 64-byte runs; K5 blocks of TB_F columns read halves)
@@ -158,21 +166,32 @@ struct Launch {
   static_assert(THREADS % P == 0, "threads per line must divide the block");
 };
 
+template <int N> struct LS { static constexpr int value = N + N / 32 + 4; };
+
 // K1 and K4: one warp per line at n = 1024 FP32
 template <typename T, int N>
 struct K1Launch : Launch<T, N, Tiles<T>::TB_I, 1024> {};
+// K4 with XT x lines per block: three fields of every x line at once
+// (register-fed form, phase 1 of k_zfwd), or two (tensor-core form)
+template <typename T, int N, int XT, bool TCM = false>
+struct K4LaunchX : Launch<T, N, (TCM ? 2 : 3) * XT * Tiles<T>::YT4, 1024> {
+  static constexpr int NF = TCM ? 2 : 3;
+  // resident blocks the registers are sized for: about 112 registers a
+  // thread in the register-fed form (its last pass holds a line's operands
+  // and the store addresses), one to eight blocks
+  static constexpr int TH = Launch<T, N, NF * XT * Tiles<T>::YT4, 1024>::THREADS;
+  static constexpr int MINB_F = 65536 / (TH * 112) < 1 ? 1 : (65536 / (TH * 112) > 8 ? 8 : 65536 / (TH * 112));
+  static constexpr int MINB = TCM ? 2 : MINB_F;
+  static constexpr size_t SMEM =
+      sizeof(C2<T>) * (FFTPlan<T, N>::TWSIZE + (size_t)NF * XT * Tiles<T>::YT4 * LS<N>::value);
+};
 template <typename T, int N>
-struct K4Launch : Launch<T, N, 2 * Tiles<T>::XT4 * Tiles<T>::YT4, 1024> {};
-// K4 with XT x lines per block (the ensemble tuner's tile variants)
-template <typename T, int N, int XT>
-struct K4LaunchX : Launch<T, N, 2 * XT * Tiles<T>::YT4, 1024> {};
+struct K4Launch : K4LaunchX<T, N, k4_xt(sizeof(T) == 8, N)> {};
 
 // K5 holds one CTA per SM (its (4 + nc) * TB_F lines fill shared memory), so
 // it runs every line of a block at once
 template <typename T, int N, int NC>
 struct K5Launch : Launch<T, N, (4 + NC) * Tiles<T>::TB_F, 1024> {};
-
-template <int N> struct LS { static constexpr int value = N + N / 32 + 4; };
 
 // Mixed-precision form of the stage kernels (template flag TCM, FP32 state
 // at n = 1024): every 1024-point transform runs on the tensor cores
@@ -186,6 +205,10 @@ struct TcArgs {
   unsigned* err = nullptr;
 };
 constexpr size_t kTcTail = tc::kBBytes + 16;
+// z tiles of the tensor-core kernels, independent of Tiles<float>: an operand
+// tile (32 KB) overlays four lines, so every line buffer that one transform
+// call runs on holds at least four lines
+constexpr int kTcXT2 = 8, kTcXT4 = 4;
 // TMEM columns for nlines lines: 64 per tile of four, as a power of two
 __host__ __device__ constexpr int tc_cols(int nlines) {
   int c = 64 * ((nlines + 3) / 4), p = 32;
@@ -318,7 +341,8 @@ k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>*
   // 4 = i b11 kx theta and slot 5 = i b33 kz theta (both from ub 3),
   // itransform.f:188-198
   using C = C2<T>;
-  constexpr int XT = XTO > 0 ? XTO : Tiles<T>::XT2, TB = Tiles<T>::TB_I, TZ = Tiles<T>::TZ;
+  constexpr int XT = XTO > 0 ? XTO : Tiles<T>::XT2, TZ = Tiles<T>::TZ;
+  static_assert(!TCM || XT >= 4, "an operand tile overlays four lines");
   constexpr int THREADS = Launch<T, N, XT>::THREADS;
   constexpr int L = LS<N>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -469,6 +493,147 @@ __device__ __forceinline__ void xchain_pack(const Geo& g, const C2<T>* __restric
     }
 }
 
+// Register-level pair packing for plans of two passes whose last radix is
+// the operand count E (so P = R0 threads per line, inside one warp).  Thread
+// t of a line then holds the elements t + P m (m < R1) both as the operands
+// of pass 0 and as the outputs of the last pass, and the Hermitian partner
+// N - x of its element x sits in lane P - t (slot R1 - 1 - m; lane 0 pairs
+// with itself, slot R1 - m).  The packing before the inverse transform and
+// the unpacking after the forward one then exchange values by warp shuffles
+// instead of a shared-memory round trip of every line.
+template <typename T, int N>
+struct XFuse {
+  using PL = FFTPlan<T, N>;
+  static constexpr bool value =
+      is_pow2(N) && PL::NPASS == 2 && PL::rad(1) == PL::E && PL::P <= 32 && (32 % PL::P) == 0;
+};
+
+// xchain_pack followed by pass 0 of the transform, with the operands
+// loaded from uz into registers: line l = v NPAIR + p gets
+// conj(A + i B) of the real lines z = zt TZ + 2p, 2p + 1 of slot v0 + v (the
+// band kx in [kxn, N - kxn] zero), and pass 0's output goes to shared memory.
+// Every thread of the block runs the same rounds (the shuffles name whole
+// warps); loads and stores are predicated on the line being one of NV NPAIR.
+template <typename T, int N, int NV, int THREADS>
+__device__ __forceinline__ void xchain_load_pass0(const Geo& g, const C2<T>* __restrict__ uz, int v0, int y,
+                                                  int zt, C2<T>* buf, int L) {
+  using C = C2<T>;
+  using PL = FFTPlan<T, N>;
+  static_assert(XFuse<T, N>::value, "plan without register-level packing");
+  constexpr int TZ = Tiles<T>::TZ, NPAIR = TZ / 2;
+  constexpr int R0 = PL::rad(0), R1 = PL::rad(1), P = PL::P, E = PL::E, H = R1 / 2;
+  constexpr int LPR = THREADS / P, NB = E / R0;
+  static_assert(THREADS % 32 == 0, "whole warps");
+  const int kxn = g.kxn;
+  const int lr = threadIdx.x / P, t = threadIdx.x % P;
+  const int src = (P - t) & (P - 1);
+  for (int l0 = 0; l0 < NV * NPAIR; l0 += LPR) {
+    const int l = l0 + lr;
+    const bool act = l < NV * NPAIR;
+    const int v = act ? l / NPAIR : 0, p = l % NPAIR;
+    const C* col = uz + (((size_t)(v0 + v) * N + y) * g.nzt + zt) * (size_t)kxn * TZ + 2 * p;
+    C a[H], b[H];
+#pragma unroll
+    for (int m = 0; m < H; m++) {
+      const int x = t + P * m;
+      a[m] = cmk<C>(0, 0);
+      b[m] = cmk<C>(0, 0);
+      if (act && x < kxn) {
+        if constexpr (sizeof(C) == 8) {
+          const float4 q = *reinterpret_cast<const float4*>(col + (size_t)x * TZ);
+          a[m] = cmk<C>(q.x, q.y);
+          b[m] = cmk<C>(q.z, q.w);
+        } else {
+          a[m] = col[(size_t)x * TZ];
+          b[m] = col[(size_t)x * TZ + 1];
+        }
+      }
+    }
+    // slot m < H: element x = t + P m; slot m >= H: element N - x' of lane
+    // P - t's x' at slot R1 - 1 - m (lane 0: its own x' at slot R1 - m, and
+    // zero at slot H, x = N/2)
+    C z[R1];
+#pragma unroll
+    for (int m = H; m < R1; m++) z[m] = cmk<C>(0, 0);
+#pragma unroll
+    for (int m = 0; m < H; m++) {
+      const C av = a[m], bv = b[m];
+      z[m] = (t == 0 && m == 0) ? cmk<C>(av.x, -bv.x) : cmk<C>(av.x - bv.y, -(av.y + bv.x));
+      const C mv = cmk<C>(av.x + bv.y, -(bv.x - av.y));   // element N - x
+      const C got = cmk<C>(__shfl_sync(0xffffffffu, mv.x, src, P), __shfl_sync(0xffffffffu, mv.y, src, P));
+      if (t != 0) {
+        z[R1 - 1 - m] = got;
+      } else if (m >= 1) {
+        z[R1 - m] = mv;
+      }
+    }
+    if (act) {
+      C* line = buf + (size_t)l * L;
+#pragma unroll
+      for (int q = 0; q < NB; q++) {
+        C w[R0];
+#pragma unroll
+        for (int r = 0; r < R0; r++) w[r] = z[q + NB * r];   // element t + q P + r R1
+        dft_s<R0, 1>(w);
+        const int j = t + q * P;
+#pragma unroll
+        for (int r = 0; r < R0; r++) line[pad32(j * R0 + r)] = w[r];
+      }
+    }
+  }
+}
+
+// The last pass of the forward transform of nlines lines with xchain_store's
+// unpacking done in registers: A(x), B(x) of the real lines z = zt TZ + 2p,
+// 2p + 1 go to uz slot l / NPAIR for x < kxn.  Called by every thread of
+// the block (whole warps per round).
+template <typename T, int N, int THREADS>
+__device__ __forceinline__ void xchain_last_store(const Geo& g, const C2<T>* buf, int nlines, int L,
+                                                  const C2<T>* tw, C2<T>* __restrict__ uz, int y, int zt,
+                                                  T half_factor) {
+  using C = C2<T>;
+  using PL = FFTPlan<T, N>;
+  static_assert(XFuse<T, N>::value, "plan without register-level packing");
+  constexpr int TZ = Tiles<T>::TZ, NPAIR = TZ / 2;
+  constexpr int R1 = PL::rad(1), P = PL::P, E = PL::E, H = R1 / 2, NS = PL::ns(1);
+  constexpr int LPR = THREADS / P;
+  static_assert(NS == P && E == R1, "the last pass holds elements t + P m");
+  const int kxn = g.kxn;
+  const int lr = threadIdx.x / P, t = threadIdx.x % P;
+  const int src = (P - t) & (P - 1);
+  for (int l0 = 0; l0 < nlines; l0 += LPR) {
+    const int l = l0 + lr;
+    const bool act = l < nlines;
+    C v[E];
+    if (act) {
+      pass_butterflies<C, N, R1, NS, E, P, PL::fact(1)>(buf + (size_t)l * L, t, tw + PL::twoff(1), v);
+    } else {
+#pragma unroll
+      for (int m = 0; m < E; m++) v[m] = cmk<C>(0, 0);
+    }
+    const int b = act ? l / NPAIR : 0, p = l % NPAIR;
+    C* col = uz + (((size_t)b * N + y) * g.nzt + zt) * (size_t)kxn * TZ + 2 * p;
+#pragma unroll
+    for (int m = 0; m < H; m++) {
+      const int x = t + P * m;
+      const C Y = v[m];
+      const C sent = v[R1 - 1 - m];
+      const C got = cmk<C>(__shfl_sync(0xffffffffu, sent.x, src, P), __shfl_sync(0xffffffffu, sent.y, src, P));
+      const C Yn = t == 0 ? v[(R1 - m) % R1] : got;
+      if (act && x < kxn) {
+        const T ax = (Y.x + Yn.x) * half_factor, ay = (Y.y - Yn.y) * half_factor;
+        const T bx = (Y.y + Yn.y) * half_factor, by = (Yn.x - Y.x) * half_factor;
+        if constexpr (sizeof(C) == 8) {
+          *reinterpret_cast<float4*>(col + (size_t)x * TZ) = make_float4(ax, ay, bx, by);
+        } else {
+          col[(size_t)x * TZ] = cmk<C>(ax, ay);
+          col[(size_t)x * TZ + 1] = cmk<C>(bx, by);
+        }
+      }
+    }
+  }
+}
+
 // K3 runs the five output products of a tile as one batch of 5 * TZ/2
 // lines: one warp per line at n = 1024 (a multiple of 32 threads, so that
 // the velmax warp reduction sees whole warps)
@@ -491,7 +656,7 @@ struct K3Launch {
 };
 
 template <typename T, int N, int NC = 0, bool TCM = false>
-__global__ void __launch_bounds__(K3Launch<T, N, NC>::THREADS)
+__global__ void __launch_bounds__(K3Launch<T, N, NC>::THREADS, TCM ? 1 : 2)
 k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T b22, T b33,
          unsigned long long* velmax_bits, int want_velmax, T cb1 = T(0), T cb2 = T(0), T cb3 = T(0),
          TcArgs tca = TcArgs()) {
@@ -521,16 +686,27 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
   uz += box * g.zbox;
   velmax_bits += box;
   const int kxn = g.kxn;
-  // zero the band kx in [kxn, n-kxn] (includes the Nyquist column)
-  for (int e = threadIdx.x; e < NVIN * NPAIR * N; e += THREADS) {
-    const int k = e % N;
-    if (k >= kxn && k <= N - kxn) bufU[(e / N) * L + pad32(k)] = cmk<C>(0, 0);
+  // the pair packing and unpacking in registers (XFuse) on the FFT path; the
+  // tensor-core path and the other plans go through shared memory
+  constexpr bool FUSE = !TCM && XFuse<T, N>::value;
+  if constexpr (FUSE) {
+    xchain_load_pass0<T, N, NVIN, THREADS>(g, uz, 0, y, zt, bufU, L);
+    cp_async_wait_all();
+    __syncthreads();
+    fft_passes<T, N, THREADS, 1>(bufU, NVIN * NPAIR, L, tw);
+    __syncthreads();
+  } else {
+    // zero the band kx in [kxn, n-kxn] (includes the Nyquist column)
+    for (int e = threadIdx.x; e < NVIN * NPAIR * N; e += THREADS) {
+      const int k = e % N;
+      if (k >= kxn && k <= N - kxn) bufU[(e / N) * L + pad32(k)] = cmk<C>(0, 0);
+    }
+    xchain_pack<T, N, 3, THREADS>(g, uz, 0, y, zt, bufU, L);
+    if constexpr (NC > 0) xchain_pack<T, N, 3, THREADS>(g, uz, 3, y, zt, bufU + 3 * NPAIR * L, L);
+    cp_async_wait_all();
+    __syncthreads();
+    lines_fft<T, N, THREADS, TCM>(bufU, NVIN * NPAIR, L, tw, w);
   }
-  xchain_pack<T, N, 3, THREADS>(g, uz, 0, y, zt, bufU, L);
-  if constexpr (NC > 0) xchain_pack<T, N, 3, THREADS>(g, uz, 3, y, zt, bufU + 3 * NPAIR * L, L);
-  cp_async_wait_all();
-  __syncthreads();
-  lines_fft<T, N, THREADS, TCM>(bufU, NVIN * NPAIR, L, tw, w);
   // buffers now hold conj(a + i b): a = re, b = -im
   const T hf = T(0.5) / T(N);
   // realspace_vel.f:105-114, in place: slot 0 = b11 u^2 - bv2, 1 = uv,
@@ -568,17 +744,24 @@ k_xchain(Geo g, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11, T
     if ((threadIdx.x & 31) == 0) atomic_max_pos<T>(velmax_bits, vm);
   }
   __syncthreads();
-  lines_fft<T, N, THREADS, TCM>(bufU, (5 + NC) * NPAIR, L, tw, w);
-  if constexpr (TCM) tc::teardown<NCOL>(w);
-  xchain_store<T, N>(g, bufU, 5 + NC, L, uz, 0, y, zt, hf);
+  if constexpr (FUSE) {
+    // pass 0 in shared memory; each line's last pass runs on the warp that
+    // wrote it, so a warp barrier (inside fft_pass) orders the two
+    fft_passes_until<T, N, THREADS, 0, 1>(bufU, (5 + NC) * NPAIR, L, tw);
+    xchain_last_store<T, N, THREADS>(g, bufU, (5 + NC) * NPAIR, L, tw, uz, y, zt, hf);
+  } else {
+    lines_fft<T, N, THREADS, TCM>(bufU, (5 + NC) * NPAIR, L, tw, w);
+    if constexpr (TCM) tc::teardown<NCOL>(w);
+    xchain_store<T, N>(g, bufU, 5 + NC, L, uz, 0, y, zt, hf);
+  }
 }
 
 // ---------------------------------------------------------------------------
 // K4: z forward FFT + derivative combination + cylinder pack into ub (TB_F)
-// grid (n, ceil(kxn/XT4)).  Output slots: 0 = d/dx(u^2-v^2)+d/dz(uw) partial,
+// grid (n, ceil(kxn/k4_xt)).  Output slots: 0 = d/dx(u^2-v^2)+d/dz(uw) partial,
 // 1 = uv, 2 = d/dx(uw)+d/dz(w^2-v^2), 3 = vw (y derivatives added in K5).
 // ---------------------------------------------------------------------------
-template <typename T, int N, int XT = Tiles<T>::XT4>
+template <typename T, int N, int XT>
 __device__ __forceinline__ void zfwd_load(const Geo& g, const C2<T>* __restrict__ uz, int slot, int y0, int ny,
                                           int x0, int nl, C2<T>* buf, int L) {
   // lines l = yy*nl + xl, rows y0+yy, columns x0+xl; full tiles (nl = XT)
@@ -604,7 +787,7 @@ __device__ __forceinline__ void zfwd_load(const Geo& g, const C2<T>* __restrict_
   }
 }
 
-template <typename T, int N, int MODE, int XT = Tiles<T>::XT4>
+template <typename T, int N, int MODE, int XT>
 __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const C2<T>* s1, int L,
                                            C2<T>* __restrict__ ub, int slot, int y0, int /*ny*/, int x0, int x1,
                                            T b11, T b33) {
@@ -657,75 +840,160 @@ __device__ __forceinline__ void zfwd_store(const Geo& g, const C2<T>* s0, const 
   }
 }
 
-// XTO > 0: XTO x lines per block instead of Tiles<T>::XT4 (ensemble tuner)
+// K4 with register-fed transforms (the FP32 and FP64 stage kernels): pass 0
+// of every z transform takes its operands straight from uz, and the last pass
+// of P1, P3, P2, P4 (and of the scalar term) writes the cylinder entries of ub
+// from registers (consecutive z of a warp are consecutive cylinder indices),
+// so shared memory carries only the exchanges between passes and the P5
+// lines that the derivative combinations of P1 and P3 read.
+// Phase 1: P5, P1, P3 (P5's last pass in shared memory; then P1 -> ub slot 0,
+// P3 -> slot 2); phase 2: P2 -> slot 1, P4 -> slot 3 (uz slot 5 -> ub slot 4
+// with a scalar).  Field f of x line xl is line f nl + xl of its phase.
+template <typename T, int N, int NC, int THREADS>
+__device__ __forceinline__ void zfwd_fused(const Geo& g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub,
+                                           C2<T>* buf, const C2<T>* tw, int y, int x0, int nl, T b11, T b33) {
+  using C = C2<T>;
+  using PL = FFTPlan<T, N>;
+  static_assert(Tiles<T>::YT4 == 1, "one y row per block");
+  static_assert(PL::NPASS >= 2, "load and store passes must differ");
+  constexpr int TZ = Tiles<T>::TZ, TB = Tiles<T>::TBL_F, L = LS<N>::value;
+  constexpr size_t zstride = (size_t)kxn_of(N) * TZ;   // g.kxn, as a constant
+  const size_t var = ubf_var_elems<T>(g.nab_f, N);
+  // uz field `slot` of x line x0 + xl at row y: entry z at (z / TZ) zstride + z % TZ
+  struct In { const C* src; };
+  auto in_line = [&](int slot, int xl) {
+    return In{uz + ((((size_t)slot * N + y) * g.nzt) * g.kxn + x0 + xl) * TZ};
+  };
+  auto fetch = [&](const In& s, int z) { return __ldg(s.src + ((unsigned)z / TZ) * zstride + (unsigned)z % TZ); };
+  auto nofix = [](const In&, int, C v) { return v; };
+  // ub slot of x line x0 + xl: column x holds kz = 0..kc then -kc..-1 from
+  // cylinder index c0 (mpisetup.f:322-357); mode 0: i kx P1 + i b33 kz P5,
+  // mode 1: i b11 kx P5 + i kz P3, mode 2: the value itself
+  struct Out { C* dst; const C* p5; int x, c0, kc, mode; };
+  auto out_line = [&](int slot, int xl, int mode) {
+    const int c0 = __ldg(g.colstart + x0 + xl);
+    return Out{ub + (size_t)slot * var, buf + (size_t)xl * L, x0 + xl, c0,
+               (__ldg(g.colstart + x0 + xl + 1) - c0 - 1) / 2, mode};
+  };
+  auto store = [&](const Out& s, int base, const C* v, auto Rc, auto NSc) {
+    constexpr int R = decltype(Rc)::value, NS = decltype(NSc)::value;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int z = base + r * NS;
+      if (z > s.kc && z < N - s.kc) continue;
+      C out = v[r];
+      if (s.mode == 0) {
+        const T kx = T(s.x), bk3 = b33 * T(kwave<N>(z));
+        const C p5 = s.p5[pad32(z)];
+        out = cmk<C>(-kx * v[r].y - bk3 * p5.y, kx * v[r].x + bk3 * p5.x);
+      } else if (s.mode == 1) {
+        const T bk1 = b11 * T(s.x), kz = T(kwave<N>(z));
+        const C p5 = s.p5[pad32(z)];
+        out = cmk<C>(-bk1 * p5.y - kz * v[r].y, bk1 * p5.x + kz * v[r].x);
+      }
+      const int a = s.c0 + (z <= s.kc ? z : z - N + 2 * s.kc + 1);
+      s.dst[((size_t)((unsigned)a / TB) * N + y) * TB + ((unsigned)a % TB)] = out;
+    }
+  };
+  // phase 1
+  fft_pass0_load<T, N, THREADS>(
+      buf, 3 * nl, L, [&](int l) { return in_line(l < nl ? 4 : (l < 2 * nl ? 0 : 2), l % nl); }, fetch, nofix);
+  cp_async_wait_all();
+  __syncthreads();
+  fft_passes_until<T, N, THREADS, 1, PL::NPASS - 1>(buf, 3 * nl, L, tw);
+  fft_passes_until<T, N, THREADS, PL::NPASS - 1, PL::NPASS>(buf, nl, L, tw);
+  __syncthreads();   // P5 lines complete
+  fft_pass_last_store<T, N, THREADS>(buf + (size_t)nl * L, 2 * nl, L, tw,
+                                     [&](int l) { return l < nl ? out_line(0, l, 0) : out_line(2, l - nl, 1); },
+                                     store);
+  __syncthreads();   // every line of phase 1 read
+  // phase 2
+  constexpr int NV2 = 2 + NC;
+  fft_pass0_load<T, N, THREADS>(
+      buf, NV2 * nl, L, [&](int l) { return in_line(l < nl ? 1 : (l < 2 * nl ? 3 : 5), l % nl); }, fetch, nofix);
+  __syncthreads();
+  fft_passes_until<T, N, THREADS, 1, PL::NPASS - 1>(buf, NV2 * nl, L, tw);
+  fft_pass_last_store<T, N, THREADS>(
+      buf, NV2 * nl, L, tw,
+      [&](int l) { return out_line(l < nl ? 1 : (l < 2 * nl ? 3 : 4), l % nl, 2); }, store);
+}
+
+// XTO > 0: XTO x lines per block instead of k4_xt (ensemble tuner)
 template <typename T, int N, int NC = 0, bool TCM = false, int XTO = 0>
-__global__ void __launch_bounds__(K4LaunchX<T, N, (XTO > 0 ? XTO : Tiles<T>::XT4)>::THREADS, TCM ? 2 : 3)
+__global__ void __launch_bounds__(K4LaunchX<T, N, (XTO > 0 ? XTO : k4_xt(sizeof(T) == 8, N)), TCM>::THREADS,
+                                  K4LaunchX<T, N, (XTO > 0 ? XTO : k4_xt(sizeof(T) == 8, N)), TCM>::MINB)
 k_zfwd(Geo g, const C2<T>* __restrict__ uz, C2<T>* __restrict__ ub, const C2<T>* __restrict__ tw_g,
        T b11, T b33, TcArgs tca = TcArgs()) {
   // NC = 1: the scalar advection term (uz slot 5) goes to ub slot 4 without
   // derivatives (transform.f: i2f = 4+nc)
-  // grid (n / YT4, ceil(kxn / XT4)): YT4 adjacent y rows x XT4 x lines
+  // grid (n / YT4, ceil(kxn / XT)): YT4 adjacent y rows x XT x lines
   using C = C2<T>;
-  constexpr int XT = XTO > 0 ? XTO : Tiles<T>::XT4, YT = Tiles<T>::YT4, NLT = XT * YT;
-  constexpr int THREADS = K4LaunchX<T, N, XT>::THREADS;
+  constexpr int XT = XTO > 0 ? XTO : k4_xt(sizeof(T) == 8, N), YT = Tiles<T>::YT4, NLT = XT * YT;
+  static_assert(!TCM || NLT >= 4, "an operand tile overlays four lines of s0 or s1");
+  constexpr int THREADS = K4LaunchX<T, N, XT, TCM>::THREADS;
   constexpr int L = LS<N>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   C* s0 = tw + FFTPlan<T, N>::TWSIZE;
   C* s1 = s0 + NLT * L;
   load_twiddles<T, N>(tw, tw_g);
-  constexpr int NCOL = tc_cols(2 * NLT);
-  tc::Work w;
-  if constexpr (TCM) tc_begin<NCOL>(w, reinterpret_cast<unsigned char*>(s1 + NLT * L), tca);
-  // grid (n / YT4, ceil(kxn / XT4), boxes)
+  // grid (n / YT4, ceil(kxn / XT), boxes)
   const int y0 = blockIdx.x * YT, x0 = blockIdx.y * XT, box = blockIdx.z;
   uz += box * g.zbox;
   ub += box * g.bbox;
   const int x1 = min(x0 + XT, g.kxn);
   const int nl = x1 - x0;
-  const int nt = nl * YT;
-  // round 1: P5 -> s0, P1 -> s1
-  zfwd_load<T, N, XT>(g, uz, 4, y0, YT, x0, nl, s0, L);
-  zfwd_load<T, N, XT>(g, uz, 0, y0, YT, x0, nl, s1, L);
-  cp_async_wait_all();
-  __syncthreads();
-  if (nl == XT) {
-    lines_fft<T, N, THREADS, TCM>(s0, 2 * NLT, L, tw, w);
+  if constexpr (!TCM) {
+    zfwd_fused<T, N, NC, THREADS>(g, uz, ub, s0, tw, y0, x0, nl, b11, b33);
   } else {
-    lines_fft<T, N, THREADS, TCM>(s0, nt, L, tw, w);
-    lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
-  }
-  zfwd_store<T, N, 0, XT>(g, s0, s1, L, ub, 0, y0, YT, x0, x1, b11, b33);
-  __syncthreads();
-  // round 2: P3 -> s1
-  zfwd_load<T, N, XT>(g, uz, 2, y0, YT, x0, nl, s1, L);
-  cp_async_wait_all();
-  __syncthreads();
-  lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
-  zfwd_store<T, N, 1, XT>(g, s0, s1, L, ub, 2, y0, YT, x0, x1, b11, b33);
-  __syncthreads();
-  // round 3: P2 -> s0, P4 -> s1
-  zfwd_load<T, N, XT>(g, uz, 1, y0, YT, x0, nl, s0, L);
-  zfwd_load<T, N, XT>(g, uz, 3, y0, YT, x0, nl, s1, L);
-  cp_async_wait_all();
-  __syncthreads();
-  if (nl == XT) {
-    lines_fft<T, N, THREADS, TCM>(s0, 2 * NLT, L, tw, w);
-  } else {
-    lines_fft<T, N, THREADS, TCM>(s0, nt, L, tw, w);
-    lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
-  }
-  // P2 -> ub slot 1 and P4 -> ub slot 3 in one pass over the cylinder indices
-  zfwd_store<T, N, 4, XT>(g, s0, s1, L, ub, 1, y0, YT, x0, x1, b11, b33);
-  if constexpr (NC > 0) {
+    // tensor-core form: rounds of two fields through shared memory
+    constexpr int NCOL = tc_cols(2 * NLT);
+    tc::Work w;
+    tc_begin<NCOL>(w, reinterpret_cast<unsigned char*>(s1 + NLT * L), tca);
+    const int nt = nl * YT;
+    // round 1: P5 -> s0, P1 -> s1
+    zfwd_load<T, N, XT>(g, uz, 4, y0, YT, x0, nl, s0, L);
+    zfwd_load<T, N, XT>(g, uz, 0, y0, YT, x0, nl, s1, L);
+    cp_async_wait_all();
     __syncthreads();
-    zfwd_load<T, N, XT>(g, uz, 5, y0, YT, x0, nl, s1, L);
+    if (nl == XT) {
+      lines_fft<T, N, THREADS, TCM>(s0, 2 * NLT, L, tw, w);
+    } else {
+      lines_fft<T, N, THREADS, TCM>(s0, nt, L, tw, w);
+      lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
+    }
+    zfwd_store<T, N, 0, XT>(g, s0, s1, L, ub, 0, y0, YT, x0, x1, b11, b33);
+    __syncthreads();
+    // round 2: P3 -> s1
+    zfwd_load<T, N, XT>(g, uz, 2, y0, YT, x0, nl, s1, L);
     cp_async_wait_all();
     __syncthreads();
     lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
-    zfwd_store<T, N, 3, XT>(g, s0, s1, L, ub, 4, y0, YT, x0, x1, b11, b33);
+    zfwd_store<T, N, 1, XT>(g, s0, s1, L, ub, 2, y0, YT, x0, x1, b11, b33);
+    __syncthreads();
+    // round 3: P2 -> s0, P4 -> s1
+    zfwd_load<T, N, XT>(g, uz, 1, y0, YT, x0, nl, s0, L);
+    zfwd_load<T, N, XT>(g, uz, 3, y0, YT, x0, nl, s1, L);
+    cp_async_wait_all();
+    __syncthreads();
+    if (nl == XT) {
+      lines_fft<T, N, THREADS, TCM>(s0, 2 * NLT, L, tw, w);
+    } else {
+      lines_fft<T, N, THREADS, TCM>(s0, nt, L, tw, w);
+      lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
+    }
+    // P2 -> ub slot 1 and P4 -> ub slot 3 in one pass over the cylinder indices
+    zfwd_store<T, N, 4, XT>(g, s0, s1, L, ub, 1, y0, YT, x0, x1, b11, b33);
+    if constexpr (NC > 0) {
+      __syncthreads();
+      zfwd_load<T, N, XT>(g, uz, 5, y0, YT, x0, nl, s1, L);
+      cp_async_wait_all();
+      __syncthreads();
+      lines_fft<T, N, THREADS, TCM>(s1, nt, L, tw, w);
+      zfwd_store<T, N, 3, XT>(g, s0, s1, L, ub, 4, y0, YT, x0, x1, b11, b33);
+    }
+    tc::teardown<NCOL>(w);
   }
-  if constexpr (TCM) tc::teardown<NCOL>(w);
 }
 
 // ---------------------------------------------------------------------------
@@ -1007,14 +1275,22 @@ k_xspline(Geo g, const C2<T>* __restrict__ uz, typename V4T<T>::type* __restrict
   load_twiddles<T, N>(tw, tw_g);
   const int zt = blockIdx.x, y = blockIdx.y;
   const int kxn = g.kxn;
-  for (int e = threadIdx.x; e < 3 * NPAIR * N; e += THREADS) {
-    const int k = e % N;
-    if (k >= kxn && k <= N - kxn) bufU[(e / N) * L + pad32(k)] = cmk<C>(0, 0);
+  if constexpr (XFuse<T, N>::value) {
+    xchain_load_pass0<T, N, 3, THREADS>(g, uz, 0, y, zt, bufU, L);
+    cp_async_wait_all();
+    __syncthreads();
+    fft_passes<T, N, THREADS, 1>(bufU, 3 * NPAIR, L, tw);
+    __syncthreads();
+  } else {
+    for (int e = threadIdx.x; e < 3 * NPAIR * N; e += THREADS) {
+      const int k = e % N;
+      if (k >= kxn && k <= N - kxn) bufU[(e / N) * L + pad32(k)] = cmk<C>(0, 0);
+    }
+    xchain_pack<T, N, 3, THREADS>(g, uz, 0, y, zt, bufU, L);
+    cp_async_wait_all();
+    __syncthreads();
+    fft_lines<T, N, THREADS>(bufU, 3 * NPAIR, L, tw);
   }
-  xchain_pack<T, N, 3, THREADS>(g, uz, 0, y, zt, bufU, L);
-  cp_async_wait_all();
-  __syncthreads();
-  fft_lines<T, N, THREADS>(bufU, 3 * NPAIR, L, tw);
   // buffer = conj(a + i b): line z = 2p is re, line 2p+1 is -im
   for (int e = threadIdx.x; e < TZ * N; e += THREADS) {
     const int zz = e / N, x = e % N, p = zz / 2;

@@ -206,7 +206,8 @@ static int run(const psdns_params* prm, int kstep, const double* gsh, double dt,
   }
   {
     constexpr int TH = K4Launch<T, N>::THREADS;
-    k_zfwd<T, N><<<dim3(N / TL::YT4, (kxn + TL::XT4 - 1) / TL::XT4), TH, TWB + sizeof(C) * 2 * TL::XT4 * TL::YT4 * L, st>>>(
+    constexpr int XT4 = k4_xt(sizeof(T) == 8, N);
+    k_zfwd<T, N><<<dim3(N / TL::YT4, (kxn + XT4 - 1) / XT4), TH, K4Launch<T, N>::SMEM, st>>>(
         geo, uz, ub, twd, stb.b11, stb.b33);
   }
   {
