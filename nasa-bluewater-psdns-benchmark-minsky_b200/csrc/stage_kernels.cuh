@@ -331,8 +331,12 @@ __host__ __device__ __forceinline__ int k1_blocks(int nab_i) { return nab_i; }
 // ---------------------------------------------------------------------------
 // XTO > 0: XTO x lines per block instead of Tiles<T>::XT2 (a tile variant
 // of the ensemble autotuner; every line is transformed the same way)
+// The FP32 velocity form's registers are sized for five resident blocks
+// (102 a thread at 128 threads): 1024^3 5.65 -> 5.33 ms against three; six
+// blocks (85, small spills) 6.01 ms.
 template <typename T, int N, int NC = 0, bool GRAD = false, bool TCM = false, int XTO = 0>
-__global__ void __launch_bounds__(Launch<T, N, (XTO > 0 ? XTO : Tiles<T>::XT2)>::THREADS, TCM ? 2 : 3)
+__global__ void __launch_bounds__(Launch<T, N, (XTO > 0 ? XTO : Tiles<T>::XT2)>::THREADS,
+                                  TCM ? 2 : (sizeof(T) == 4 && NC == 0 && !GRAD ? 5 : 3))
 k_zinv(Geo g, const C2<T>* __restrict__ ub, C2<T>* __restrict__ uz, const C2<T>* __restrict__ tw_g, T b11 = T(1),
        T b33 = T(1), TcArgs tca = TcArgs()) {
   // GRAD (grid.z = 2): uz slot 0 = i b11 kx u, slot 1 = i b33 kz w, the
