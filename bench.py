@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--dft-lines", type=int, default=0,
                     help="instead: the 1024-point line DFT on its own (FP32 Stockham and split-BF16 tensor cores), "
                          "L lines through psdns_gpu_dft_lines")
+    ap.add_argument("--diagnostics", action="store_true",
+                    help="time the diagnostics (shell spectra, 1-D spectra and scales, gradient "
+                         "moments, transfer spectrum) on the --n box instead of the step")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="instead: B boxes of n in {32,48,64,96}, log-uniform viscosity, fixed dt")
     return ap.parse_args()
@@ -320,8 +323,52 @@ def run_dft_lines(args):
     return 0
 
 
+def run_diagnostics(args):
+    """The diagnostics of the library on the bench's box (no particles): each
+    call timed on the host around the synchronous C-ABI call (device work plus
+    the small result copies), median of --steps calls after --warmup."""
+    import math
+    import statistics
+    import torch
+    import psdns_gpu as P
+    torch.cuda.set_device(0)
+    n = args.n
+    prec = P.PREC_FP32 if args.prec == "fp32" else P.PREC_FP64
+    kmax = math.sqrt(2.0) * n / 3.0
+    nu = (1.5 / kmax) ** (4.0 / 3.0) * 0.1 ** (1.0 / 3.0)
+    s = P.Solver(n=n, precision=prec, viscos=nu, cfl=math.pi, dt=0.0, kshift=1, kforce=2.99, tforce=0.5,
+                 epsfor=0.1 / (4.0 * (4.0 * math.pi / 3.0) * 27.0), tfiuo=0.0)
+    s.field_init(1234)
+    for _ in range(2):
+        s.step()
+    s.sync()
+    calls = {
+        "spectra": lambda: s.spectra(P.FIELD_UN),
+        "spectra_scales": lambda: s.spectra_scales(P.FIELD_UN),
+        "gradient_moments": lambda: s.gradient_moments(P.FIELD_UN, (0.1, 0.2, 0.3)),
+        "transfer_spectrum": lambda: s.transfer_spectrum((0.1, 0.2, 0.3)),
+        "step": lambda: (s.step(), s.sync()),
+    }
+    out = {"metric": "diagnostics at %d^3 (ms per call, median)" % n, "n": n, "precision": args.prec,
+           "timing": "host clock around each synchronous call"}
+    for name, f in calls.items():
+        for _ in range(max(1, args.warmup)):
+            f()
+        ts = []
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            f()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        out[name + "_ms"] = statistics.median(ts)
+    s.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.diagnostics:
+        return run_diagnostics(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.dft_lines > 0:
