@@ -1021,10 +1021,10 @@ static int spectra_scales_of(const Geo& g, const void* src, int prec, const psdn
   const size_t smem = nv * sizeof(double);
   if (prec == PSDNS_PREC_FP64) {
     CK(cudaFuncSetAttribute(k_spectra_1d<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_spectra_1d<double><<<148, 512, smem, stream>>>(g, (const double2*)src, b22, d_out);
+    k_spectra_1d<double><<<148 * 2, 512, smem, stream>>>(g, (const double2*)src, b22, d_out);
   } else {
     CK(cudaFuncSetAttribute(k_spectra_1d<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_spectra_1d<float><<<148, 512, smem, stream>>>(g, (const float2*)src, b22, d_out);
+    k_spectra_1d<float><<<148 * 2, 512, smem, stream>>>(g, (const float2*)src, b22, d_out);
   }
   CK(cudaGetLastError());
   std::vector<double> h(nv);
