@@ -60,6 +60,8 @@ def parse():
                     help="1: also advance a passive scalar (Sc = 1, mean gradient (0, 1, 0))")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision arm (1-D transforms on the tensor cores, split BF16)")
+    ap.add_argument("--no-extra-arms", action="store_true",
+                    help="skip the FP64-state and passive-scalar timings at 1024^3")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned arm (128^3 + spectral-correction network against 512^3 DNS)")
     ap.add_argument("--accuracy-steps", type=int, default=3,
@@ -529,9 +531,10 @@ def main():
                          f"{cores} threads, {t:.2f} s); Gpts/s = {args.cpu_n}^3/t"}
     s.close()
 
-    def make_solver(p_, mode):
+    def make_solver(p_, mode, nc=None):
         t = P.Solver(n=n, precision=p_, viscos=nu, cfl=math.pi, dt=0.0, kshift=1, kforce=kforce, tforce=0.5,
-                     epsfor=epsfor, tfiuo=0.0, nc=args.nc, pr=1.0, grad=(0.0, 1.0, 0.0), dft=mode)
+                     epsfor=epsfor, tfiuo=0.0, nc=args.nc if nc is None else nc, pr=1.0, grad=(0.0, 1.0, 0.0),
+                     dft=mode)
         t.field_init(1234 + rank)
         if npart > 0:
             t.particles_set(1.0 + np.random.default_rng(4321 + rank).random((npart, 3)) * n)
@@ -567,6 +570,32 @@ def main():
                      "gpu_launches": int(sum(mc[:5]) + 4 * mc[5])}
         except Exception as ex:
             mixed = {"error": str(ex)[:300]}
+    # the same workload with an FP64 state, and with one passive scalar (Sc 1,
+    # mean gradient (0, 1, 0)), timed like the plain arm (CUDA events on the
+    # solver's stream, --warmup then --steps steps); one GPU only
+    def timed_arm(t):
+        tstream = torch.cuda.ExternalStream(t.stream())
+        for _ in range(args.warmup):
+            t.step()
+        torch.cuda.synchronize()
+        e0.record(tstream)
+        for _ in range(args.steps):
+            t.step()
+        e1.record(tstream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    other_arms = {}
+    if rank == 0 and world == 1 and n == 1024 and prec == P.PREC_FP32 and args.nc == 0 and not args.no_extra_arms:
+        for name, p_, nc_ in (("fp64_state", P.PREC_FP64, 0), ("scalar_nc1_fp32", P.PREC_FP32, 1)):
+            try:
+                t = make_solver(p_, P.DFT_FP32, nc_)
+                ams = timed_arm(t)
+                t.close()
+                other_arms[name] = {"ms_per_step": ams, "value": aggregate_rate(world, n, ams), "unit": UNIT,
+                                    "particles": npart, "nc": nc_}
+            except Exception as ex:
+                other_arms[name] = {"error": str(ex)[:300]}
     # learned arm: 512^3 forced DNS (kmax eta = 1.5) against a 128^3 box with
     # the spectral-correction network, trained on the device on filtered
     # 512^3 data made in the same run (learned.py); wall time per step of
@@ -610,8 +639,8 @@ def main():
                          "step_achieved": step_bytes / (ms_step * 1e-3) / 1e9,
                          "step_frac": step_bytes / (ms_step * 1e-3) / 1e9 / peak},
             "kernels": kernel_table,
-            "arms": {"plain_fp32": {"ms_per_step": ms_step, "value": value, "unit": UNIT}, "mixed_bf16x3": mixed,
-                     "learned_128_vs_512": learned_arm},
+            "arms": dict({"plain_fp32": {"ms_per_step": ms_step, "value": value, "unit": UNIT},
+                          "mixed_bf16x3": mixed, "learned_128_vs_512": learned_arm}, **other_arms),
             "accuracy": accuracy,
             "cpu_baseline": cpu,
             "e2e": e2e,

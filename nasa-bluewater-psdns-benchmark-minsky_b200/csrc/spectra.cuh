@@ -54,8 +54,8 @@ __global__ void __launch_bounds__(512) k_spectra(Geo g, const C2<T>* __restrict_
       if (y == n / 2 || kya > km) continue;
       const double ky = y > n / 2 ? y - n : y;
       // sptr.f:85-97: Nyquist rows contribute no wavenumber (masked anyway)
-      const double rk2 = rxz + b22 * ky * ky;
-      const int ik = (int)(sqrt(rk2) + 1.5) - 1;
+      const double rk2 = rxz + b22 * ky * ky, rk = sqrt(rk2);
+      const int ik = (int)(rk + 1.5) - 1;
       if (ik < 0 || ik >= nshell) continue;
       if (ik != cur) {
         flush();
@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(512) k_spectra(Geo g, const C2<T>* __restrict_
       const double tr = e11 + e22 + e33;
       acc[6] += rk2 * tr;
       acc[7] += rk2 * rk2 * tr;
-      if (rk2 != 0.) acc[8] += (e11 * b11 + e22 * b22 + e33 * b33) / sqrt(rk2);
+      if (rk2 != 0.) acc[8] += (e11 * b11 + e22 * b22 + e33 * b33) / rk;
     }
     flush();
   }
