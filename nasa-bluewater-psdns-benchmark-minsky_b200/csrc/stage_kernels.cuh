@@ -1406,12 +1406,16 @@ static __global__ void __launch_bounds__(256) k_moments_reduce(const double* __r
 // along one axis.  jloc = ipx mod n in [0, n) (the reference adds 1000 n to
 // a negative ipx before its modulo), taken as fl - n floor(fl / n): exact in
 // FP64 while |ipx| < 2^52 / n, so bfp has the reference's value bit for bit.
+// For n = 2^k, fl / n is the exact product fl * 2^-k (2^-k built from its
+// exponent bits), so the FP64 division is taken only for other n.
 __device__ __forceinline__ void spline_weights(double pos, double gfn, int n, int& ib, double w[4]) {
   const double px1 = pos - gfn;
   const double px = px1 - (double)n;
   const double fl = floor(px);
   const double dn = (double)n;
-  const double jloc = fl - dn * floor(fl / dn);
+  const double q = (n & (n - 1)) == 0 ? fl * __longlong_as_double((long long)(1023 - (31 - __clz(n))) << 52)
+                                      : fl / dn;
+  const double jloc = fl - dn * floor(q);
   const double bfp = (jloc + px) - fl;
   ib = (int)bfp;
   const double t = bfp - ib;
